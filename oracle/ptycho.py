@@ -1,0 +1,94 @@
+"""NumPy restatement of the reference ptychography operator.
+
+TEST INFRASTRUCTURE (the oracle).  Follows:
+
+* constructor        src/cuda/ptychofft.cu:5-33
+* setobj             src/cuda/ptychofft.cu:48-56 + takeshifts (kernels.cuh:306-317)
+* fwd                src/cuda/ptychofft.cu:58-76 + mul (kernels.cuh:243-265), shifts (:319-336)
+* adj                src/cuda/ptychofft.cu:78-93 + shiftsa (kernels.cuh:338-355), mula (:267-288)
+
+Layouts: object psi is [Ntheta, Nz, N]; data g is [Ntheta, Nscan, detx, dety];
+scan is [2, Ntheta, Nscan] float32 (x then y); prb is [Nprb, Nprb].
+Frame element (ix, iy) multiplies prb[ix, iy] with psi[sty+iy, stx+ix]
+(kernels.cuh:257-263): the detector row runs along the object column.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PI_REF = 3.1415926535  # kernels.cuh:1
+
+
+def roundf(v):
+    """C roundf: half away from zero (evaluated in float64, exact for float32)."""
+    v = np.asarray(v, np.float64)
+    return np.sign(v) * np.floor(np.abs(v) + 0.5)
+
+
+def scan_corners(scan):
+    """Integer patch corners (stx, sty) = roundf(scan), kernels.cuh:255-256."""
+    scan = np.asarray(scan, np.float32)
+    return roundf(scan[0]).astype(np.int64), roundf(scan[1]).astype(np.int64)
+
+
+def scan_phases(scan):
+    """takeshifts, kernels.cuh:306-317: exp(2*pi*i*(scan - roundf(scan)))."""
+    scan = np.asarray(scan, np.float32)
+    out = []
+    for v in (scan[0], scan[1]):
+        frac = (v - roundf(v).astype(np.float32)).astype(np.float32)
+        arg = np.float32(2 * PI_REF * frac.astype(np.float64)).astype(np.float64)
+        out.append(np.cos(arg) + 1j * np.sin(arg))
+    return out[0], out[1]
+
+
+class PtychoFFT:
+    """Oracle twin of class ptychofft (ptychofft.cuh, ptychofft.cu)."""
+
+    def __init__(self, ntheta, nz, n, ntheta0, nscan, detx, dety, nprb):
+        self.ntheta, self.nz, self.n = ntheta, nz, n
+        self.nscan, self.detx, self.dety, self.nprb = nscan, detx, dety, nprb
+        self.c = 1.0 / np.sqrt(np.float32(detx * dety))   # kernels.cuh:260
+
+    def setobj(self, scan, prb):
+        scan = np.asarray(scan, np.float32).reshape(2, self.ntheta, self.nscan)
+        self.stx, self.sty = scan_corners(scan)
+        sx, sy = scan_phases(scan)
+        self.phase = sx * sy
+        self.prb = np.asarray(prb).astype(np.complex128).reshape(self.nprb, self.nprb)
+        P = self.nprb
+        ok = (self.stx >= 0) & (self.sty >= 0)
+        if np.any(ok & ((self.stx + P > self.n) | (self.sty + P > self.nz))):
+            raise ValueError("scan patch exceeds the object (reference has no upper bound check)")
+
+    def fwd(self, f):
+        P, dx, dy = self.nprb, self.detx, self.dety
+        f = np.asarray(f).reshape(self.ntheta, self.nz, self.n)
+        rs, cs = (dx - P) // 2, (dy - P) // 2
+        g = np.zeros((self.ntheta, self.nscan, dx, dy), np.complex128)
+        for t in range(self.ntheta):
+            for s in range(self.nscan):
+                x0, y0 = self.stx[t, s], self.sty[t, s]
+                if x0 < 0 or y0 < 0:
+                    continue
+                patch = f[t, y0:y0 + P, x0:x0 + P].astype(np.complex128).T   # [ix, iy]
+                g[t, s, rs:rs + P, cs:cs + P] = self.c * self.prb * patch
+        g = np.fft.fft2(g, axes=(-2, -1))
+        g *= self.phase[:, :, None, None]
+        return g
+
+    def adj(self, g):
+        P, dx, dy = self.nprb, self.detx, self.dety
+        g = np.asarray(g).reshape(self.ntheta, self.nscan, dx, dy).astype(np.complex128)
+        rs, cs = (dx - P) // 2, (dy - P) // 2
+        g = g * np.conj(self.phase)[:, :, None, None]
+        g = np.fft.ifft2(g, axes=(-2, -1)) * (dx * dy)
+        f = np.zeros((self.ntheta, self.nz, self.n), np.complex128)
+        cp = self.c * np.conj(self.prb)
+        for t in range(self.ntheta):
+            for s in range(self.nscan):
+                x0, y0 = self.stx[t, s], self.sty[t, s]
+                if x0 < 0 or y0 < 0:
+                    continue
+                f[t, y0:y0 + P, x0:x0 + P] += (cp * g[t, s, rs:rs + P, cs:cs + P]).T
+        return f

@@ -1,0 +1,327 @@
+// Ptychography operator for sm_100a.
+//
+// Replaces class ptychofft of the reference (src/cuda/ptychofft.cu:1-93,
+// kernels mul/mula/takeshifts/shifts/shiftsa in src/include/kernels.cuh).
+//
+//  forward  g = F Q psi   (ptychofft.cu:58-76): one block per frame
+//    (angle, scan).  The probe-weighted patch is written transposed into a
+//    det x det shared-memory frame (detector row = object column,
+//    kernels.cuh:257-263), the 2-D FFT runs in shared memory and the
+//    constant per-scan phase (kernels.cuh:306-336) is applied on the way
+//    out.  No zero-filled frame buffer, no device-to-device copies.
+//  adjoint  psi = Q* F* g (ptychofft.cu:78-93): one block per angle walks its
+//    scans in order: conjugate phase, inverse 2-D FFT in shared memory,
+//    conj(probe) and accumulation into that angle's object slab.  Only this
+//    block writes the slab, so the sum is deterministic and needs no atomics.
+#include <cmath>
+#include <vector>
+
+#include "pt_common.cuh"
+#include "pt_fft.cuh"
+
+namespace {
+
+constexpr double PI_REF = 3.1415926535;  // kernels.cuh:1
+
+template <int DET>
+constexpr int ptycho_fft_threads() { return (512 / DET) < 4 ? 4 : ((512 / DET) > 32 ? 32 : 512 / DET); }
+template <int DET>
+constexpr int ptycho_block() { return DET * ptycho_fft_threads<DET>(); }
+
+// setobj tables: integer corners (kernels.cuh:255-256) and the per-scan
+// phase shiftx*shifty (takeshifts, kernels.cuh:306-317, same expressions).
+__global__ void k_ptycho_tables(const float *__restrict__ scan, int *__restrict__ corner,
+                                float2 *__restrict__ phase, int nframes)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nframes) return;
+    const float sx = scan[i], sy = scan[nframes + i];
+    corner[2 * i] = (int)roundf(sx);
+    corner[2 * i + 1] = (int)roundf(sy);
+    float2 px, py;
+    px.x = cosf(2 * PI_REF * (sx - roundf(sx)));
+    px.y = sinf(2 * PI_REF * (sx - roundf(sx)));
+    py.x = cosf(2 * PI_REF * (sy - roundf(sy)));
+    py.y = sinf(2 * PI_REF * (sy - roundf(sy)));
+    phase[i] = cmul(px, py);
+}
+
+template <int DET>
+__global__ void __launch_bounds__(ptycho_block<DET>(), 1)
+    k_ptycho_fwd(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
+                 const float2 *__restrict__ phase, const float2 *__restrict__ prb, int nz, int n, int nscan,
+                 int P, float c, float scale, const float2 *__restrict__ tw)
+{
+    constexpr int T = ptycho_fft_threads<DET>(), NT = ptycho_block<DET>(), PITCH = DET + 1;
+    extern __shared__ float2 fr[];
+    const int s = blockIdx.x, th = blockIdx.y;
+    const int fid = th * nscan + s;
+    const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
+    float2 *out = g + (size_t)fid * DET * DET;
+    if (stx < 0 || sty < 0) {  // skipped scan: the reference leaves a zero frame
+        for (int e = threadIdx.x; e < DET * DET; e += NT) out[e] = czero();
+        return;
+    }
+    if (P < DET) {
+        for (int e = threadIdx.x; e < DET * DET; e += NT) fr[(e / DET) * PITCH + e % DET] = czero();
+        __syncthreads();
+    }
+    const int off = (DET - P) / 2;
+    const float2 *src = psi + ((size_t)th * nz + sty) * n + stx;
+    for (int e = threadIdx.x; e < P * P; e += NT) {
+        const int iy = e / P, ix = e % P;
+        const float2 v = src[(size_t)iy * n + ix];
+        const float2 pr = prb[ix * P + iy];
+        fr[(off + ix) * PITCH + off + iy] = c * cmul(pr, v);
+    }
+    __syncthreads();
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    ptfft::fft<DET, -1, T>(fr + f * PITCH, 1, t, tw);  // along the detector row
+    ptfft::fft<DET, -1, T>(fr + f, PITCH, t, tw);      // along the detector column
+    const float2 ph = scale * phase[fid];
+    for (int e = threadIdx.x; e < DET * DET; e += NT) out[e] = cmul(fr[(e / DET) * PITCH + e % DET], ph);
+}
+
+template <int DET>
+__global__ void __launch_bounds__(ptycho_block<DET>(), 1)
+    k_ptycho_adj(const float2 *__restrict__ g, float2 *__restrict__ psi, const int *__restrict__ corner,
+                 const float2 *__restrict__ phase, const float2 *__restrict__ prb, int nz, int n, int nscan,
+                 int P, float c, float scale, const float2 *__restrict__ tw)
+{
+    constexpr int T = ptycho_fft_threads<DET>(), NT = ptycho_block<DET>(), PITCH = DET + 1;
+    extern __shared__ float2 fr[];
+    const int th = blockIdx.x;
+    float2 *slab = psi + (size_t)th * nz * n;
+    for (int e = threadIdx.x; e < nz * n; e += NT) slab[e] = czero();
+    __syncthreads();
+    const int off = (DET - P) / 2;
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    const float cs = c * scale;
+    for (int s = 0; s < nscan; ++s) {
+        const int fid = th * nscan + s;
+        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
+        if (stx < 0 || sty < 0) continue;
+        const float2 ph = phase[fid];
+        const float2 *in = g + (size_t)fid * DET * DET;
+        for (int e = threadIdx.x; e < DET * DET; e += NT) fr[(e / DET) * PITCH + e % DET] = cmulc(ph, in[e]);
+        __syncthreads();
+        ptfft::fft<DET, +1, T>(fr + f * PITCH, 1, t, tw);
+        ptfft::fft<DET, +1, T>(fr + f, PITCH, t, tw);
+        float2 *dst = slab + (size_t)sty * n + stx;
+        for (int e = threadIdx.x; e < P * P; e += NT) {
+            const int iy = e / P, ix = e % P;
+            const float2 v = cs * cmulc(prb[ix * P + iy], fr[(off + ix) * PITCH + off + iy]);
+            float2 *d = dst + (size_t)iy * n + ix;
+            *d = *d + v;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+struct pt_ptycho {
+    int ntheta = 0, nz = 0, n = 0, nscan = 0, det = 0, P = 0;
+    int device = -1;
+    bool ready = false;
+    float c = 0.f;
+    float2 *tw = nullptr, *prb = nullptr, *phase = nullptr;
+    int *corner = nullptr;
+};
+
+namespace {
+
+#define PT_PTYCHO_DETS(X) X(8) X(16) X(32) X(64) X(128)
+
+template <int DET>
+int ptycho_attrs()
+{
+    const int s = DET * (DET + 1) * sizeof(float2);
+    PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+    PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+    return PT_OK;
+}
+
+template <int DET>
+int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st)
+{
+    const size_t s = DET * (DET + 1) * sizeof(float2);
+    if (!adj) {
+        k_ptycho_fwd<DET><<<dim3(h->nscan, h->ntheta), ptycho_block<DET>(), s, st>>>(
+            in, out, h->corner, h->phase, h->prb, h->nz, h->n, h->nscan, h->P, h->c, scale, h->tw);
+        PT_LAUNCHED("k_ptycho_fwd");
+    } else {
+        k_ptycho_adj<DET><<<h->ntheta, ptycho_block<DET>(), s, st>>>(in, out, h->corner, h->phase, h->prb,
+                                                                   h->nz, h->n, h->nscan, h->P, h->c,
+                                                                   scale, h->tw);
+        PT_LAUNCHED("k_ptycho_adj");
+    }
+    return PT_OK;
+}
+
+bool det_supported(int d)
+{
+#define PT_CASE(D) \
+    if (d == D) return true;
+    PT_PTYCHO_DETS(PT_CASE)
+#undef PT_CASE
+    return false;
+}
+
+int ptycho_set_attrs(int d)
+{
+#define PT_CASE(D) \
+    if (d == D) return ptycho_attrs<D>();
+    PT_PTYCHO_DETS(PT_CASE)
+#undef PT_CASE
+    return PT_ERR_UNSUPPORTED;
+}
+
+int ptycho_dispatch(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st)
+{
+#define PT_CASE(D) \
+    if (h->det == D) return ptycho_run<D>(h, adj, out, in, scale, st);
+    PT_PTYCHO_DETS(PT_CASE)
+#undef PT_CASE
+    pt::set_error("ptychofft: detector size %d not compiled", h->det);
+    return PT_ERR_UNSUPPORTED;
+}
+
+void ptycho_free(pt_ptycho *h)
+{
+    void *bufs[] = {h->tw, h->prb, h->phase, h->corner};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+}
+
+}  // namespace
+
+extern "C" int pt_ptycho_create(size_t ntheta, size_t nz, size_t n, size_t ntheta0, size_t nscan, size_t detx,
+                                size_t dety, size_t nprb, pt_ptycho **out)
+{
+    (void)ntheta0;
+    pt::clear_error();
+    PT_CHECK_ARG(out != nullptr, "ptychofft: null output handle");
+    *out = nullptr;
+    PT_CHECK_ARG(ntheta >= 1 && nz >= 1 && n >= 1 && nscan >= 1 && nprb >= 1,
+                 "ptychofft: sizes must be positive (Ntheta=%zu Nz=%zu N=%zu Nscan=%zu Nprb=%zu)", ntheta, nz, n,
+                 nscan, nprb);
+    PT_CHECK_ARG(ntheta * nscan < (1u << 31) && ntheta * nz * n < ((size_t)1 << 40), "ptychofft: sizes too large");
+    if (detx != dety || !det_supported((int)detx)) {
+        pt::set_error("ptychofft: detector %zux%zu not compiled (square 8,16,32,64,128)", detx, dety);
+        return PT_ERR_UNSUPPORTED;
+    }
+    PT_CHECK_ARG(nprb <= detx, "ptychofft: probe %zu larger than detector %zu", nprb, detx);
+    PT_CHECK_ARG(nprb <= n && nprb <= nz, "ptychofft: probe %zu larger than the object %zux%zu", nprb, nz, n);
+    pt_ptycho *h = new pt_ptycho();
+    h->ntheta = (int)ntheta;
+    h->nz = (int)nz;
+    h->n = (int)n;
+    h->nscan = (int)nscan;
+    h->det = (int)detx;
+    h->P = (int)nprb;
+    h->c = 1 / sqrtf(detx * dety);  // kernels.cuh:260
+    if (cudaGetDevice(&h->device) != cudaSuccess) {
+        delete h;
+        pt::set_error("ptychofft: no CUDA device");
+        return PT_ERR_CUDA;
+    }
+    bool ok = cudaMalloc((void **)&h->tw, detx * sizeof(float2)) == cudaSuccess &&
+              cudaMalloc((void **)&h->prb, nprb * nprb * sizeof(float2)) == cudaSuccess &&
+              cudaMalloc((void **)&h->phase, ntheta * nscan * sizeof(float2)) == cudaSuccess &&
+              cudaMalloc((void **)&h->corner, 2 * ntheta * nscan * sizeof(int)) == cudaSuccess;
+    if (!ok) {
+        ptycho_free(h);
+        delete h;
+        pt::set_error("ptychofft: device allocation failed");
+        return PT_ERR_ALLOC;
+    }
+    std::vector<float2> tw(detx);
+    pt_make_twiddles(tw.data(), (int)detx);
+    int rc = ptycho_set_attrs((int)detx);
+    if (rc == PT_OK && cudaMemcpy(h->tw, tw.data(), detx * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+        pt::set_error("ptychofft: twiddle upload failed");
+        rc = PT_ERR_CUDA;
+    }
+    if (rc != PT_OK) {
+        ptycho_free(h);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return PT_OK;
+}
+
+extern "C" int pt_ptycho_destroy(pt_ptycho *h)
+{
+    pt::clear_error();
+    if (!h) return PT_OK;
+    ptycho_free(h);
+    delete h;
+    return PT_OK;
+}
+
+extern "C" int pt_ptycho_setobj(pt_ptycho *h, const float *scan, const void *prb, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h != nullptr, "ptychofft.setobj: null handle");
+    PT_CHECK_ARG(scan != nullptr && prb != nullptr, "ptychofft.setobj: null scan or probe");
+    int dev = -1;
+    PT_CUDA(cudaGetDevice(&dev));
+    PT_CHECK_ARG(dev == h->device, "ptychofft handle belongs to device %d, current device is %d", h->device, dev);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nf = h->ntheta * h->nscan;
+    h->ready = false;
+    PT_CUDA(cudaMemcpyAsync(h->prb, prb, (size_t)h->P * h->P * sizeof(float2), cudaMemcpyDefault, st));
+    k_ptycho_tables<<<(nf + 255) / 256, 256, 0, st>>>(scan, h->corner, h->phase, nf);
+    PT_LAUNCHED("k_ptycho_tables");
+    std::vector<int> corner(2 * (size_t)nf);
+    PT_CUDA(cudaMemcpyAsync(corner.data(), h->corner, corner.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < nf; ++i) {
+        const int x = corner[2 * i], y = corner[2 * i + 1];
+        if (x < 0 || y < 0) continue;  // sentinel: scan skipped
+        if (x + h->P > h->n || y + h->P > h->nz) {
+            pt::set_error("ptychofft.setobj: scan %d of angle %d at (%d,%d) puts the %dx%d probe outside the "
+                          "%dx%d object",
+                          i % h->nscan, i / h->nscan, x, y, h->P, h->P, h->nz, h->n);
+            return PT_ERR_ARG;
+        }
+    }
+    h->ready = true;
+    return PT_OK;
+}
+
+namespace {
+int ptycho_call(pt_ptycho *h, bool adj, void *out, const void *in, float scale, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h != nullptr, "ptychofft: null handle");
+    PT_CHECK_ARG(out != nullptr && in != nullptr, "ptychofft.%s: null array pointer", adj ? "adj" : "fwd");
+    if (!h->ready) {
+        pt::set_error("ptychofft.%s: setobj(scan, prb) has not been called", adj ? "adj" : "fwd");
+        return PT_ERR_STATE;
+    }
+    int dev = -1;
+    PT_CUDA(cudaGetDevice(&dev));
+    PT_CHECK_ARG(dev == h->device, "ptychofft handle belongs to device %d, current device is %d", h->device, dev);
+    return ptycho_dispatch(h, adj, (float2 *)out, (const float2 *)in, scale, (cudaStream_t)stream);
+}
+}  // namespace
+
+extern "C" int pt_ptycho_fwd(pt_ptycho *h, void *g, const void *f, void *stream)
+{
+    return ptycho_call(h, false, g, f, 1.0f, stream);
+}
+extern "C" int pt_ptycho_adj(pt_ptycho *h, void *f, const void *g, void *stream)
+{
+    return ptycho_call(h, true, f, g, 1.0f, stream);
+}
+extern "C" int pt_ptycho_fwd_scaled(pt_ptycho *h, void *g, const void *f, float scale, void *stream)
+{
+    return ptycho_call(h, false, g, f, scale, stream);
+}
+extern "C" int pt_ptycho_adj_scaled(pt_ptycho *h, void *f, const void *g, float scale, void *stream)
+{
+    return ptycho_call(h, true, f, g, scale, stream);
+}

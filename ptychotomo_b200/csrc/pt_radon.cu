@@ -1,0 +1,750 @@
+// USFFT Radon transform (tomography operator) for sm_100a.
+//
+// Replaces class radonusfft of the reference (src/cuda/radonusfft.cu:1-144,
+// kernels src/include/kernels.cuh:5-216).  Same mathematics, different
+// machinery:
+//
+//  forward  R f   (radonusfft.cu:54-92)
+//    K1 k_fwd_rows    pad2 edge replication + circ mask + deapodisation 1/phi
+//                     + centring sign, zero-pad to 2N, row FFT (the N rows
+//                     that are non-zero)                       [smem FFT]
+//    K2 k_fwd_cols    column FFT of length 2N (zero rows implicit) with the
+//                     post-FFT centring sign folded in          [smem FFT]
+//    K3 k_fwd_gather  Gaussian-kernel gather at the polar points, 1-D
+//                     centred inverse FFT along the detector, crop n of N
+//  adjoint  R* g  (radonusfft.cu:94-139)
+//    A1 k_adj_lines   edge-replicating pad, centred 1-D FFT
+//    A2 k_adj_scatter deterministic binned scatter: each block owns a tile of
+//                     the Fourier grid and sums, in a fixed order, the
+//                     contributions of the polar points whose kernel window
+//                     covers it (no float atomics, no halo, no fold pass)
+//    A3 k_adj_cols    column inverse FFT, keeping only the n rows that
+//                     survive the final crop
+//    A4 k_adj_rows    row inverse FFT + centring sign + 1/phi + circ + crop
+//
+// Slices are processed in chunks of ZC = 8; inside a chunk all intermediates
+// are stored slice-minor ([.. ][ZC]) so every tap of the gather, and every row
+// of the column kernels, is a contiguous 64-byte segment.  A chunk's
+// intermediates (N*2N + (2N)^2 complex per slice) stay far below L2 size.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "pt_common.cuh"
+#include "pt_fft.cuh"
+
+namespace {
+
+constexpr int ZC = 8;   // slices per chunk (slice-minor lanes)
+constexpr int CK = 2;   // grid columns per block in the column kernels
+constexpr int GB = 64;  // polar points staged per batch in the adjoint scatter
+constexpr double PI_REF = 3.1415926535;  // kernels.cuh:1
+
+template <int L>
+constexpr int fft_threads() { return L >= 1024 ? 64 : 32; }
+
+// circ, kernels.cuh:160-172 (r = 1.0f/N); evaluated without FMA contraction so
+// that it equals the float32 expression (4x*x + 4y*y) < 1 - r exactly.
+__device__ __forceinline__ float circ_keep(int tx, int ty, int N)
+{
+    const float x = (float)(tx - N / 2) / (float)N;
+    const float y = (float)(ty - N / 2) / (float)N;
+    const float lhs = __fadd_rn(__fmul_rn(__fmul_rn(4.f, x), x), __fmul_rn(__fmul_rn(4.f, y), y));
+    const float r = 1.0f / (float)N;
+    return lhs < 1.f - r ? 1.f : 0.f;
+}
+
+// phi, kernels.cuh:12 and :23 (same expression as the reference)
+__device__ __forceinline__ float deapod(int tx, int ty, int N, float mu)
+{
+    return __expf(-mu * (tx - N / 2) * (tx - N / 2) - mu * (ty - N / 2) * (ty - N / 2));
+}
+
+__device__ __forceinline__ int wrapG(int c, int G) { return c < 0 ? c + G : (c >= G ? c - G : c); }
+
+// ---- geometry: takexy, kernels.cuh:84-95 (identical expression) -----------
+__global__ void k_takexy(float *x, float *y, const float *theta, int N, int ntheta)
+{
+    const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ty = blockIdx.y;
+    if (tx >= N || ty >= ntheta) return;
+    float xv = (tx - N / 2) / (float)N * __cosf(theta[ty]);
+    float yv = -(tx - N / 2) / (float)N * __sinf(theta[ty]);
+    if (xv >= 0.5f) xv = 0.5f - 1e-5;
+    if (yv >= 0.5f) yv = 0.5f - 1e-5;
+    x[tx + ty * N] = xv;
+    y[tx + ty * N] = yv;
+}
+
+// ---- K1: pad2 + circ + divphi + fftshiftc + row FFT ------------------------
+template <int G>
+__global__ void __launch_bounds__(ZC *fft_threads<G>())
+    k_fwd_rows(const float2 *__restrict__ u, float2 *__restrict__ rbuf, int nz, int z0, float mu,
+               const float2 *__restrict__ tw)
+{
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, PITCH = G + 1;
+    constexpr int c0 = N / 6, c1 = 5 * N / 6 - 1;
+    extern __shared__ float2 sm[];
+    const int y = blockIdx.x;
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    const int z = z0 + f;
+    const int sr = min(max(y, c0), c1) - c0;
+    const int Y = y + N / 2;
+    const float den = (float)(4 * N * N);
+    float2 *b = sm + f * PITCH;
+    for (int X = t; X < G; X += T) {
+        float2 v = czero();
+        const int tx = X - N / 2;
+        if (tx >= 0 && tx < N && z < nz) {
+            const int sc = min(max(tx, c0), c1) - c0;
+            v = u[((size_t)z * n + sr) * n + sc];
+            const float keep = circ_keep(tx, y, N);
+            const float phi = deapod(tx, y, N, mu);
+            v.x = v.x * keep / phi / den;
+            v.y = v.y * keep / phi / den;
+            if ((X + Y) & 1) v = -1.f * v;
+        }
+        b[X] = v;
+    }
+    __syncthreads();
+    ptfft::fft<G, -1, T>(b, 1, t, tw);
+    for (int e = threadIdx.x; e < G * ZC; e += blockDim.x) {
+        const int kx = e / ZC, q = e % ZC;
+        rbuf[((size_t)y * G + kx) * ZC + q] = sm[q * PITCH + kx];
+    }
+}
+
+// ---- K2: column FFT of the 2N grid, centring sign folded in ----------------
+template <int G>
+__global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
+    k_fwd_cols(const float2 *__restrict__ rbuf, float2 *__restrict__ fg, const float2 *__restrict__ tw)
+{
+    constexpr int T = fft_threads<G>(), N = G / 2, PITCH = G + 1, NF = CK * ZC;
+    extern __shared__ float2 sm[];
+    const int kx0 = blockIdx.x * CK;
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    for (int e = threadIdx.x; e < N * NF; e += blockDim.x) {
+        const int y = e / NF, q = e % NF;
+        sm[q * PITCH + N / 2 + y] = rbuf[((size_t)y * G + kx0) * ZC + q];
+    }
+    for (int e = threadIdx.x; e < N * NF; e += blockDim.x) {
+        const int q = e / N, i = e % N;
+        sm[q * PITCH + (i < N / 2 ? i : i + N)] = czero();
+    }
+    __syncthreads();
+    ptfft::fft<G, -1, T>(sm + f * PITCH, 1, t, tw);
+    for (int e = threadIdx.x; e < G * NF; e += blockDim.x) {
+        const int ky = e / NF, q = e % NF;
+        const int kx = kx0 + q / ZC;
+        float2 v = sm[q * PITCH + ky];
+        if ((kx + ky) & 1) v = -1.f * v;
+        fg[((size_t)ky * G + kx0) * ZC + q] = v;
+    }
+}
+
+// ---- K3: gather (kernels.cuh:97-126) + fftshift1c/IFFT/fftshift1c + crop ---
+template <int N, int M>
+__global__ void __launch_bounds__(ZC * 32)
+    k_fwd_gather(const float2 *__restrict__ fg, float2 *__restrict__ out, const float *__restrict__ xt,
+                 const float *__restrict__ yt, int nz, int z0, float a, float pre, float scale,
+                 const float2 *__restrict__ tw)
+{
+    constexpr int G = 2 * N, n = 2 * N / 3, c0 = N / 6, W = 2 * M + 1, PITCH = N + 1, T = 32;
+    extern __shared__ float2 sm[];
+    const int th = blockIdx.x;
+    const int lane = threadIdx.x % ZC, grp = threadIdx.x / ZC;
+    for (int k = grp; k < N; k += 32) {
+        const float x0 = xt[th * N + k], y0 = yt[th * N + k];
+        // x0, y0 in [-1/2, 1/2) (validated at setobj); clamp keeps reads in bounds
+        const int fx = min(max((int)floorf((float)G * x0), -N), N - 1);
+        const int fy = min(max((int)floorf((float)G * y0), -N), N - 1);
+        float wx[W], wy[W];
+        int col[W];
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+            const float w0 = (float)(fx - M + i) / (float)G - x0;
+            const float w1 = (float)(fy - M + i) / (float)G - y0;
+            wx[i] = expf(-a * (w0 * w0));
+            wy[i] = expf(-a * (w1 * w1));
+            col[i] = wrapG(N + fx - M + i, G) * ZC + lane;
+        }
+        float2 acc = czero();
+#pragma unroll
+        for (int i1 = 0; i1 < W; ++i1) {
+            const float2 *rowp = fg + (size_t)wrapG(N + fy - M + i1, G) * G * ZC;
+            float2 rs = czero();
+#pragma unroll
+            for (int i0 = 0; i0 < W; ++i0) {
+                const float2 v = __ldg(rowp + col[i0]);
+                rs.x = fmaf(wx[i0], v.x, rs.x);
+                rs.y = fmaf(wx[i0], v.y, rs.y);
+            }
+            acc.x = fmaf(wy[i1], rs.x, acc.x);
+            acc.y = fmaf(wy[i1], rs.y, acc.y);
+        }
+        // fftshift1c sign (1-2((k+1)%2)) and the 1/N of kernels.cuh:124-125
+        sm[lane * PITCH + k] = ((k & 1) ? pre : -pre) * acc;
+    }
+    __syncthreads();
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    ptfft::fft<N, +1, T>(sm + f * PITCH, 1, t, tw);
+    for (int e = threadIdx.x; e < ZC * n; e += blockDim.x) {
+        const int q = e / n, j = e % n;
+        const int z = z0 + q;
+        if (z < nz) {
+            const int k = c0 + j;
+            out[((size_t)th * nz + z) * n + j] = ((k & 1) ? scale : -scale) * sm[q * PITCH + k];
+        }
+    }
+}
+
+// ---- A1: pad (kernels.cuh:189-206) + fftshift1c/FFT/fftshift1c -------------
+template <int N>
+__global__ void __launch_bounds__(ZC * 32)
+    k_adj_lines(const float2 *__restrict__ g, float2 *__restrict__ lines, int nz, int z0, float pre,
+                const float2 *__restrict__ tw)
+{
+    constexpr int n = 2 * N / 3, c0 = N / 6, c1 = 5 * N / 6 - 1, PITCH = N + 1, T = 32;
+    extern __shared__ float2 sm[];
+    const int th = blockIdx.x;
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    const int z = z0 + f;
+    float2 *b = sm + f * PITCH;
+    for (int k = t; k < N; k += T) {
+        float2 v = czero();
+        if (z < nz) v = g[((size_t)th * nz + z) * n + (min(max(k, c0), c1) - c0)];
+        b[k] = (k & 1) ? v : -1.f * v;
+    }
+    __syncthreads();
+    ptfft::fft<N, -1, T>(b, 1, t, tw);
+    for (int e = threadIdx.x; e < N * ZC; e += blockDim.x) {
+        const int k = e / ZC, q = e % ZC;
+        lines[((size_t)th * N + k) * ZC + q] = ((k & 1) ? pre : -pre) * sm[q * PITCH + k];
+    }
+}
+
+// ---- A2: binned deterministic scatter (transpose of the gather) ------------
+// Block = one TS x TS tile of the (2N)^2 Fourier grid, thread = one cell,
+// ZC slices in registers.  Points whose 15x15 window covers the tile are
+// listed (increasing point index) in a CSR built at setobj.
+template <int M, int TS>
+__global__ void __launch_bounds__(TS *TS)
+    k_adj_scatter(const float2 *__restrict__ lines, float2 *__restrict__ fadj, const int *__restrict__ tile_off,
+                  const int *__restrict__ tile_pts, const int *__restrict__ fxy, const float *__restrict__ xt,
+                  const float *__restrict__ yt, int N, float a)
+{
+    constexpr int W = 2 * M + 1;
+    __shared__ float s_wx[GB][W];
+    __shared__ float s_wy[GB][W];
+    __shared__ int s_ox[GB], s_oy[GB];
+    __shared__ float2 s_g[GB][ZC];
+    const int G = 2 * N;
+    const int ntx = G / TS;
+    const int tile = blockIdx.x;
+    const int cx = (tile % ntx) * TS + threadIdx.x % TS;
+    const int cy = (tile / ntx) * TS + threadIdx.x / TS;
+    float2 acc[ZC];
+#pragma unroll
+    for (int q = 0; q < ZC; ++q) acc[q] = czero();
+    const int beg = tile_off[tile], end = tile_off[tile + 1];
+    for (int b0 = beg; b0 < end; b0 += GB) {
+        const int cnt = min(GB, end - b0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < cnt * 2 * W; e += blockDim.x) {
+            const int p = e / (2 * W), i = e % (2 * W);
+            const int pid = tile_pts[b0 + p];
+            if (i < W) {
+                const float x0 = xt[pid];
+                const float w0 = (float)(fxy[2 * pid] - M + i) / (float)G - x0;
+                s_wx[p][i] = expf(-a * (w0 * w0));
+            } else {
+                const float y0 = yt[pid];
+                const float w1 = (float)(fxy[2 * pid + 1] - M + (i - W)) / (float)G - y0;
+                s_wy[p][i - W] = expf(-a * (w1 * w1));
+            }
+        }
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+            const int pid = tile_pts[b0 + e];
+            s_ox[e] = wrapG(N + fxy[2 * pid] - M, G);
+            s_oy[e] = wrapG(N + fxy[2 * pid + 1] - M, G);
+        }
+        for (int e = threadIdx.x; e < cnt * ZC; e += blockDim.x) {
+            const int p = e / ZC, q = e % ZC;
+            s_g[p][q] = lines[(size_t)tile_pts[b0 + p] * ZC + q];
+        }
+        __syncthreads();
+        for (int p = 0; p < cnt; ++p) {
+            int dx = cx - s_ox[p];
+            dx += dx < 0 ? G : 0;
+            int dy = cy - s_oy[p];
+            dy += dy < 0 ? G : 0;
+            if (dx < W && dy < W) {
+                const float w = s_wx[p][dx] * s_wy[p][dy];
+#pragma unroll
+                for (int q = 0; q < ZC; ++q) {
+                    const float2 v = s_g[p][q];
+                    acc[q].x = fmaf(w, v.x, acc[q].x);
+                    acc[q].y = fmaf(w, v.y, acc[q].y);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < ZC; ++q) fadj[((size_t)cy * G + cx) * ZC + q] = acc[q];
+}
+
+// ---- A3: centring sign + column inverse FFT, keep the n cropped rows ------
+template <int G>
+__global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
+    k_adj_cols(const float2 *__restrict__ fadj, float2 *__restrict__ rbuf, const float2 *__restrict__ tw)
+{
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, PITCH = G + 1, NF = CK * ZC;
+    extern __shared__ float2 sm[];
+    const int kx0 = blockIdx.x * CK;
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    for (int e = threadIdx.x; e < G * NF; e += blockDim.x) {
+        const int ky = e / NF, q = e % NF;
+        const int kx = kx0 + q / ZC;
+        float2 v = fadj[((size_t)ky * G + kx0) * ZC + q];
+        if ((kx + ky) & 1) v = -1.f * v;
+        sm[q * PITCH + ky] = v;
+    }
+    __syncthreads();
+    ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
+    constexpr int Y0 = N / 2 + N / 6;
+    for (int e = threadIdx.x; e < n * NF; e += blockDim.x) {
+        const int r = e / NF, q = e % NF;
+        rbuf[((size_t)r * G + kx0) * ZC + q] = sm[q * PITCH + Y0 + r];
+    }
+}
+
+// ---- A4: row inverse FFT + fftshiftc + unpaddivphi + circ + crop -----------
+template <int G>
+__global__ void __launch_bounds__(ZC *fft_threads<G>())
+    k_adj_rows(const float2 *__restrict__ rbuf, float2 *__restrict__ out, int nz, int z0, float mu, float scale,
+               const float2 *__restrict__ tw)
+{
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, c0 = N / 6, PITCH = G + 1;
+    extern __shared__ float2 sm[];
+    const int r = blockIdx.x;
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    for (int e = threadIdx.x; e < G * ZC; e += blockDim.x) {
+        const int kx = e / ZC, q = e % ZC;
+        sm[q * PITCH + kx] = rbuf[((size_t)r * G + kx) * ZC + q];
+    }
+    __syncthreads();
+    ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
+    const float den = (float)(4 * N * N);
+    for (int e = threadIdx.x; e < ZC * n; e += blockDim.x) {
+        const int q = e / n, c = e % n;
+        const int z = z0 + q;
+        if (z < nz) {
+            const int tx = c0 + c, ty = c0 + r;
+            const int X = N / 2 + tx, Y = N / 2 + ty;
+            float2 v = sm[q * PITCH + X];
+            if ((X + Y) & 1) v = -1.f * v;
+            const float phi = deapod(tx, ty, N, mu);
+            v.x = v.x / phi / den;
+            v.y = v.y / phi / den;
+            const float keep = circ_keep(tx, ty, N);
+            out[((size_t)z * n + r) * n + c] = (keep * scale) * v;
+        }
+    }
+}
+
+}  // namespace
+
+// ============================================================================
+// handle
+// ============================================================================
+struct pt_radon {
+    int ntheta = 0, nz = 0, n = 0, N = 0, G = 0, M = 0, TS = 0;
+    float mu = 0.f;
+    int device = -1;
+    bool ready = false;
+    float2 *tw_G = nullptr, *tw_N = nullptr;
+    float *theta = nullptr, *x = nullptr, *y = nullptr;
+    int *fxy = nullptr;
+    float2 *rbuf = nullptr, *fgrid = nullptr, *lines = nullptr;
+    int *tile_off = nullptr, *tile_pts = nullptr;
+    size_t tile_pts_cap = 0;
+};
+
+namespace {
+
+void radon_free(pt_radon *h)
+{
+    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->rbuf,
+                    h->fgrid, h->lines, h->tile_off, h->tile_pts};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+}
+
+// Kernel half-width for a forced M: choose -log(eps) so that the reference's
+// formula (radonusfft.cu:12) yields exactly M, then mu = -log(eps)/(2N^2).
+void radon_params(int n, int m_override, int *N, int *M, float *mu)
+{
+    *N = n * 3 / 2;
+    const size_t NN = (size_t)*N;
+    if (m_override <= 0) {
+        float eps = 1e-6;  // radonusfft.cu:10-12, same expressions and types
+        *mu = -log(eps) / (2 * NN * NN);
+        *M = (int)ceil(2 * NN * 1 / PI_REF * sqrt(-*mu * log(eps) + (*mu * NN) * (*mu * NN) / 4));
+    } else {
+        const double L = m_override * PI_REF / 1.5 - 1e-3;  // ceil(2/pi*0.75*L) = M
+        *mu = (float)(L / (2.0 * (double)NN * (double)NN));
+        *M = m_override;
+    }
+}
+
+typedef int (*radon_run_fn)(pt_radon *, float2 *, const float2 *, float, cudaStream_t);
+
+template <int G>
+int set_attrs()
+{
+    constexpr int N = G / 2;
+    const int s1 = ZC * (G + 1) * sizeof(float2);
+    const int s2 = CK * ZC * (G + 1) * sizeof(float2);
+    PT_CUDA(cudaFuncSetAttribute(k_fwd_rows<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
+    PT_CUDA(cudaFuncSetAttribute(k_fwd_cols<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    PT_CUDA(cudaFuncSetAttribute(k_adj_cols<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    PT_CUDA(cudaFuncSetAttribute(k_adj_rows<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
+    const int s3 = ZC * (N + 1) * sizeof(float2);
+    PT_CUDA(cudaFuncSetAttribute(k_fwd_gather<N, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    PT_CUDA(cudaFuncSetAttribute(k_fwd_gather<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    PT_CUDA(cudaFuncSetAttribute(k_adj_lines<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    return PT_OK;
+}
+
+template <int G, int M>
+int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t st)
+{
+    constexpr int N = G / 2, T = fft_threads<G>();
+    const size_t s1 = ZC * (G + 1) * sizeof(float2);
+    const size_t s2 = CK * ZC * (G + 1) * sizeof(float2);
+    const size_t s3 = ZC * (N + 1) * sizeof(float2);
+    const float a = (float)(PI_REF * PI_REF / h->mu);
+    const float pre = (float)(PI_REF / std::fabs(h->mu)) / (float)N;
+    for (int z0 = 0; z0 < h->nz; z0 += ZC) {
+        k_fwd_rows<G><<<N, ZC * T, s1, st>>>(f, h->rbuf, h->nz, z0, h->mu, h->tw_G);
+        PT_LAUNCHED("k_fwd_rows");
+        k_fwd_cols<G><<<G / CK, CK * ZC * T, s2, st>>>(h->rbuf, h->fgrid, h->tw_G);
+        PT_LAUNCHED("k_fwd_cols");
+        k_fwd_gather<N, M><<<h->ntheta, ZC * 32, s3, st>>>(h->fgrid, g, h->x, h->y, h->nz, z0, a, pre,
+                                                           scale, h->tw_N);
+        PT_LAUNCHED("k_fwd_gather");
+    }
+    return PT_OK;
+}
+
+template <int G, int M>
+int run_adj(pt_radon *h, float2 *f, const float2 *g, float scale, cudaStream_t st)
+{
+    constexpr int N = G / 2, n = G / 3, T = fft_threads<G>();
+    const size_t s1 = ZC * (G + 1) * sizeof(float2);
+    const size_t s2 = CK * ZC * (G + 1) * sizeof(float2);
+    const size_t s3 = ZC * (N + 1) * sizeof(float2);
+    const float a = (float)(PI_REF * PI_REF / h->mu);
+    const float pre = (float)(PI_REF / std::fabs(h->mu)) / (float)N;
+    const int ntiles = (G / h->TS) * (G / h->TS);
+    for (int z0 = 0; z0 < h->nz; z0 += ZC) {
+        k_adj_lines<N><<<h->ntheta, ZC * 32, s3, st>>>(g, h->lines, h->nz, z0, pre, h->tw_N);
+        PT_LAUNCHED("k_adj_lines");
+        if (h->TS == 16)
+            k_adj_scatter<M, 16><<<ntiles, 256, 0, st>>>(h->lines, h->fgrid, h->tile_off, h->tile_pts, h->fxy,
+                                                        h->x, h->y, N, a);
+        else
+            k_adj_scatter<M, 8><<<ntiles, 64, 0, st>>>(h->lines, h->fgrid, h->tile_off, h->tile_pts, h->fxy,
+                                                      h->x, h->y, N, a);
+        PT_LAUNCHED("k_adj_scatter");
+        k_adj_cols<G><<<G / CK, CK * ZC * T, s2, st>>>(h->fgrid, h->rbuf, h->tw_G);
+        PT_LAUNCHED("k_adj_cols");
+        k_adj_rows<G><<<n, ZC * T, s1, st>>>(h->rbuf, f, h->nz, z0, h->mu, scale, h->tw_G);
+        PT_LAUNCHED("k_adj_rows");
+    }
+    return PT_OK;
+}
+
+// Compiled grid sizes 2N = 3n (n = 8, 16, 32, 64, 128, 256, 512).
+#define PT_RADON_GRIDS(X) X(24) X(48) X(96) X(192) X(384) X(768) X(1536)
+
+bool grid_supported(int G)
+{
+#define PT_CASE(GG) \
+    if (G == GG) return true;
+    PT_RADON_GRIDS(PT_CASE)
+#undef PT_CASE
+    return false;
+}
+
+int radon_set_attrs(int G)
+{
+#define PT_CASE(GG) \
+    if (G == GG) return set_attrs<GG>();
+    PT_RADON_GRIDS(PT_CASE)
+#undef PT_CASE
+    pt::set_error("radonusfft: unsupported grid size %d", G);
+    return PT_ERR_UNSUPPORTED;
+}
+
+int radon_dispatch(pt_radon *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st)
+{
+#define PT_CASE(GG)                                                                 \
+    if (h->G == GG) {                                                               \
+        if (h->M == 7) return adj ? run_adj<GG, 7>(h, out, in, scale, st)           \
+                                  : run_fwd<GG, 7>(h, out, in, scale, st);          \
+        if (h->M == 4) return adj ? run_adj<GG, 4>(h, out, in, scale, st)           \
+                                  : run_fwd<GG, 4>(h, out, in, scale, st);          \
+    }
+    PT_RADON_GRIDS(PT_CASE)
+#undef PT_CASE
+    pt::set_error("radonusfft: no kernel for grid %d with half-width M=%d", h->G, h->M);
+    return PT_ERR_UNSUPPORTED;
+}
+
+template <typename T>
+int dmalloc(T **p, size_t count)
+{
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T) + 16);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        pt::set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        return PT_ERR_ALLOC;
+    }
+    return PT_OK;
+}
+
+int check_device(const pt_radon *h)
+{
+    int dev = -1;
+    PT_CUDA(cudaGetDevice(&dev));
+    if (dev != h->device) {
+        pt::set_error("radonusfft handle belongs to device %d, current device is %d", h->device, dev);
+        return PT_ERR_ARG;
+    }
+    return PT_OK;
+}
+
+}  // namespace
+
+extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_override, pt_radon **out)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(out != nullptr, "radonusfft: null output handle");
+    *out = nullptr;
+    PT_CHECK_ARG(ntheta >= 1 && ntheta <= (1u << 20), "radonusfft: bad Ntheta %zu", ntheta);
+    PT_CHECK_ARG(nz >= 1 && nz <= (1u << 20), "radonusfft: bad Nz %zu", nz);
+    PT_CHECK_ARG(n >= 8 && n % 8 == 0, "radonusfft: n=%zu must be a positive multiple of 8", n);
+    PT_CHECK_ARG(m_override == 0 || m_override == 4 || m_override == 7,
+                 "radonusfft: kernel half-width override %d not compiled (0, 4 or 7)", m_override);
+    const int G = (int)(3 * n);
+    if (!grid_supported(G)) {
+        pt::set_error("radonusfft: n=%zu not compiled (supported n: 8,16,32,64,128,256,512)", n);
+        return PT_ERR_UNSUPPORTED;
+    }
+    pt_radon *h = new pt_radon();
+    h->ntheta = (int)ntheta;
+    h->nz = (int)nz;
+    h->n = (int)n;
+    radon_params((int)n, m_override, &h->N, &h->M, &h->mu);
+    h->G = G;
+    h->TS = (G % 16 == 0) ? 16 : 8;
+    if (cudaGetDevice(&h->device) != cudaSuccess) {
+        delete h;
+        pt::set_error("radonusfft: no CUDA device");
+        return PT_ERR_CUDA;
+    }
+    if (h->M != 7 && h->M != 4) {
+        pt::set_error("radonusfft: reference half-width M=%d has no compiled kernel", h->M);
+        delete h;
+        return PT_ERR_UNSUPPORTED;
+    }
+    int rc = PT_OK;
+    const size_t N = h->N;
+    if (rc == PT_OK) rc = dmalloc(&h->tw_G, (size_t)G);
+    if (rc == PT_OK) rc = dmalloc(&h->tw_N, N);
+    if (rc == PT_OK) rc = dmalloc(&h->theta, ntheta);
+    if (rc == PT_OK) rc = dmalloc(&h->x, ntheta * N);
+    if (rc == PT_OK) rc = dmalloc(&h->y, ntheta * N);
+    if (rc == PT_OK) rc = dmalloc(&h->fxy, 2 * ntheta * N);
+    if (rc == PT_OK) rc = dmalloc(&h->rbuf, N * G * ZC);
+    if (rc == PT_OK) rc = dmalloc(&h->fgrid, (size_t)G * G * ZC);
+    if (rc == PT_OK) rc = dmalloc(&h->lines, ntheta * N * ZC);
+    if (rc == PT_OK) rc = dmalloc(&h->tile_off, (size_t)(G / h->TS) * (G / h->TS) + 1);
+    if (rc == PT_OK) rc = radon_set_attrs(G);
+    if (rc == PT_OK) {
+        std::vector<float2> tw(G);
+        pt_make_twiddles(tw.data(), G);
+        if (cudaMemcpy(h->tw_G, tw.data(), G * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = PT_ERR_CUDA;
+        pt_make_twiddles(tw.data(), (int)N);
+        if (rc == PT_OK &&
+            cudaMemcpy(h->tw_N, tw.data(), N * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = PT_ERR_CUDA;
+        if (rc != PT_OK) pt::set_error("radonusfft: twiddle upload failed");
+    }
+    if (rc != PT_OK) {
+        radon_free(h);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return PT_OK;
+}
+
+extern "C" int pt_radon_create(size_t ntheta, size_t nz, size_t n, pt_radon **out)
+{
+    return pt_radon_create_ex(ntheta, nz, n, 0, out);
+}
+
+extern "C" int pt_radon_destroy(pt_radon *h)
+{
+    pt::clear_error();
+    if (!h) return PT_OK;
+    radon_free(h);
+    delete h;
+    return PT_OK;
+}
+
+extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h != nullptr, "radonusfft.setobj: null handle");
+    PT_CHECK_ARG(theta != nullptr, "radonusfft.setobj: null theta");
+    int rc = check_device(h);
+    if (rc != PT_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    h->ready = false;
+    const int N = h->N, G = h->G, M = h->M, W = 2 * M + 1, TS = h->TS, ntheta = h->ntheta;
+    PT_CUDA(cudaMemcpyAsync(h->theta, theta, ntheta * sizeof(float), cudaMemcpyDefault, st));
+    k_takexy<<<dim3((N + 127) / 128, ntheta), 128, 0, st>>>(h->x, h->y, h->theta, N, ntheta);
+    PT_LAUNCHED("k_takexy");
+    const size_t npts = (size_t)ntheta * N;
+    std::vector<float> xs(npts), ys(npts);
+    PT_CUDA(cudaMemcpyAsync(xs.data(), h->x, npts * sizeof(float), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaMemcpyAsync(ys.data(), h->y, npts * sizeof(float), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaStreamSynchronize(st));
+    // window corners floor(2N x) exactly as kernels.cuh:112-115 (float product)
+    std::vector<int> fxy(2 * npts);
+    for (size_t p = 0; p < npts; ++p) {
+        if (!(xs[p] >= -0.5f && xs[p] < 0.5f && ys[p] >= -0.5f && ys[p] < 0.5f)) {
+            pt::set_error("radonusfft.setobj: theta[%zu] is not a finite angle", p / N);
+            h->ready = false;
+            return PT_ERR_ARG;
+        }
+        fxy[2 * p] = (int)floorf((float)G * xs[p]);
+        fxy[2 * p + 1] = (int)floorf((float)G * ys[p]);
+    }
+    // CSR of tile -> points whose window [o, o+W) (mod G) touches the tile
+    const int nt = G / TS, ntiles = nt * nt;
+    std::vector<int> cnt(ntiles + 1, 0);
+    auto tiles_of = [&](int o, int *list) {
+        int k = 0;
+        for (int i = 0; i < W; ++i) {
+            const int t = ((o + i) % G) / TS;
+            bool seen = false;
+            for (int j = 0; j < k; ++j) seen |= (list[j] == t);
+            if (!seen) list[k++] = t;
+        }
+        return k;
+    };
+    int lx[32], ly[32];
+    for (int pass = 0; pass < 2; ++pass) {
+        std::vector<int> pos;
+        if (pass == 1) {
+            for (int t = 0; t < ntiles; ++t) cnt[t + 1] += cnt[t];
+            pos.assign(cnt.begin(), cnt.end() - 1);
+        }
+        std::vector<int> pts;
+        if (pass == 1) pts.resize(cnt[ntiles]);
+        for (size_t p = 0; p < npts; ++p) {
+            const int ox = ((N + fxy[2 * p] - M) % G + G) % G;
+            const int oy = ((N + fxy[2 * p + 1] - M) % G + G) % G;
+            const int kx = tiles_of(ox, lx), ky = tiles_of(oy, ly);
+            for (int j = 0; j < ky; ++j)
+                for (int i = 0; i < kx; ++i) {
+                    const int t = ly[j] * nt + lx[i];
+                    if (pass == 0)
+                        cnt[t + 1]++;
+                    else
+                        pts[pos[t]++] = (int)p;
+                }
+        }
+        if (pass == 1) {
+            const size_t need = pts.size();
+            if (need > h->tile_pts_cap) {
+                if (h->tile_pts) cudaFree(h->tile_pts);
+                h->tile_pts = nullptr;
+                h->tile_pts_cap = 0;
+                rc = dmalloc(&h->tile_pts, need);
+                if (rc != PT_OK) return rc;
+                h->tile_pts_cap = need;
+            }
+            PT_CUDA(cudaMemcpy(h->tile_pts, pts.data(), need * sizeof(int), cudaMemcpyHostToDevice));
+            PT_CUDA(cudaMemcpy(h->tile_off, cnt.data(), (ntiles + 1) * sizeof(int), cudaMemcpyHostToDevice));
+        }
+    }
+    PT_CUDA(cudaMemcpy(h->fxy, fxy.data(), 2 * npts * sizeof(int), cudaMemcpyHostToDevice));
+    h->ready = true;
+    return PT_OK;
+}
+
+namespace {
+int radon_call(pt_radon *h, bool adj, void *out, const void *in, float scale, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h != nullptr, "radonusfft: null handle");
+    PT_CHECK_ARG(out != nullptr && in != nullptr, "radonusfft.%s: null array pointer", adj ? "adj" : "fwd");
+    if (!h->ready) {
+        pt::set_error("radonusfft.%s: setobj(theta) has not been called", adj ? "adj" : "fwd");
+        return PT_ERR_STATE;
+    }
+    int rc = check_device(h);
+    if (rc != PT_OK) return rc;
+    return radon_dispatch(h, adj, (float2 *)out, (const float2 *)in, scale, (cudaStream_t)stream);
+}
+}  // namespace
+
+extern "C" int pt_radon_fwd(pt_radon *h, void *g, const void *f, void *stream)
+{
+    return radon_call(h, false, g, f, 1.0f, stream);
+}
+extern "C" int pt_radon_adj(pt_radon *h, void *f, const void *g, void *stream)
+{
+    return radon_call(h, true, f, g, 1.0f, stream);
+}
+extern "C" int pt_radon_fwd_scaled(pt_radon *h, void *g, const void *f, float scale, void *stream)
+{
+    return radon_call(h, false, g, f, scale, stream);
+}
+extern "C" int pt_radon_adj_scaled(pt_radon *h, void *f, const void *g, float scale, void *stream)
+{
+    return radon_call(h, true, f, g, scale, stream);
+}
+
+extern "C" int pt_radon_get_params(const pt_radon *h, int *N, int *M, float *mu)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h != nullptr, "radonusfft: null handle");
+    if (N) *N = h->N;
+    if (M) *M = h->M;
+    if (mu) *mu = h->mu;
+    return PT_OK;
+}
+
+extern "C" int pt_radon_get_xy(const pt_radon *h, float *x, float *y, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h != nullptr, "radonusfft: null handle");
+    if (!h->ready) {
+        pt::set_error("radonusfft.get_xy: setobj(theta) has not been called");
+        return PT_ERR_STATE;
+    }
+    const size_t bytes = (size_t)h->ntheta * h->N * sizeof(float);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (x) PT_CUDA(cudaMemcpyAsync(x, h->x, bytes, cudaMemcpyDefault, st));
+    if (y) PT_CUDA(cudaMemcpyAsync(y, h->y, bytes, cudaMemcpyDefault, st));
+    return PT_OK;
+}

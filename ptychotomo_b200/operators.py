@@ -1,0 +1,115 @@
+"""Drop-in Python classes ``radonusfft`` and ``ptychofft``.
+
+Same constructor arguments and methods as the reference's SWIG classes
+(src/cuda/radonusfft.i:15-46, src/cuda/ptychofft.i:14-48): arrays are
+passed as device addresses (ints, as CuPy's ``.data.ptr``), or as CUDA
+tensors for convenience.  Work is queued on the caller's current torch
+stream (or on ``stream=`` when given).  Failures raise
+:class:`~ptychotomo_b200._lib.PtychotomoError` instead of silently
+producing garbage.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from ._lib import as_ptr, check, current_stream, lib
+
+
+class radonusfft:  # noqa: N801 - reference class name
+    """USFFT Radon transform; ``radonusfft(Ntheta, Nz, N)`` as radonusfft.cu:5."""
+
+    def __init__(self, Ntheta, Nz, N, m_override: int = 0):
+        h = ctypes.c_void_p()
+        check(lib().pt_radon_create_ex(int(Ntheta), int(Nz), int(N), int(m_override), ctypes.byref(h)),
+              "radonusfft create")
+        self._h = h
+        self.Ntheta, self.Nz, self.n = int(Ntheta), int(Nz), int(N)
+        Np, M, mu = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        check(lib().pt_radon_get_params(h, ctypes.byref(Np), ctypes.byref(M), ctypes.byref(mu)))
+        self.N, self.M, self.mu = Np.value, M.value, mu.value
+
+    def setobj(self, theta, stream=None):
+        """radonusfft::setobj(theta), radonusfft.cu:141."""
+        check(lib().pt_radon_setobj(self._h, as_ptr(theta), _s(stream)), "radonusfft.setobj")
+
+    def fwd(self, g, f, stream=None, scale: float | None = None):
+        """radonusfft::fwd(g, f), radonusfft.cu:54: g[Ntheta,Nz,n] = R f[Nz,n,n]."""
+        if scale is None:
+            check(lib().pt_radon_fwd(self._h, as_ptr(g), as_ptr(f), _s(stream)), "radonusfft.fwd")
+        else:
+            check(lib().pt_radon_fwd_scaled(self._h, as_ptr(g), as_ptr(f), float(scale), _s(stream)),
+                  "radonusfft.fwd")
+
+    def adj(self, f, g, stream=None, scale: float | None = None):
+        """radonusfft::adj(f, g), radonusfft.cu:94: f[Nz,n,n] = R* g[Ntheta,Nz,n]."""
+        if scale is None:
+            check(lib().pt_radon_adj(self._h, as_ptr(f), as_ptr(g), _s(stream)), "radonusfft.adj")
+        else:
+            check(lib().pt_radon_adj_scaled(self._h, as_ptr(f), as_ptr(g), float(scale), _s(stream)),
+                  "radonusfft.adj")
+
+    def get_xy(self, x, y, stream=None):
+        """Copy the polar coordinate tables (each float32 [Ntheta, N])."""
+        check(lib().pt_radon_get_xy(self._h, as_ptr(x), as_ptr(y), _s(stream)), "radonusfft.get_xy")
+
+    def free(self):
+        if getattr(self, "_h", None):
+            lib().pt_radon_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:  # interpreter shutdown
+            pass
+
+
+class ptychofft:  # noqa: N801 - reference class name
+    """Ptychography operator; ``ptychofft(Ntheta, Nz, N, Ntheta0, Nscan, detx, dety, Nprb)``."""
+
+    def __init__(self, Ntheta, Nz, N, Ntheta0, Nscan, detx, dety, Nprb):
+        h = ctypes.c_void_p()
+        check(lib().pt_ptycho_create(int(Ntheta), int(Nz), int(N), int(Ntheta0), int(Nscan), int(detx),
+                                     int(dety), int(Nprb), ctypes.byref(h)), "ptychofft create")
+        self._h = h
+        self.Ntheta, self.Nz, self.N = int(Ntheta), int(Nz), int(N)
+        self.Nscan, self.detx, self.dety, self.Nprb = int(Nscan), int(detx), int(dety), int(Nprb)
+
+    def setobj(self, scan, prb, stream=None):
+        """ptychofft::setobj(scan, prb), ptychofft.cu:48."""
+        check(lib().pt_ptycho_setobj(self._h, as_ptr(scan), as_ptr(prb), _s(stream)), "ptychofft.setobj")
+
+    def fwd(self, g, f, stream=None, scale: float | None = None):
+        """ptychofft::fwd(g, f), ptychofft.cu:58."""
+        if scale is None:
+            check(lib().pt_ptycho_fwd(self._h, as_ptr(g), as_ptr(f), _s(stream)), "ptychofft.fwd")
+        else:
+            check(lib().pt_ptycho_fwd_scaled(self._h, as_ptr(g), as_ptr(f), float(scale), _s(stream)),
+                  "ptychofft.fwd")
+
+    def adj(self, f, g, stream=None, scale: float | None = None):
+        """ptychofft::adj(f, g), ptychofft.cu:78."""
+        if scale is None:
+            check(lib().pt_ptycho_adj(self._h, as_ptr(f), as_ptr(g), _s(stream)), "ptychofft.adj")
+        else:
+            check(lib().pt_ptycho_adj_scaled(self._h, as_ptr(f), as_ptr(g), float(scale), _s(stream)),
+                  "ptychofft.adj")
+
+    def free(self):
+        if getattr(self, "_h", None):
+            lib().pt_ptycho_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _s(stream):
+    if stream is None:
+        return current_stream()
+    if hasattr(stream, "cuda_stream"):
+        return stream.cuda_stream
+    return int(stream)

@@ -1,0 +1,223 @@
+"""GPU parity of the radonusfft / ptychofft operators.
+
+Compared with (1) the NumPy oracle on the same seeded inputs and the same
+polar coordinate tables, (2) the reference's own CUDA operators
+(oracle/_ref) when built, (3) the adjoint identity <A x, y> = <x, A* y>, and
+(4) run-to-run bitwise determinism.  Tolerance: relative L2 <= 1e-5 for
+fwd/adj (the float32 operators against complex128 / float32 references).
+"""
+import numpy as np
+import pytest
+
+import refcuda
+from oracle.ptycho import PtychoFFT
+from oracle.usfft import RadonUSFFT, takexy
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def crand(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def make_radon(n, nz, ntheta, theta, m_override=0):
+    from ptychotomo_b200 import radonusfft
+    op = radonusfft(ntheta, nz, n, m_override=m_override)
+    op.setobj(dev(theta))
+    x = torch.empty((ntheta, op.N), dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    op.get_xy(x, y)
+    torch.cuda.synchronize()
+    orc = RadonUSFFT(ntheta, nz, n)
+    orc.setobj(theta, xy=(x.cpu().numpy(), y.cpu().numpy()))
+    return op, orc
+
+
+def radon_fwd(op, f):
+    g = torch.zeros((op.Ntheta, op.Nz, op.n), dtype=torch.complex64, device="cuda")
+    op.fwd(g, f)
+    return g
+
+
+def radon_adj(op, g):
+    f = torch.zeros((op.Nz, op.n, op.n), dtype=torch.complex64, device="cuda")
+    op.adj(f, g)
+    return f
+
+
+RADON_SIZES = [(16, 5, 12), (32, 8, 24), (32, 11, 17), (64, 3, 40), (128, 9, 128)]
+
+
+@pytest.mark.parametrize("n,nz,ntheta", RADON_SIZES)
+def test_radon_fwd_adj_vs_oracle(n, nz, ntheta):
+    rng = np.random.default_rng(n + nz)
+    theta = np.sort(rng.uniform(0, np.pi, ntheta)).astype(np.float32)
+    op, orc = make_radon(n, nz, ntheta, theta)
+    f = crand(rng, (nz, n, n))
+    g = crand(rng, (ntheta, nz, n))
+    gf = radon_fwd(op, dev(f)).cpu().numpy()
+    fa = radon_adj(op, dev(g)).cpu().numpy()
+    assert rel(gf, orc.fwd(f)) <= TOL
+    assert rel(fa, orc.adj(g)) <= TOL
+
+
+def test_radon_polar_tables_match_exact_geometry():
+    """Device tables use the reference's __cosf/__sinf; they must lie within
+    the documented intrinsic error (|err| <= 2^-21.41 on [-pi, pi]) scaled
+    by |k-N/2|/N <= 1/2 of float32 cos/sin tables."""
+    n, ntheta = 64, 90
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype(np.float32)
+    op, orc = make_radon(n, 2, ntheta, theta)
+    xe, ye = takexy(theta, op.N)
+    assert np.max(np.abs(orc.x - xe)) <= 0.5 * 2 ** -21.41 + 1e-7
+    assert np.max(np.abs(orc.y - ye)) <= 0.5 * 2 ** -21.41 + 1e-7
+
+
+def test_radon_adjoint_identity():
+    n, nz, ntheta = 64, 10, 48
+    rng = np.random.default_rng(3)
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype(np.float32)
+    op, _ = make_radon(n, nz, ntheta, theta)
+    f = crand(rng, (nz, n, n))
+    f[:, 0, :] = f[:, -1, :] = f[:, :, 0] = f[:, :, -1] = 0   # border-zero (pad2 vs crop)
+    g = crand(rng, (ntheta, nz, n))
+    g[:, :, 0] = g[:, :, -1] = 0
+    a = np.vdot(radon_fwd(op, dev(f)).cpu().numpy().astype(np.complex128), g.astype(np.complex128))
+    b = np.vdot(f.astype(np.complex128), radon_adj(op, dev(g)).cpu().numpy().astype(np.complex128))
+    assert abs(a - b) / abs(a) <= TOL
+
+
+def test_radon_deterministic():
+    n, nz, ntheta = 64, 8, 64
+    rng = np.random.default_rng(4)
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype(np.float32)
+    op, _ = make_radon(n, nz, ntheta, theta)
+    g = dev(crand(rng, (ntheta, nz, n)))
+    f = dev(crand(rng, (nz, n, n)))
+    assert torch.equal(radon_adj(op, g), radon_adj(op, g))
+    assert torch.equal(radon_fwd(op, f), radon_fwd(op, f))
+
+
+def test_radon_scaled_entry_points():
+    n, nz, ntheta = 32, 4, 16
+    rng = np.random.default_rng(5)
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype(np.float32)
+    op, _ = make_radon(n, nz, ntheta, theta)
+    f = dev(crand(rng, (nz, n, n)))
+    g = torch.zeros((ntheta, nz, n), dtype=torch.complex64, device="cuda")
+    op.fwd(g, f, scale=0.25)
+    assert rel(g.cpu().numpy(), 0.25 * radon_fwd(op, f).cpu().numpy()) <= 1e-6
+
+
+@pytest.mark.skipif(not refcuda.available(), reason="reference CUDA operators not built (make -C oracle)")
+@pytest.mark.parametrize("n,nz,ntheta", [(32, 8, 24), (128, 16, 128)])
+def test_radon_vs_reference_cuda(n, nz, ntheta):
+    rng = np.random.default_rng(7)
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype(np.float32)
+    th = dev(theta)
+    op, _ = make_radon(n, nz, ntheta, theta)
+    f = dev(crand(rng, (nz, n, n)))
+    g = dev(crand(rng, (ntheta, nz, n)))
+    ref = refcuda.RefRadon(ntheta, nz, n)
+    ref.setobj(th.data_ptr())
+    gr = torch.zeros((ntheta, nz, n), dtype=torch.complex64, device="cuda")
+    fr = torch.zeros((nz, n, n), dtype=torch.complex64, device="cuda")
+    ref.fwd(gr.data_ptr(), f.data_ptr())
+    ref.adj(fr.data_ptr(), g.data_ptr())
+    ref.free()
+    assert rel(radon_fwd(op, f).cpu().numpy(), gr.cpu().numpy()) <= TOL
+    assert rel(radon_adj(op, g).cpu().numpy(), fr.cpu().numpy()) <= TOL
+
+
+# ---------------------------------------------------------------------------
+# ptychography
+# ---------------------------------------------------------------------------
+def make_ptycho(ntheta, nz, n, nscan, det, nprb, rng, sentinel=True):
+    from ptychotomo_b200 import ptychofft
+    scan = np.empty((2, ntheta, nscan), np.float32)
+    scan[0] = rng.uniform(0, n - nprb - 0.5, (ntheta, nscan))
+    scan[1] = rng.uniform(0, nz - nprb - 0.5, (ntheta, nscan))
+    if sentinel:
+        scan[:, 0, 1] = -1
+    prb = crand(rng, (nprb, nprb))
+    op = ptychofft(ntheta, nz, n, ntheta, nscan, det, det, nprb)
+    op.setobj(dev(scan), dev(prb))
+    orc = PtychoFFT(ntheta, nz, n, ntheta, nscan, det, det, nprb)
+    orc.setobj(scan, prb)
+    return op, orc, scan, prb
+
+
+def p_fwd(op, f):
+    g = torch.zeros((op.Ntheta, op.Nscan, op.detx, op.dety), dtype=torch.complex64, device="cuda")
+    op.fwd(g, f)
+    return g
+
+
+def p_adj(op, g):
+    f = torch.zeros((op.Ntheta, op.Nz, op.N), dtype=torch.complex64, device="cuda")
+    op.adj(f, g)
+    return f
+
+
+PTYCHO_SIZES = [(3, 32, 32, 7, 16, 16), (2, 24, 40, 5, 32, 16), (2, 64, 64, 9, 64, 64),
+                (2, 130, 140, 6, 128, 128), (4, 20, 20, 3, 8, 8)]
+
+
+@pytest.mark.parametrize("ntheta,nz,n,nscan,det,nprb", PTYCHO_SIZES)
+def test_ptycho_fwd_adj_vs_oracle(ntheta, nz, n, nscan, det, nprb):
+    rng = np.random.default_rng(det + nscan)
+    op, orc, _, _ = make_ptycho(ntheta, nz, n, nscan, det, nprb, rng)
+    f = crand(rng, (ntheta, nz, n))
+    g = crand(rng, (ntheta, nscan, det, det))
+    assert rel(p_fwd(op, dev(f)).cpu().numpy(), orc.fwd(f)) <= TOL
+    assert rel(p_adj(op, dev(g)).cpu().numpy(), orc.adj(g)) <= TOL
+
+
+def test_ptycho_adjoint_identity_and_determinism():
+    rng = np.random.default_rng(11)
+    op, _, _, _ = make_ptycho(3, 64, 64, 12, 64, 32, rng)
+    f = dev(crand(rng, (3, 64, 64)))
+    g = dev(crand(rng, (3, 12, 64, 64)))
+    a = torch.vdot(p_fwd(op, f).flatten().cdouble(), g.flatten().cdouble()).item()
+    b = torch.vdot(f.flatten().cdouble(), p_adj(op, g).flatten().cdouble()).item()
+    assert abs(a - b) / abs(a) <= TOL
+    assert torch.equal(p_adj(op, g), p_adj(op, g))
+
+
+def test_ptycho_rejects_out_of_object_scan():
+    from ptychotomo_b200 import PtychotomoArgError, ptychofft
+    op = ptychofft(1, 32, 32, 1, 2, 16, 16, 16)
+    scan = dev(np.array([[[0.0, 17.0]], [[0.0, 0.0]]], np.float32))
+    with pytest.raises(PtychotomoArgError):
+        op.setobj(scan, dev(np.ones((16, 16), np.complex64)))
+
+
+@pytest.mark.skipif(not refcuda.available(), reason="reference CUDA operators not built (make -C oracle)")
+@pytest.mark.parametrize("ntheta,nz,n,nscan,det,nprb", [(3, 48, 48, 9, 32, 32), (2, 64, 64, 6, 64, 16)])
+def test_ptycho_vs_reference_cuda(ntheta, nz, n, nscan, det, nprb):
+    rng = np.random.default_rng(13)
+    op, _, scan, prb = make_ptycho(ntheta, nz, n, nscan, det, nprb, rng)
+    f = dev(crand(rng, (ntheta, nz, n)))
+    g = dev(crand(rng, (ntheta, nscan, det, det)))
+    sc, pr = dev(scan), dev(prb)
+    ref = refcuda.RefPtycho(ntheta, nz, n, nscan, det, nprb)
+    ref.setobj(sc.data_ptr(), pr.data_ptr())
+    gr = torch.zeros((ntheta, nscan, det, det), dtype=torch.complex64, device="cuda")
+    fr = torch.zeros((ntheta, nz, n), dtype=torch.complex64, device="cuda")
+    ref.fwd(gr.data_ptr(), f.data_ptr())
+    ref.adj(fr.data_ptr(), g.data_ptr())
+    ref.free()
+    assert rel(p_fwd(op, f).cpu().numpy(), gr.cpu().numpy()) <= TOL
+    assert rel(p_adj(op, g).cpu().numpy(), fr.cpu().numpy()) <= TOL
