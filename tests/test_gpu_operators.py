@@ -147,8 +147,8 @@ def test_radon_vs_reference_cuda(n, nz, ntheta):
 def make_ptycho(ntheta, nz, n, nscan, det, nprb, rng, sentinel=True):
     from ptychotomo_b200 import ptychofft
     scan = np.empty((2, ntheta, nscan), np.float32)
-    scan[0] = rng.uniform(0, n - nprb - 0.5, (ntheta, nscan))
-    scan[1] = rng.uniform(0, nz - nprb - 0.5, (ntheta, nscan))
+    scan[0] = rng.uniform(0, max(n - nprb - 0.5, 0), (ntheta, nscan))
+    scan[1] = rng.uniform(0, max(nz - nprb - 0.5, 0), (ntheta, nscan))
     if sentinel:
         scan[:, 0, 1] = -1
     prb = crand(rng, (nprb, nprb))
