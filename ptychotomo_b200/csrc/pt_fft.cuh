@@ -109,6 +109,46 @@ struct Dft<8, DIR> {
     }
 };
 
+// 16-point DFT as 4 x 4 (n = 4 n1 + n2, k = k1 + 4 k2), natural-order output.
+template <int DIR>
+struct Dft<16, DIR> {
+    static __device__ __forceinline__ void run(float2 *v)
+    {
+        const float c1 = 0.92387953251128675613f;  // cos(pi/8)
+        const float s1 = 0.38268343236508977173f;  // sin(pi/8)
+        const float h = 0.70710678118654752440f;
+        const float d = (float)DIR;
+        float2 a[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+            a[n2][0] = v[n2];
+            a[n2][1] = v[4 + n2];
+            a[n2][2] = v[8 + n2];
+            a[n2][3] = v[12 + n2];
+            dft4<DIR>(a[n2][0], a[n2][1], a[n2][2], a[n2][3]);
+        }
+        // a[n2][k1] *= W16^(n2 k1), W16 = exp(DIR 2 pi i / 16)
+        a[1][1] = cmul(a[1][1], make_float2(c1, d * s1));
+        a[1][2] = cmul(a[1][2], make_float2(h, d * h));
+        a[1][3] = cmul(a[1][3], make_float2(s1, d * c1));
+        a[2][1] = cmul(a[2][1], make_float2(h, d * h));
+        a[2][2] = mul_i<DIR>(a[2][2]);
+        a[2][3] = cmul(a[2][3], make_float2(-h, d * h));
+        a[3][1] = cmul(a[3][1], make_float2(s1, d * c1));
+        a[3][2] = cmul(a[3][2], make_float2(-h, d * h));
+        a[3][3] = cmul(a[3][3], make_float2(-c1, -d * s1));
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            float2 b0 = a[0][k1], b1 = a[1][k1], b2 = a[2][k1], b3 = a[3][k1];
+            dft4<DIR>(b0, b1, b2, b3);
+            v[k1] = b0;
+            v[k1 + 4] = b1;
+            v[k1 + 8] = b2;
+            v[k1 + 12] = b3;
+        }
+    }
+};
+
 // One Stockham pass, in place in shared memory.  `buf` is this FFT's base,
 // `es` the element stride, `t` the thread's index among the T threads that
 // share this FFT.  All threads of the block must call it (it synchronises).

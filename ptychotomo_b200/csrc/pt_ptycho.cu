@@ -4,15 +4,20 @@
 // kernels mul/mula/takeshifts/shifts/shiftsa in src/include/kernels.cuh).
 //
 //  forward  g = F Q psi   (ptychofft.cu:58-76): one block per frame
-//    (angle, scan).  The probe-weighted patch is written transposed into a
-//    det x det shared-memory frame (detector row = object column,
-//    kernels.cuh:257-263), the 2-D FFT runs in shared memory and the
-//    constant per-scan phase (kernels.cuh:306-336) is applied on the way
-//    out.  No zero-filled frame buffer, no device-to-device copies.
-//  adjoint  psi = Q* F* g (ptychofft.cu:78-93): one block per angle walks its
-//    scans in order: conjugate phase, inverse 2-D FFT in shared memory,
-//    conj(probe) and accumulation into that angle's object slab.  Only this
-//    block writes the slab, so the sum is deterministic and needs no atomics.
+//    (angle, scan).  Each 1-D DFT of length det is a four-step factorisation
+//    det = N1 x N2: N1 points per thread in registers, N2 threads per line,
+//    one swizzled shared-memory exchange inside the group.  The probe-weighted
+//    patch (detector row = object column, kernels.cuh:257-263) is loaded
+//    straight into registers, transformed along the object row, transposed
+//    once through shared memory, transformed along the other axis and written
+//    with the per-scan phase (kernels.cuh:306-336) applied.
+//  adjoint  psi = Q* F* g (ptychofft.cu:78-93): the same transform in reverse;
+//    block (part, angle) walks scans s = part, part + parts, ... in order and
+//    accumulates conj(probe) x frame into its own slab; with parts > 1 the
+//    slabs are summed in a fixed order by a second kernel.  Deterministic,
+//    no atomics.
+//  Detector 8x8 uses a plain shared-memory Stockham path.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -48,7 +53,7 @@ __global__ void k_ptycho_tables(const float *__restrict__ scan, int *__restrict_
 
 template <int DET>
 __global__ void __launch_bounds__(ptycho_block<DET>(), 1)
-    k_ptycho_fwd(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
+    k_ptycho_fwd_small(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
                  const float2 *__restrict__ phase, const float2 *__restrict__ prb, int nz, int n, int nscan,
                  int P, float c, float scale, const float2 *__restrict__ tw)
 {
@@ -84,7 +89,7 @@ __global__ void __launch_bounds__(ptycho_block<DET>(), 1)
 
 template <int DET>
 __global__ void __launch_bounds__(ptycho_block<DET>(), 1)
-    k_ptycho_adj(const float2 *__restrict__ g, float2 *__restrict__ psi, const int *__restrict__ corner,
+    k_ptycho_adj_small(const float2 *__restrict__ g, float2 *__restrict__ psi, const int *__restrict__ corner,
                  const float2 *__restrict__ phase, const float2 *__restrict__ prb, int nz, int n, int nscan,
                  int P, float c, float scale, const float2 *__restrict__ tw)
 {
@@ -118,14 +123,235 @@ __global__ void __launch_bounds__(ptycho_block<DET>(), 1)
     }
 }
 
+
+// ---- register four-step transforms (det >= 16) -----------------------------
+template <int DET>
+struct PF {
+    static constexpr int N2 = DET >= 64 ? 8 : 4;           // threads per line
+    static constexpr int N1 = DET / N2;                    // points per thread
+    static constexpr int KPT = N1 / N2;                    // k1 values per thread after the exchange
+    static constexpr int NT = DET * N2 < 512 ? DET * N2 : 512;  // threads per block
+    static constexpr int NG = NT / N2;                     // thread groups
+    static constexpr int CPG = DET / NG;                   // lines per group
+    static constexpr int P = DET + 8;                      // frame pitch (P = 8 mod 16)
+    static constexpr size_t SMEM = (size_t)(DET * P + DET) * sizeof(float2);
+};
+
+// frame swizzle: row r, column c live at r * P + (c ^ fswz(r))
+template <int DET>
+__device__ __forceinline__ int fswz(int r)
+{
+    return ((r / PF<DET>::KPT) % PF<DET>::N2) * 2;
+}
+
+// DFT of one line held as v[m] = x[t + N2 m] by the N2 threads t of a group.
+// On return v[j N2 + k2] = X[t KPT + j + N1 k2].  `sc` is the group's
+// scratch (DET + 1 complex), `tws` the table exp(-2 pi i m / DET).
+template <int DET, int DIR>
+__device__ __forceinline__ void line_dft(float2 (&v)[PF<DET>::N1], int t, float2 *sc, const float2 *tws)
+{
+    using F = PF<DET>;
+    ptfft::Dft<F::N1, DIR>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < F::N1; ++k1) {
+        float2 w = tws[t * k1];
+        if (DIR > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < F::N1; ++k1) sc[t * F::N1 + ((k1 + t * F::KPT) % F::N1)] = v[k1];
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < F::KPT; ++j) {
+        float2 u[F::N2];
+        const int k1 = t * F::KPT + j;
+#pragma unroll
+        for (int n2 = 0; n2 < F::N2; ++n2) u[n2] = sc[n2 * F::N1 + ((k1 + n2 * F::KPT) % F::N1)];
+        ptfft::Dft<F::N2, DIR>::run(u);
+#pragma unroll
+        for (int k2 = 0; k2 < F::N2; ++k2) v[j * F::N2 + k2] = u[k2];
+    }
+}
+
+template <int DET>
+__global__ void __launch_bounds__(PF<DET>::NT, 1)
+    k_ptycho_fwd(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
+                 const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
+                 int nframes, int P, float scale, const float2 *__restrict__ tw)
+{
+    using F = PF<DET>;
+    extern __shared__ float2 sm[];
+    float2 *fr = sm;
+    float2 *tws = sm + DET * F::P;
+    for (int i = threadIdx.x; i < DET; i += F::NT) tws[i] = tw[i];
+    const int t = threadIdx.x % F::N2, grp = threadIdx.x / F::N2;
+    float2 *sc = fr + grp * (DET + 1);
+    const int off = (DET - P) / 2;
+    __syncthreads();
+    for (int fid = blockIdx.x; fid < nframes; fid += gridDim.x) {
+        const int th = fid / nscan;
+        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
+        float2 *out = g + (size_t)fid * DET * DET;
+        if (stx < 0 || sty < 0) {  // skipped scan: the reference leaves a zero frame
+            for (int e = threadIdx.x; e < DET * DET; e += F::NT) out[e] = czero();
+            continue;
+        }
+        const float2 *src = psi + ((size_t)th * nz + sty) * n + stx;
+        float2 v[F::CPG][F::N1];
+        // along the object row: line = detector column iy, points ix = t + N2 m
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            const int py = grp + F::NG * c - off;
+#pragma unroll
+            for (int m = 0; m < F::N1; ++m) {
+                const int px = t + F::N2 * m - off;
+                float2 val = czero();
+                if (py >= 0 && py < P && px >= 0 && px < P)
+                    val = cmul(__ldg(&prbT[py * P + px]), __ldg(&src[(size_t)py * n + px]));
+                v[c][m] = val;
+            }
+            line_dft<DET, -1>(v[c], t, sc, tws);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            const int iy = grp + F::NG * c;
+#pragma unroll
+            for (int j = 0; j < F::KPT; ++j)
+#pragma unroll
+                for (int k2 = 0; k2 < F::N2; ++k2) {
+                    const int kx = t * F::KPT + j + F::N1 * k2;
+                    fr[kx * F::P + (iy ^ fswz<DET>(kx))] = v[c][j * F::N2 + k2];
+                }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            const int kx = grp + F::NG * c;
+            const int sw = fswz<DET>(kx);
+#pragma unroll
+            for (int m = 0; m < F::N1; ++m) v[c][m] = fr[kx * F::P + ((t + F::N2 * m) ^ sw)];
+        }
+        __syncthreads();
+        const float2 ph = scale * phase[fid];
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            line_dft<DET, -1>(v[c], t, sc, tws);
+            const int kx = grp + F::NG * c;
+#pragma unroll
+            for (int k2 = 0; k2 < F::N2; ++k2)
+#pragma unroll
+                for (int j = 0; j < F::KPT; ++j)
+                    out[kx * DET + t * F::KPT + j + F::N1 * k2] = cmul(v[c][j * F::N2 + k2], ph);
+        }
+        __syncthreads();
+    }
+}
+
+// grid (parts, ntheta): block (part, angle) owns slab dst[angle][part]
+template <int DET>
+__global__ void __launch_bounds__(PF<DET>::NT, 1)
+    k_ptycho_adj(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
+                 const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
+                 int P, float scale, const float2 *__restrict__ tw)
+{
+    using F = PF<DET>;
+    extern __shared__ float2 sm[];
+    float2 *fr = sm;
+    float2 *tws = sm + DET * F::P;
+    const int part = blockIdx.x, parts = gridDim.x, th = blockIdx.y;
+    float2 *slab = dst + ((size_t)th * parts + part) * nz * n;
+    for (int i = threadIdx.x; i < DET; i += F::NT) tws[i] = tw[i];
+    for (int e = threadIdx.x; e < nz * n; e += F::NT) slab[e] = czero();
+    const int t = threadIdx.x % F::N2, grp = threadIdx.x / F::N2;
+    float2 *sc = fr + grp * (DET + 1);
+    const int off = (DET - P) / 2;
+    __syncthreads();
+    for (int s = part; s < nscan; s += parts) {
+        const int fid = th * nscan + s;
+        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
+        if (stx < 0 || sty < 0) continue;
+        const float2 ph = phase[fid];
+        const float2 *in = g + (size_t)fid * DET * DET;
+        float2 v[F::CPG][F::N1];
+        // along the detector row: line = kx, points ky = t + N2 m (contiguous)
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            const int kx = grp + F::NG * c;
+#pragma unroll
+            for (int m = 0; m < F::N1; ++m) v[c][m] = scale * cmulc(ph, __ldg(&in[kx * DET + t + F::N2 * m]));
+            line_dft<DET, +1>(v[c], t, sc, tws);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            const int kx = grp + F::NG * c;
+#pragma unroll
+            for (int j = 0; j < F::KPT; ++j)
+#pragma unroll
+                for (int k2 = 0; k2 < F::N2; ++k2) {
+                    const int iy = t * F::KPT + j + F::N1 * k2;
+                    fr[iy * F::P + (kx ^ fswz<DET>(iy))] = v[c][j * F::N2 + k2];
+                }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            const int iy = grp + F::NG * c;
+            const int sw = fswz<DET>(iy);
+#pragma unroll
+            for (int m = 0; m < F::N1; ++m) v[c][m] = fr[iy * F::P + ((t + F::N2 * m) ^ sw)];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            line_dft<DET, +1>(v[c], t, sc, tws);
+            const int py = grp + F::NG * c - off;
+            if (py < 0 || py >= P) continue;
+            float2 *row = slab + (size_t)(sty + py) * n + stx;
+#pragma unroll
+            for (int k2 = 0; k2 < F::N2; ++k2)
+#pragma unroll
+                for (int j = 0; j < F::KPT; ++j) {
+                    const int px = t * F::KPT + j + F::N1 * k2 - off;
+                    if (px >= 0 && px < P) row[px] = row[px] + cmulc(__ldg(&prbT[py * P + px]), v[c][j * F::N2 + k2]);
+                }
+        }
+        __syncthreads();
+    }
+}
+
+// out[angle] = sum over parts of dst[angle][part], fixed order
+__global__ void k_ptycho_reduce(const float2 *__restrict__ part, float2 *__restrict__ out, size_t slab,
+                                int parts, size_t total)
+{
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t th = e / slab, i = e % slab;
+        const float2 *p = part + th * parts * slab + i;
+        float2 acc = p[0];
+        for (int k = 1; k < parts; ++k) acc = acc + p[k * slab];
+        out[e] = acc;
+    }
+}
+
+// prbT[iy][ix] = c * prb[ix][iy] (the reference's mul/mula index prb[iy + ix*Nprb])
+__global__ void k_probe_t(const float2 *__restrict__ prb, float2 *__restrict__ prbT, int P, float c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P * P) return;
+    const int iy = i / P, ix = i % P;
+    prbT[i] = c * prb[ix * P + iy];
+}
+
 }  // namespace
 
 struct pt_ptycho {
-    int ntheta = 0, nz = 0, n = 0, nscan = 0, det = 0, P = 0;
+    int ntheta = 0, nz = 0, n = 0, nscan = 0, det = 0, P = 0, parts = 1;
     int device = -1;
     bool ready = false;
     float c = 0.f;
-    float2 *tw = nullptr, *prb = nullptr, *phase = nullptr;
+    float2 *tw = nullptr, *prb = nullptr, *prbT = nullptr, *phase = nullptr, *partial = nullptr;
     int *corner = nullptr;
 };
 
@@ -136,25 +362,51 @@ namespace {
 template <int DET>
 int ptycho_attrs()
 {
-    const int s = DET * (DET + 1) * sizeof(float2);
-    PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
-    PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+    if constexpr (DET < 16) {
+        const int s = DET * (DET + 1) * sizeof(float2);
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd_small<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj_small<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+    } else {
+        const int s = (int)PF<DET>::SMEM;
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+    }
     return PT_OK;
 }
 
 template <int DET>
 int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st)
 {
-    const size_t s = DET * (DET + 1) * sizeof(float2);
-    if (!adj) {
-        k_ptycho_fwd<DET><<<dim3(h->nscan, h->ntheta), ptycho_block<DET>(), s, st>>>(
-            in, out, h->corner, h->phase, h->prb, h->nz, h->n, h->nscan, h->P, h->c, scale, h->tw);
-        PT_LAUNCHED("k_ptycho_fwd");
+    if constexpr (DET < 16) {
+        const size_t s = DET * (DET + 1) * sizeof(float2);
+        if (!adj) {
+            k_ptycho_fwd_small<DET><<<dim3(h->nscan, h->ntheta), ptycho_block<DET>(), s, st>>>(
+                in, out, h->corner, h->phase, h->prb, h->nz, h->n, h->nscan, h->P, h->c, scale, h->tw);
+            PT_LAUNCHED("k_ptycho_fwd_small");
+        } else {
+            k_ptycho_adj_small<DET><<<h->ntheta, ptycho_block<DET>(), s, st>>>(
+                in, out, h->corner, h->phase, h->prb, h->nz, h->n, h->nscan, h->P, h->c, scale, h->tw);
+            PT_LAUNCHED("k_ptycho_adj_small");
+        }
     } else {
-        k_ptycho_adj<DET><<<h->ntheta, ptycho_block<DET>(), s, st>>>(in, out, h->corner, h->phase, h->prb,
-                                                                   h->nz, h->n, h->nscan, h->P, h->c,
-                                                                   scale, h->tw);
-        PT_LAUNCHED("k_ptycho_adj");
+        using F = PF<DET>;
+        const int nframes = h->ntheta * h->nscan;
+        if (!adj) {
+            k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
+                                                              h->nscan, nframes, h->P, scale, h->tw);
+            PT_LAUNCHED("k_ptycho_fwd");
+        } else {
+            float2 *dst = h->parts > 1 ? h->partial : out;
+            k_ptycho_adj<DET><<<dim3(h->parts, h->ntheta), F::NT, F::SMEM, st>>>(
+                in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
+            PT_LAUNCHED("k_ptycho_adj");
+            if (h->parts > 1) {
+                const size_t slab = (size_t)h->nz * h->n, total = slab * h->ntheta;
+                const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+                k_ptycho_reduce<<<blocks, 256, 0, st>>>(h->partial, out, slab, h->parts, total);
+                PT_LAUNCHED("k_ptycho_reduce");
+            }
+        }
     }
     return PT_OK;
 }
@@ -189,7 +441,7 @@ int ptycho_dispatch(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float
 
 void ptycho_free(pt_ptycho *h)
 {
-    void *bufs[] = {h->tw, h->prb, h->phase, h->corner};
+    void *bufs[] = {h->tw, h->prb, h->prbT, h->phase, h->partial, h->corner};
     for (void *p : bufs)
         if (p) cudaFree(p);
 }
@@ -226,8 +478,15 @@ extern "C" int pt_ptycho_create(size_t ntheta, size_t nz, size_t n, size_t nthet
         pt::set_error("ptychofft: no CUDA device");
         return PT_ERR_CUDA;
     }
+    // adjoint split: enough (part, angle) blocks to fill the GPU twice
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+    h->parts = (detx >= 16 && (int)ntheta < 2 * nsm) ? (int)std::min<size_t>(nscan, (2 * nsm + ntheta - 1) / ntheta) : 1;
     bool ok = cudaMalloc((void **)&h->tw, detx * sizeof(float2)) == cudaSuccess &&
               cudaMalloc((void **)&h->prb, nprb * nprb * sizeof(float2)) == cudaSuccess &&
+              cudaMalloc((void **)&h->prbT, nprb * nprb * sizeof(float2)) == cudaSuccess &&
+              (h->parts == 1 || cudaMalloc((void **)&h->partial, (size_t)h->parts * ntheta * nz * n * sizeof(float2)) ==
+                                    cudaSuccess) &&
               cudaMalloc((void **)&h->phase, ntheta * nscan * sizeof(float2)) == cudaSuccess &&
               cudaMalloc((void **)&h->corner, 2 * ntheta * nscan * sizeof(int)) == cudaSuccess;
     if (!ok) {
@@ -275,6 +534,8 @@ extern "C" int pt_ptycho_setobj(pt_ptycho *h, const float *scan, const void *prb
     PT_CUDA(cudaMemcpyAsync(h->prb, prb, (size_t)h->P * h->P * sizeof(float2), cudaMemcpyDefault, st));
     k_ptycho_tables<<<(nf + 255) / 256, 256, 0, st>>>(scan, h->corner, h->phase, nf);
     PT_LAUNCHED("k_ptycho_tables");
+    k_probe_t<<<(h->P * h->P + 255) / 256, 256, 0, st>>>(h->prb, h->prbT, h->P, h->c);
+    PT_LAUNCHED("k_probe_t");
     std::vector<int> corner(2 * (size_t)nf);
     PT_CUDA(cudaMemcpyAsync(corner.data(), h->corner, corner.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
     PT_CUDA(cudaStreamSynchronize(st));

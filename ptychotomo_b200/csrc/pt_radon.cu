@@ -13,19 +13,22 @@
 //    K3 k_fwd_gather  Gaussian-kernel gather at the polar points, 1-D
 //                     centred inverse FFT along the detector, crop n of N
 //  adjoint  R* g  (radonusfft.cu:94-139)
-//    A1 k_adj_lines   edge-replicating pad, centred 1-D FFT
-//    A2 k_adj_scatter deterministic binned scatter: each block owns a tile of
-//                     the Fourier grid and sums, in a fixed order, the
-//                     contributions of the polar points whose kernel window
-//                     covers it (no float atomics, no halo, no fold pass)
-//    A3 k_adj_cols    column inverse FFT, keeping only the n rows that
-//                     survive the final crop
-//    A4 k_adj_rows    row inverse FFT + centring sign + 1/phi + circ + crop
+//    A1 k_adj_lines     edge-replicating pad, centred 1-D FFT, written for all
+//                       slices as lines[point][slice]
+//    A2 k_adj_colgather one block per (grid column, 16 slices): every cell of
+//                       the column sums, in a fixed order, w * g over the polar
+//                       points whose kernel window covers it (cell -> (point,
+//                       weight) lists built once at setobj; no float atomics,
+//                       no halo, no fold), then the column inverse FFT runs in
+//                       the same block and only the n rows that survive the
+//                       final crop are written
+//    A4 k_adj_rows      row inverse FFT + centring sign + 1/phi + circ + crop
 //
-// Slices are processed in chunks of ZC = 8; inside a chunk all intermediates
-// are stored slice-minor ([.. ][ZC]) so every tap of the gather, and every row
-// of the column kernels, is a contiguous 64-byte segment.  A chunk's
-// intermediates (N*2N + (2N)^2 complex per slice) stay far below L2 size.
+// The forward processes slices in chunks of ZC = 8 with slice-minor
+// intermediates ([..][ZC]) so every gather tap and every row of the column
+// kernel is a contiguous 64-byte segment, and a chunk's intermediates
+// (N*2N + (2N)^2 complex per slice) stay well inside L2.  The adjoint keeps
+// slice-minor full-volume buffers ([..][nzp], nzp = nz rounded up to 16).
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -201,14 +204,15 @@ __global__ void __launch_bounds__(ZC * 32)
 }
 
 // ---- A1: pad (kernels.cuh:189-206) + fftshift1c/FFT/fftshift1c -------------
+// grid (ntheta, nzp / ZC); writes lines[(theta*N + k) * nzp + z]
 template <int N>
 __global__ void __launch_bounds__(ZC * 32)
-    k_adj_lines(const float2 *__restrict__ g, float2 *__restrict__ lines, int nz, int z0, float pre,
+    k_adj_lines(const float2 *__restrict__ g, float2 *__restrict__ lines, int nz, int nzp, float pre,
                 const float2 *__restrict__ tw)
 {
     constexpr int n = 2 * N / 3, c0 = N / 6, c1 = 5 * N / 6 - 1, PITCH = N + 1, T = 32;
     extern __shared__ float2 sm[];
-    const int th = blockIdx.x;
+    const int th = blockIdx.x, z0 = blockIdx.y * ZC;
     const int f = threadIdx.x / T, t = threadIdx.x % T;
     const int z = z0 + f;
     float2 *b = sm + f * PITCH;
@@ -221,118 +225,101 @@ __global__ void __launch_bounds__(ZC * 32)
     ptfft::fft<N, -1, T>(b, 1, t, tw);
     for (int e = threadIdx.x; e < N * ZC; e += blockDim.x) {
         const int k = e / ZC, q = e % ZC;
-        lines[((size_t)th * N + k) * ZC + q] = ((k & 1) ? pre : -pre) * sm[q * PITCH + k];
+        lines[((size_t)th * N + k) * nzp + z0 + q] = ((k & 1) ? pre : -pre) * sm[q * PITCH + k];
     }
 }
 
-// ---- A2: binned deterministic scatter (transpose of the gather) ------------
-// Block = one TS x TS tile of the (2N)^2 Fourier grid, thread = one cell,
-// ZC slices in registers.  Points whose 15x15 window covers the tile are
-// listed (increasing point index) in a CSR built at setobj.
-template <int M, int TS>
-__global__ void __launch_bounds__(TS *TS)
-    k_adj_scatter(const float2 *__restrict__ lines, float2 *__restrict__ fadj, const int *__restrict__ tile_off,
-                  const int *__restrict__ tile_pts, const int *__restrict__ fxy, const float *__restrict__ xt,
-                  const float *__restrict__ yt, int N, float a)
-{
-    constexpr int W = 2 * M + 1;
-    __shared__ float s_wx[GB][W];
-    __shared__ float s_wy[GB][W];
-    __shared__ int s_ox[GB], s_oy[GB];
-    __shared__ float2 s_g[GB][ZC];
-    const int G = 2 * N;
-    const int ntx = G / TS;
-    const int tile = blockIdx.x;
-    const int cx = (tile % ntx) * TS + threadIdx.x % TS;
-    const int cy = (tile / ntx) * TS + threadIdx.x / TS;
-    float2 acc[ZC];
-#pragma unroll
-    for (int q = 0; q < ZC; ++q) acc[q] = czero();
-    const int beg = tile_off[tile], end = tile_off[tile + 1];
-    for (int b0 = beg; b0 < end; b0 += GB) {
-        const int cnt = min(GB, end - b0);
-        __syncthreads();
-        for (int e = threadIdx.x; e < cnt * 2 * W; e += blockDim.x) {
-            const int p = e / (2 * W), i = e % (2 * W);
-            const int pid = tile_pts[b0 + p];
-            if (i < W) {
-                const float x0 = xt[pid];
-                const float w0 = (float)(fxy[2 * pid] - M + i) / (float)G - x0;
-                s_wx[p][i] = expf(-a * (w0 * w0));
-            } else {
-                const float y0 = yt[pid];
-                const float w1 = (float)(fxy[2 * pid + 1] - M + (i - W)) / (float)G - y0;
-                s_wy[p][i - W] = expf(-a * (w1 * w1));
-            }
-        }
-        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
-            const int pid = tile_pts[b0 + e];
-            s_ox[e] = wrapG(N + fxy[2 * pid] - M, G);
-            s_oy[e] = wrapG(N + fxy[2 * pid + 1] - M, G);
-        }
-        for (int e = threadIdx.x; e < cnt * ZC; e += blockDim.x) {
-            const int p = e / ZC, q = e % ZC;
-            s_g[p][q] = lines[(size_t)tile_pts[b0 + p] * ZC + q];
-        }
-        __syncthreads();
-        for (int p = 0; p < cnt; ++p) {
-            int dx = cx - s_ox[p];
-            dx += dx < 0 ? G : 0;
-            int dy = cy - s_oy[p];
-            dy += dy < 0 ? G : 0;
-            if (dx < W && dy < W) {
-                const float w = s_wx[p][dx] * s_wy[p][dy];
-#pragma unroll
-                for (int q = 0; q < ZC; ++q) {
-                    const float2 v = s_g[p][q];
-                    acc[q].x = fmaf(w, v.x, acc[q].x);
-                    acc[q].y = fmaf(w, v.y, acc[q].y);
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < ZC; ++q) fadj[((size_t)cy * G + cx) * ZC + q] = acc[q];
-}
-
-// ---- A3: centring sign + column inverse FFT, keep the n cropped rows ------
+// ---- A2: column gather (transpose of the forward gather) + column IFFT ----
+// grid (nzp / 16, G); block = 16 FFTs x T threads.  One warp per grid cell:
+// lanes 0-15 and 16-31 take alternate entries of the cell's list for 16
+// slices and are combined at the end (fixed order -> deterministic).
+constexpr int ZQ = 16;
 template <int G>
-__global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
-    k_adj_cols(const float2 *__restrict__ fadj, float2 *__restrict__ rbuf, const float2 *__restrict__ tw)
+__global__ void __launch_bounds__(ZQ *fft_threads<G>())
+    k_adj_colgather(const float2 *__restrict__ lines, float2 *__restrict__ rbuf, const int *__restrict__ cell_off,
+                    const int2 *__restrict__ entries, const int *__restrict__ col_order, int nzp,
+                    const float2 *__restrict__ tw)
 {
-    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, PITCH = G + 1, NF = CK * ZC;
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, PITCH = G + 1;
+    constexpr int Y0 = N / 2 + N / 6;
+    constexpr int U = 4;  // entries in flight per lane
     extern __shared__ float2 sm[];
-    const int kx0 = blockIdx.x * CK;
-    const int f = threadIdx.x / T, t = threadIdx.x % T;
-    for (int e = threadIdx.x; e < G * NF; e += blockDim.x) {
-        const int ky = e / NF, q = e % NF;
-        const int kx = kx0 + q / ZC;
-        float2 v = fadj[((size_t)ky * G + kx0) * ZC + q];
-        if ((kx + ky) & 1) v = -1.f * v;
-        sm[q * PITCH + ky] = v;
+    const int z0 = blockIdx.x * ZQ;
+    const int kx = col_order[blockIdx.y];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = lane >> 4, zl = lane & 15;
+    const int nwarps = blockDim.x >> 5;
+    const float2 *lz = lines + z0 + zl;
+    for (int ky = warp; ky < G; ky += nwarps) {
+        const int cell = ky * G + kx;
+        const int beg = cell_off[cell], end = cell_off[cell + 1];
+        float2 acc = czero();
+        int e = beg + s;
+        for (; e + 2 * (U - 1) < end; e += 2 * U) {
+            int2 en[U];
+            float2 v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) en[u] = __ldg(&entries[e + 2 * u]);
+#pragma unroll
+            for (int u = 0; u < U; ++u) v[u] = __ldg(lz + (size_t)en[u].x * nzp);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const float w = __int_as_float(en[u].y);
+                acc.x = fmaf(w, v[u].x, acc.x);
+                acc.y = fmaf(w, v[u].y, acc.y);
+            }
+        }
+        for (; e < end; e += 2) {
+            const int2 en = __ldg(&entries[e]);
+            const float w = __int_as_float(en.y);
+            const float2 v = __ldg(lz + (size_t)en.x * nzp);
+            acc.x = fmaf(w, v.x, acc.x);
+            acc.y = fmaf(w, v.y, acc.y);
+        }
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, 16);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, 16);
+        if (s == 0) sm[zl * PITCH + ky] = ((kx + ky) & 1) ? -1.f * acc : acc;  // fftshiftc
     }
     __syncthreads();
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
     ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
-    constexpr int Y0 = N / 2 + N / 6;
-    for (int e = threadIdx.x; e < n * NF; e += blockDim.x) {
-        const int r = e / NF, q = e % NF;
-        rbuf[((size_t)r * G + kx0) * ZC + q] = sm[q * PITCH + Y0 + r];
+    for (int e = threadIdx.x; e < n * ZQ; e += blockDim.x) {
+        const int r = e / ZQ, q = e % ZQ;
+        rbuf[((size_t)r * G + kx) * nzp + z0 + q] = sm[q * PITCH + Y0 + r];
     }
+}
+
+// setobj: the weight of every (cell, point) entry, same expression as the
+// forward gather (wx * wy, kernels.cuh:115-119 written separably)
+template <int M>
+__global__ void k_make_entries(const int *__restrict__ keys, int2 *__restrict__ entries, size_t total,
+                               const int *__restrict__ fxy, const float *__restrict__ xt,
+                               const float *__restrict__ yt, int G, float a)
+{
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int key = keys[e];
+    const int p = key >> 8, i1 = (key >> 4) & 15, i0 = key & 15;
+    const float w0 = (float)(fxy[2 * p] - M + i0) / (float)G - xt[p];
+    const float w1 = (float)(fxy[2 * p + 1] - M + i1) / (float)G - yt[p];
+    const float w = expf(-a * (w0 * w0)) * expf(-a * (w1 * w1));
+    entries[e] = make_int2(p, __float_as_int(w));
 }
 
 // ---- A4: row inverse FFT + fftshiftc + unpaddivphi + circ + crop -----------
+// grid (n, nzp / ZC); reads rbuf[(r * G + kx) * nzp + z]
 template <int G>
 __global__ void __launch_bounds__(ZC *fft_threads<G>())
-    k_adj_rows(const float2 *__restrict__ rbuf, float2 *__restrict__ out, int nz, int z0, float mu, float scale,
+    k_adj_rows(const float2 *__restrict__ rbuf, float2 *__restrict__ out, int nz, int nzp, float mu, float scale,
                const float2 *__restrict__ tw)
 {
     constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, c0 = N / 6, PITCH = G + 1;
     extern __shared__ float2 sm[];
-    const int r = blockIdx.x;
+    const int r = blockIdx.x, z0 = blockIdx.y * ZC;
     const int f = threadIdx.x / T, t = threadIdx.x % T;
     for (int e = threadIdx.x; e < G * ZC; e += blockDim.x) {
         const int kx = e / ZC, q = e % ZC;
-        sm[q * PITCH + kx] = rbuf[((size_t)r * G + kx) * ZC + q];
+        sm[q * PITCH + kx] = rbuf[((size_t)r * G + kx) * nzp + z0 + q];
     }
     __syncthreads();
     ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
@@ -360,24 +347,28 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
 // handle
 // ============================================================================
 struct pt_radon {
-    int ntheta = 0, nz = 0, n = 0, N = 0, G = 0, M = 0, TS = 0;
+    int ntheta = 0, nz = 0, n = 0, N = 0, G = 0, M = 0, nzp = 0;
     float mu = 0.f;
     int device = -1;
     bool ready = false;
     float2 *tw_G = nullptr, *tw_N = nullptr;
     float *theta = nullptr, *x = nullptr, *y = nullptr;
     int *fxy = nullptr;
-    float2 *rbuf = nullptr, *fgrid = nullptr, *lines = nullptr;
-    int *tile_off = nullptr, *tile_pts = nullptr;
-    size_t tile_pts_cap = 0;
+    // forward (per chunk of ZC slices)
+    float2 *rbuf = nullptr, *fgrid = nullptr;
+    // adjoint (all slices, slice-minor with nzp lanes)
+    float2 *lines = nullptr, *rbuf_adj = nullptr;
+    int *cell_off = nullptr, *col_order = nullptr;
+    int2 *entries = nullptr;
+    size_t entries_cap = 0;
 };
 
 namespace {
 
 void radon_free(pt_radon *h)
 {
-    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->rbuf,
-                    h->fgrid, h->lines, h->tile_off, h->tile_pts};
+    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->rbuf, h->fgrid,
+                    h->lines, h->rbuf_adj, h->cell_off, h->col_order, h->entries};
     for (void *p : bufs)
         if (p) cudaFree(p);
 }
@@ -409,7 +400,8 @@ int set_attrs()
     const int s2 = CK * ZC * (G + 1) * sizeof(float2);
     PT_CUDA(cudaFuncSetAttribute(k_fwd_rows<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
     PT_CUDA(cudaFuncSetAttribute(k_fwd_cols<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
-    PT_CUDA(cudaFuncSetAttribute(k_adj_cols<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
+    const int s4 = ZQ * (G + 1) * sizeof(float2);
+    PT_CUDA(cudaFuncSetAttribute(k_adj_colgather<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s4));
     PT_CUDA(cudaFuncSetAttribute(k_adj_rows<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
     const int s3 = ZC * (N + 1) * sizeof(float2);
     PT_CUDA(cudaFuncSetAttribute(k_fwd_gather<N, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
@@ -444,26 +436,17 @@ int run_adj(pt_radon *h, float2 *f, const float2 *g, float scale, cudaStream_t s
 {
     constexpr int N = G / 2, n = G / 3, T = fft_threads<G>();
     const size_t s1 = ZC * (G + 1) * sizeof(float2);
-    const size_t s2 = CK * ZC * (G + 1) * sizeof(float2);
     const size_t s3 = ZC * (N + 1) * sizeof(float2);
-    const float a = (float)(PI_REF * PI_REF / h->mu);
+    const size_t s4 = ZQ * (G + 1) * sizeof(float2);
     const float pre = (float)(PI_REF / std::fabs(h->mu)) / (float)N;
-    const int ntiles = (G / h->TS) * (G / h->TS);
-    for (int z0 = 0; z0 < h->nz; z0 += ZC) {
-        k_adj_lines<N><<<h->ntheta, ZC * 32, s3, st>>>(g, h->lines, h->nz, z0, pre, h->tw_N);
-        PT_LAUNCHED("k_adj_lines");
-        if (h->TS == 16)
-            k_adj_scatter<M, 16><<<ntiles, 256, 0, st>>>(h->lines, h->fgrid, h->tile_off, h->tile_pts, h->fxy,
-                                                        h->x, h->y, N, a);
-        else
-            k_adj_scatter<M, 8><<<ntiles, 64, 0, st>>>(h->lines, h->fgrid, h->tile_off, h->tile_pts, h->fxy,
-                                                      h->x, h->y, N, a);
-        PT_LAUNCHED("k_adj_scatter");
-        k_adj_cols<G><<<G / CK, CK * ZC * T, s2, st>>>(h->fgrid, h->rbuf, h->tw_G);
-        PT_LAUNCHED("k_adj_cols");
-        k_adj_rows<G><<<n, ZC * T, s1, st>>>(h->rbuf, f, h->nz, z0, h->mu, scale, h->tw_G);
-        PT_LAUNCHED("k_adj_rows");
-    }
+    const int nzp = h->nzp;
+    k_adj_lines<N><<<dim3(h->ntheta, nzp / ZC), ZC * 32, s3, st>>>(g, h->lines, h->nz, nzp, pre, h->tw_N);
+    PT_LAUNCHED("k_adj_lines");
+    k_adj_colgather<G><<<dim3(nzp / ZQ, G), ZQ * T, s4, st>>>(h->lines, h->rbuf_adj, h->cell_off, h->entries,
+                                                             h->col_order, nzp, h->tw_G);
+    PT_LAUNCHED("k_adj_colgather");
+    k_adj_rows<G><<<dim3(n, nzp / ZC), ZC * T, s1, st>>>(h->rbuf_adj, f, h->nz, nzp, h->mu, scale, h->tw_G);
+    PT_LAUNCHED("k_adj_rows");
     return PT_OK;
 }
 
@@ -537,6 +520,8 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     PT_CHECK_ARG(ntheta >= 1 && ntheta <= (1u << 20), "radonusfft: bad Ntheta %zu", ntheta);
     PT_CHECK_ARG(nz >= 1 && nz <= (1u << 20), "radonusfft: bad Nz %zu", nz);
     PT_CHECK_ARG(n >= 8 && n % 8 == 0, "radonusfft: n=%zu must be a positive multiple of 8", n);
+    PT_CHECK_ARG(ntheta * (3 * n / 2) < ((size_t)1 << 23), "radonusfft: Ntheta*3n/2 = %zu polar points exceed 2^23",
+                 ntheta * (3 * n / 2));
     PT_CHECK_ARG(m_override == 0 || m_override == 4 || m_override == 7,
                  "radonusfft: kernel half-width override %d not compiled (0, 4 or 7)", m_override);
     const int G = (int)(3 * n);
@@ -550,7 +535,6 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     h->n = (int)n;
     radon_params((int)n, m_override, &h->N, &h->M, &h->mu);
     h->G = G;
-    h->TS = (G % 16 == 0) ? 16 : 8;
     if (cudaGetDevice(&h->device) != cudaSuccess) {
         delete h;
         pt::set_error("radonusfft: no CUDA device");
@@ -571,8 +555,12 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     if (rc == PT_OK) rc = dmalloc(&h->fxy, 2 * ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->rbuf, N * G * ZC);
     if (rc == PT_OK) rc = dmalloc(&h->fgrid, (size_t)G * G * ZC);
-    if (rc == PT_OK) rc = dmalloc(&h->lines, ntheta * N * ZC);
-    if (rc == PT_OK) rc = dmalloc(&h->tile_off, (size_t)(G / h->TS) * (G / h->TS) + 1);
+    h->nzp = (int)((nz + ZQ - 1) / ZQ * ZQ);
+    const size_t nzp = h->nzp;
+    if (rc == PT_OK) rc = dmalloc(&h->lines, ntheta * N * nzp);
+    if (rc == PT_OK) rc = dmalloc(&h->rbuf_adj, n * (size_t)G * nzp);
+    if (rc == PT_OK) rc = dmalloc(&h->cell_off, (size_t)G * G + 1);
+    if (rc == PT_OK) rc = dmalloc(&h->col_order, (size_t)G);
     if (rc == PT_OK) rc = radon_set_attrs(G);
     if (rc == PT_OK) {
         std::vector<float2> tw(G);
@@ -617,7 +605,7 @@ extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
     if (rc != PT_OK) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     h->ready = false;
-    const int N = h->N, G = h->G, M = h->M, W = 2 * M + 1, TS = h->TS, ntheta = h->ntheta;
+    const int N = h->N, G = h->G, M = h->M, W = 2 * M + 1, ntheta = h->ntheta;
     PT_CUDA(cudaMemcpyAsync(h->theta, theta, ntheta * sizeof(float), cudaMemcpyDefault, st));
     k_takexy<<<dim3((N + 127) / 128, ntheta), 128, 0, st>>>(h->x, h->y, h->theta, N, ntheta);
     PT_LAUNCHED("k_takexy");
@@ -637,56 +625,73 @@ extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
         fxy[2 * p] = (int)floorf((float)G * xs[p]);
         fxy[2 * p + 1] = (int)floorf((float)G * ys[p]);
     }
-    // CSR of tile -> points whose window [o, o+W) (mod G) touches the tile
-    const int nt = G / TS, ntiles = nt * nt;
-    std::vector<int> cnt(ntiles + 1, 0);
-    auto tiles_of = [&](int o, int *list) {
-        int k = 0;
+    PT_CUDA(cudaMemcpy(h->fxy, fxy.data(), 2 * npts * sizeof(int), cudaMemcpyHostToDevice));
+    // cell -> (point, tap) lists for the adjoint: every point lists its
+    // (2M+1)^2 window cells (mod G: the reference's halo fold, kernels.cuh:67-82),
+    // in increasing point order, so each cell sums in a fixed order.
+    const size_t ncell = (size_t)G * G;
+    std::vector<int> off(ncell + 1, 0);
+    int cols[32], rows[32];
+    auto window = [&](size_t p) {
+        const int ox = ((N + fxy[2 * p] - M) % G + G) % G;
+        const int oy = ((N + fxy[2 * p + 1] - M) % G + G) % G;
         for (int i = 0; i < W; ++i) {
-            const int t = ((o + i) % G) / TS;
-            bool seen = false;
-            for (int j = 0; j < k; ++j) seen |= (list[j] == t);
-            if (!seen) list[k++] = t;
+            cols[i] = (ox + i) % G;
+            rows[i] = (oy + i) % G;
         }
-        return k;
     };
-    int lx[32], ly[32];
-    for (int pass = 0; pass < 2; ++pass) {
-        std::vector<int> pos;
-        if (pass == 1) {
-            for (int t = 0; t < ntiles; ++t) cnt[t + 1] += cnt[t];
-            pos.assign(cnt.begin(), cnt.end() - 1);
-        }
-        std::vector<int> pts;
-        if (pass == 1) pts.resize(cnt[ntiles]);
+    for (size_t p = 0; p < npts; ++p) {
+        window(p);
+        for (int i1 = 0; i1 < W; ++i1)
+            for (int i0 = 0; i0 < W; ++i0) off[(size_t)rows[i1] * G + cols[i0] + 1]++;
+    }
+    for (size_t c = 0; c < ncell; ++c) off[c + 1] += off[c];
+    const size_t total = (size_t)off[ncell];
+    std::vector<int> keys(total);
+    {
+        std::vector<int> pos(off.begin(), off.end() - 1);
         for (size_t p = 0; p < npts; ++p) {
-            const int ox = ((N + fxy[2 * p] - M) % G + G) % G;
-            const int oy = ((N + fxy[2 * p + 1] - M) % G + G) % G;
-            const int kx = tiles_of(ox, lx), ky = tiles_of(oy, ly);
-            for (int j = 0; j < ky; ++j)
-                for (int i = 0; i < kx; ++i) {
-                    const int t = ly[j] * nt + lx[i];
-                    if (pass == 0)
-                        cnt[t + 1]++;
-                    else
-                        pts[pos[t]++] = (int)p;
-                }
-        }
-        if (pass == 1) {
-            const size_t need = pts.size();
-            if (need > h->tile_pts_cap) {
-                if (h->tile_pts) cudaFree(h->tile_pts);
-                h->tile_pts = nullptr;
-                h->tile_pts_cap = 0;
-                rc = dmalloc(&h->tile_pts, need);
-                if (rc != PT_OK) return rc;
-                h->tile_pts_cap = need;
-            }
-            PT_CUDA(cudaMemcpy(h->tile_pts, pts.data(), need * sizeof(int), cudaMemcpyHostToDevice));
-            PT_CUDA(cudaMemcpy(h->tile_off, cnt.data(), (ntiles + 1) * sizeof(int), cudaMemcpyHostToDevice));
+            window(p);
+            for (int i1 = 0; i1 < W; ++i1)
+                for (int i0 = 0; i0 < W; ++i0)
+                    keys[pos[(size_t)rows[i1] * G + cols[i0]]++] = (int)((p << 8) | (i1 << 4) | i0);
         }
     }
-    PT_CUDA(cudaMemcpy(h->fxy, fxy.data(), 2 * npts * sizeof(int), cudaMemcpyHostToDevice));
+    // columns ordered by decreasing work so the heavy centre columns start first
+    std::vector<long long> colw(G, 0);
+    for (size_t c = 0; c < ncell; ++c) colw[c % G] += off[c + 1] - off[c];
+    std::vector<int> order(G);
+    for (int i = 0; i < G; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int i, int j) { return colw[i] > colw[j]; });
+    if (total > h->entries_cap) {
+        if (h->entries) cudaFree(h->entries);
+        h->entries = nullptr;
+        h->entries_cap = 0;
+        rc = dmalloc(&h->entries, total);
+        if (rc != PT_OK) return rc;
+        h->entries_cap = total;
+    }
+    int *dkeys = nullptr;
+    rc = dmalloc(&dkeys, total);
+    if (rc != PT_OK) return rc;
+    cudaError_t e1 = cudaMemcpy(dkeys, keys.data(), total * sizeof(int), cudaMemcpyHostToDevice);
+    if (e1 == cudaSuccess) {
+        const float a = (float)(PI_REF * PI_REF / h->mu);
+        const unsigned blocks = (unsigned)((total + 255) / 256);
+        if (M == 7)
+            k_make_entries<7><<<blocks, 256, 0, st>>>(dkeys, h->entries, total, h->fxy, h->x, h->y, G, a);
+        else
+            k_make_entries<4><<<blocks, 256, 0, st>>>(dkeys, h->entries, total, h->fxy, h->x, h->y, G, a);
+        e1 = cudaGetLastError();
+        if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(st);
+    }
+    cudaFree(dkeys);
+    if (e1 != cudaSuccess) {
+        pt::set_error("radonusfft.setobj: building the adjoint lists failed: %s", cudaGetErrorString(e1));
+        return PT_ERR_CUDA;
+    }
+    PT_CUDA(cudaMemcpy(h->cell_off, off.data(), (ncell + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    PT_CUDA(cudaMemcpy(h->col_order, order.data(), G * sizeof(int), cudaMemcpyHostToDevice));
     h->ready = true;
     return PT_OK;
 }
