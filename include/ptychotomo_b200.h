@@ -97,6 +97,54 @@ int pt_ptycho_adj(pt_ptycho *h, void *f, const void *g, void *stream);
 int pt_ptycho_fwd_scaled(pt_ptycho *h, void *g, const void *f, float scale, void *stream);
 int pt_ptycho_adj_scaled(pt_ptycho *h, void *f, const void *g, float scale, void *stream);
 
+
+/* ---- Solver arithmetic (src/ptychotomo/solver.py:48-336) -----------------
+ * Building blocks of the drop-in Solver; complex arrays are complex64.
+ * Reductions accumulate in FP64 into `out` (device doubles) through a caller
+ * workspace of pt_reduce_workspace_bytes() bytes; results are deterministic
+ * (fixed grid, fixed summation order). */
+size_t pt_reduce_workspace_bytes(void);
+/* op 0: ||a||^2; 1: sum conj(a)*b (re, im); 2: ||a||^2, Re<a,b>, ||b||^2;
+ * 3: max|a|; 4: sum angle(a) over columns [c0, c1) of rows of length ncol
+ * (takexi's background phase, solver.py:151-156); 5: ||a - b||^2;
+ * 6: sum_i sqrt(|a_i|^2 + |a_{i+n}|^2 + |a_{i+2n}|^2) (TV term of take_lagr,
+ * solver.py:299); 7: max|angle(a)| (phase-wrap check, solver.py:238). */
+int pt_reduce_c64(int op, const void *a, const void *b, size_t n, int c0, int c1, int ncol, void *work,
+                  void *out, void *stream);
+/* Ptycho data-term decrease of the CG line search for J step lengths
+ * (solver.py:208-214, :171-177), with D = dscale * data and t(x) =
+ * |x|^2 - 2 D log max(|x|, 1e-32) (model 0, Poisson) or (|x| - sqrt D)^2
+ * (model 1, Gaussian):  out[j] = sum over frames of t(f) - t(f + gammas[j] d),
+ * formed per element in FP64.  gammas: device double[J], J <= 16. */
+int pt_ls_frames(const void *f, const void *d, const float *data, float dscale, size_t n, int model,
+                 const double *gammas, int J, void *work, void *out, void *stream);
+/* Lagrangian data term, solver.py:294-298 (D = dscale * data). */
+int pt_lagr_frames(const void *f, const float *data, float dscale, size_t n, int model, void *work, void *out,
+                   void *stream);
+/* Gradient residual of the data term (solver.py:220-224), D = dscale * data:
+ * Poisson f - D f / (|f|^2 + 1e-32); Gaussian f - sqrt(D) exp(i angle f). */
+int pt_residual_c64(void *out, const void *f, const float *data, float dscale, size_t n, int model, void *stream);
+/* out = scale * |x|^2 (float32), the intensities of fwd_ptycho_batch (solver.py:115). */
+int pt_abs2_c64(float *out, const void *x, size_t n, float scale, void *stream);
+/* out = sum_{j<k} coef[j] * x[j]  (k <= 4, coef as (re, im) float pairs). */
+int pt_lincomb_c64(void *out, size_t n, int k, const void *const *x, const float *coef, void *stream);
+/* mode 0: out = a*b; 1: out = conj(a)*(b - c); 2: out = conj(a)*b. */
+int pt_cmul_c64(void *out, const void *a, const void *b, const void *c, size_t n, int mode, void *stream);
+/* out = exp(i s x) exp(i phi)  (exptomo, solver.py:59-60, and the h update, :322). */
+int pt_expmap_c64(void *out, const void *x, size_t n, float s, float phi, void *stream);
+/* out = (cre + i cim) * mlog(x)  (mlog/logtomo, solver.py:48-64). */
+int pt_logmap_c64(void *out, const void *x, size_t n, float cre, float cim, void *stream);
+/* takexi, solver.py:163-166, from t = (psi - lamd/rho) exp(-i pshift):
+ * K = i t * inv_tmax, xi0 = K * (-i mlog(t)) * cxi. */
+int pt_takexi_c64(void *K, void *xi0, const void *t, size_t n, float inv_tmax, float cxi, void *stream);
+/* TV operator J (fwd_reg, solver.py:128-134) and J* (adj_reg, :137-146),
+ * u [nz][ny][nx], res/g [3][nz][ny][nx], scaled by s (2/sqrt(3), -2/sqrt(3)). */
+int pt_reg_fwd_c64(void *res, const void *u, int nz, int ny, int nx, float s, void *stream);
+int pt_reg_adj_c64(void *res, const void *g, int nz, int ny, int nx, float s, void *stream);
+/* solve_reg, solver.py:257-264: z = soft(J u + mu/tau, thr), isotropic over the 3 components. */
+int pt_solve_reg_c64(void *z, const void *u, const void *mu, int nz, int ny, int nx, float s, float inv_tau,
+                     float thr, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -4,8 +4,12 @@ TEST INFRASTRUCTURE (the oracle).  Mirrors src/ptychotomo/solver.py:19-336
 method by method with CuPy replaced by NumPy.  Arrays are complex64 like the
 reference; every reduction (norms, dot products, sums of the likelihood)
 is accumulated in float64, which is the precision choice the GPU engine
-makes too.  One documented fix: ``takexi`` uses ``r = prb.shape[0] // 2``
-(solver.py:151 divides with ``/`` and then slices with the float).
+makes too.  Documented fixes: ``takexi`` uses ``r = prb.shape[0] // 2``
+(solver.py:151 divides with ``/`` and then slices with the float); the CG
+loops stop once the line search returns gamma = 0 (gamma only halves, so the
+iterate cannot change any more; the reference would go on to divide by an
+exactly-zero Dai-Yuan denominator and return NaN), and a zero Dai-Yuan
+denominator gives beta = 0.
 """
 from __future__ import annotations
 
@@ -33,7 +37,7 @@ def _vdot(a, b):
 class Solver:
     """solver.py:19-46 constructor; operators as in solver.py:48-146."""
 
-    def __init__(self, prb, scan, theta, det, voxelsize, energy, ntheta, nz, n, ptheta, pnz):
+    def __init__(self, prb, scan, theta, det, voxelsize, energy, ntheta, nz, n, ptheta, pnz, xy=None):
         self.voxelsize = voxelsize
         self.energy = energy
         self.scan = np.asarray(scan, np.float32)
@@ -45,7 +49,7 @@ class Solver:
         self.ptheta, self.pnz = ptheta, pnz
         self.cl_ptycho = PtychoFFT(ptheta, nz, n, ptheta, self.nscan, self.ndety, self.ndetx, self.nprb)
         self.cl_tomo = RadonUSFFT(ntheta, pnz, n)
-        self.cl_tomo.setobj(np.asarray(theta, np.float32))
+        self.cl_tomo.setobj(np.asarray(theta, np.float32), xy=xy)
         self.coeftomo = np.float32(1 / np.sqrt(ntheta * n / 2))
         self.coefptycho = np.float32(1 / np.abs(self.prb).max())
         self.coefdata = np.float32(1 / (self.ndetx * self.ndety * (np.abs(self.prb) ** 2).max()))
@@ -140,11 +144,15 @@ class Solver:
         return xi0, xi1, K, pshift
 
     # ---- line search, solver.py:171-177 ------------------------------------
-    def line_search(self, minf, gamma, u, fu, d, fd):
+    trace = None   # list: records (kind, gamma) of every line search when set
+
+    def line_search(self, minf, gamma, u, fu, d, fd, kind=""):
         while minf(u, fu) - minf(u + gamma * d, fu + gamma * fd) < 0 and gamma > 1e-12:
             gamma *= 0.5
         if gamma <= 1e-12:
             gamma = 0
+        if self.trace is not None:
+            self.trace.append((kind, gamma))
         return gamma
 
     # ---- CG tomography, solver.py:180-203 ----------------------------------
@@ -162,12 +170,15 @@ class Solver:
             if i == 0:
                 d = -grad
             else:
-                beta = _norm2(grad) / _vdot(d, grad - grad0)
+                den = _vdot(d, grad - grad0)
+                beta = _norm2(grad) / den if den != 0 else 0.0
                 d = (-grad + beta * d).astype(np.complex64)
             grad0 = grad
             gamma = self.line_search(minf, gamma, KRu, gu,
-                                     (K * self.fwd_tomo_batch(d)).astype(np.complex64), self.fwd_reg(d))
+                                     (K * self.fwd_tomo_batch(d)).astype(np.complex64), self.fwd_reg(d), "tomo")
             u = (u + gamma * d).astype(np.complex64)
+            if gamma == 0:
+                break   # gamma only halves: u can no longer change in this call
         return u
 
     # ---- CG ptychography, solver.py:206-254 --------------------------------
@@ -193,12 +204,15 @@ class Solver:
             if i == 0:
                 d = -grad
             else:
-                beta = _norm2(grad) / _vdot(d, grad - grad0)
+                den = _vdot(d, grad - grad0)
+                beta = _norm2(grad) / den if den != 0 else 0.0
                 d = (-grad + beta * d).astype(np.complex64)
             grad0 = grad
             fd = self.fwd_ptycho(d)
-            gamma = self.line_search(minf, gamma, psi, fpsi, d, fd)
+            gamma = self.line_search(minf, gamma, psi, fpsi, d, fd, "ptycho")
             psi = (psi + gamma * d).astype(np.complex64)
+            if gamma == 0:
+                break   # gamma only halves: psi can no longer change in this call
         return psi
 
     def cg_ptycho_batch(self, data, init, h, lamd, rho, piter, model):

@@ -59,6 +59,20 @@ SIGNATURES = {
     "pt_ptycho_adj": (_int, [_vp, _vp, _vp, _vp]),
     "pt_ptycho_fwd_scaled": (_int, [_vp, _vp, _vp, _f, _vp]),
     "pt_ptycho_adj_scaled": (_int, [_vp, _vp, _vp, _f, _vp]),
+    "pt_reduce_workspace_bytes": (_sz, []),
+    "pt_reduce_c64": (_int, [_int, _vp, _vp, _sz, _int, _int, _int, _vp, _vp, _vp]),
+    "pt_ls_frames": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp, _int, _vp, _vp, _vp]),
+    "pt_lagr_frames": (_int, [_vp, _vp, _f, _sz, _int, _vp, _vp, _vp]),
+    "pt_residual_c64": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp]),
+    "pt_abs2_c64": (_int, [_vp, _vp, _sz, _f, _vp]),
+    "pt_lincomb_c64": (_int, [_vp, _sz, _int, ctypes.POINTER(_vp), ctypes.POINTER(_f), _vp]),
+    "pt_cmul_c64": (_int, [_vp, _vp, _vp, _vp, _sz, _int, _vp]),
+    "pt_expmap_c64": (_int, [_vp, _vp, _sz, _f, _f, _vp]),
+    "pt_logmap_c64": (_int, [_vp, _vp, _sz, _f, _f, _vp]),
+    "pt_takexi_c64": (_int, [_vp, _vp, _vp, _sz, _f, _f, _vp]),
+    "pt_reg_fwd_c64": (_int, [_vp, _vp, _int, _int, _int, _f, _vp]),
+    "pt_reg_adj_c64": (_int, [_vp, _vp, _int, _int, _int, _f, _vp]),
+    "pt_solve_reg_c64": (_int, [_vp, _vp, _vp, _int, _int, _int, _f, _f, _f, _vp]),
 }
 
 _lib = None

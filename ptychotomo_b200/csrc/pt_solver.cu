@@ -1,0 +1,506 @@
+// Solver-side kernels: elementwise maps, TV regulariser, FP64 reductions.
+//
+// These carry the arithmetic of the reference's CuPy Solver
+// (src/ptychotomo/solver.py:48-336) that is not an operator:
+//   linear combinations of complex arrays (CG/ADMM updates), the TV
+//   operator J and its adjoint (solver.py:128-146), the soft-threshold
+//   regulariser step (solver.py:257-264), the exp/log maps (solver.py:48-64),
+//   the linearisation of takexi (solver.py:149-168) and every norm / inner
+//   product / likelihood sum, accumulated in FP64.
+//
+// Reductions are deterministic: fixed grid, per-block partials in a caller
+// workspace, then one block sums the partials in order.
+#include <cmath>
+
+#include "pt_common.cuh"
+
+namespace {
+
+constexpr int RB = 1184;    // reduction blocks (148 SMs x 8)
+constexpr int RT = 256;     // reduction threads per block
+constexpr int MAXK = 16;    // max outputs of one reduction
+
+__device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+template <int K>
+__device__ __forceinline__ void block_reduce_store(double (&acc)[K], double *work, int blk, int nblk)
+{
+    __shared__ double red[RT / 32][MAXK];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0;
+        for (int w = 0; w < RT / 32; ++w) s += red[w][threadIdx.x];
+        work[(size_t)threadIdx.x * nblk + blk] = s;
+    }
+}
+
+// one block: out[k] = sum_b work[k * nblk + b] (fixed order per thread, then tree)
+__global__ void k_finish(const double *__restrict__ work, double *__restrict__ out, int K, int nblk, int op_max)
+{
+    __shared__ double red[RT];
+    for (int k = 0; k < K; ++k) {
+        double s = op_max ? -1.0 : 0.0;
+        for (int b = threadIdx.x; b < nblk; b += RT) {
+            const double v = work[(size_t)k * nblk + b];
+            s = op_max ? fmax(s, v) : s + v;
+        }
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = RT / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] = op_max ? fmax(red[threadIdx.x], red[threadIdx.x + w])
+                                                           : red[threadIdx.x] + red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[k] = red[0];
+        __syncthreads();
+    }
+}
+
+// ---- generic reductions over complex64 arrays --------------------------------
+// op 0: ||a||^2                         -> 1 value
+// op 1: sum conj(a) b                   -> 2 values (re, im)
+// op 2: ||a||^2, Re<a,b>, ||b||^2        -> 3 values
+// op 3: max |a|                         -> 1 value
+// op 4: sum angle(a) over columns [c0,c1) of rows of length ncol -> 1 value
+// op 5: ||a - b||^2                     -> 1 value
+// op 6: sum_i sqrt(|a_i|^2 + |a_{i+n}|^2 + |a_{i+2n}|^2) (a has 3n entries) -> 1 value
+// op 7: max |angle(a)|                  -> 1 value
+__global__ void __launch_bounds__(RT) k_reduce(int op, const float2 *__restrict__ a, const float2 *__restrict__ b,
+                                               size_t n, int c0, int c1, int ncol, double *__restrict__ work)
+{
+    double acc[3] = {0, 0, 0};
+    const bool is_max = (op == 3 || op == 7);
+    if (is_max) acc[0] = -1.0;
+    for (size_t i = (size_t)blockIdx.x * RT + threadIdx.x; i < n; i += (size_t)gridDim.x * RT) {
+        const float2 x = a[i];
+        if (op == 5) {
+            const float2 y = b[i];
+            const double dx = (double)x.x - y.x, dy = (double)x.y - y.y;
+            acc[0] += dx * dx + dy * dy;
+        } else if (op == 6) {
+            const float2 y = a[i + n], z = a[i + 2 * n];
+            acc[0] += (double)sqrtf(x.x * x.x + x.y * x.y + y.x * y.x + y.y * y.y + z.x * z.x + z.y * z.y);
+        } else if (op == 7) {
+            acc[0] = fmax(acc[0], (double)fabsf(atan2f(x.y, x.x)));
+        } else if (op == 0) {
+            acc[0] += (double)x.x * x.x + (double)x.y * x.y;
+        } else if (op == 1) {
+            const float2 y = b[i];
+            acc[0] += (double)x.x * y.x + (double)x.y * y.y;
+            acc[1] += (double)x.x * y.y - (double)x.y * y.x;
+        } else if (op == 2) {
+            const float2 y = b[i];
+            acc[0] += (double)x.x * x.x + (double)x.y * x.y;
+            acc[1] += (double)x.x * y.x + (double)x.y * y.y;
+            acc[2] += (double)y.x * y.x + (double)y.y * y.y;
+        } else if (op == 3) {
+            acc[0] = fmax(acc[0], (double)hypotf(x.x, x.y));
+        } else {
+            const int col = (int)(i % ncol);
+            if (col >= c0 && col < c1) acc[0] += (double)atan2f(x.y, x.x);
+        }
+    }
+    if (is_max) {
+        // max: reduce with max instead of sum
+        __shared__ double red[RT];
+        red[threadIdx.x] = acc[0];
+        __syncthreads();
+        for (int w = RT / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) work[blockIdx.x] = red[0];
+        return;
+    }
+    block_reduce_store<3>(acc, work, blockIdx.x, gridDim.x);
+}
+
+// ---- ptycho data terms over detector frames (solver.py:208-214, :294-298) ---
+// model 0 Poisson, 1 Gaussian.  With t(x) = |x|^2 - 2 D log(max(|x|, 1e-32))
+// (Poisson) or (|x| - sqrt D)^2 (Gaussian), out[j] = sum t(f) - t(f + g_j d):
+// the decrease of the data term for step g_j, formed per element in FP64 so
+// that it carries no cancellation of the (much larger) term itself.  |x| is
+// the float32 modulus, as np.abs / cp.abs of complex64.
+__device__ __forceinline__ double data_term(float a, float dd, int model)
+{
+    if (model == 0) return (double)a * a - 2.0 * (double)dd * log(fmax((double)a, 1e-32));
+    const double t = (double)a - (double)sqrtf(dd);
+    return t * t;
+}
+
+__global__ void __launch_bounds__(RT) k_ls_frames(const float2 *__restrict__ f, const float2 *__restrict__ d,
+                                                  const float *__restrict__ D, float dscale, size_t n, int model,
+                                                  const double *__restrict__ gam, int J, double *__restrict__ work)
+{
+    double acc[MAXK];
+#pragma unroll
+    for (int j = 0; j < MAXK; ++j) acc[j] = 0;
+    float gj[MAXK];
+#pragma unroll
+    for (int j = 0; j < MAXK; ++j) gj[j] = j < J ? (float)gam[j] : 0.f;
+    for (size_t i = (size_t)blockIdx.x * RT + threadIdx.x; i < n; i += (size_t)gridDim.x * RT) {
+        const float2 x = f[i];
+        const float2 y = d[i];
+        const float dd = D[i] * dscale;
+        const double t0 = data_term(hypotf(x.x, x.y), dd, model);
+#pragma unroll
+        for (int j = 0; j < MAXK; ++j) {
+            if (j < J) {
+                const float2 v = make_float2(x.x + gj[j] * y.x, x.y + gj[j] * y.y);
+                acc[j] += t0 - data_term(hypotf(v.x, v.y), dd, model);
+            }
+        }
+    }
+    block_reduce_store<MAXK>(acc, work, blockIdx.x, gridDim.x);
+}
+
+// Lagrangian data term, solver.py:294-298.  Poisson also subtracts the
+// minimum d - 2 d log(sqrt d) so the term is >= 0.
+__global__ void __launch_bounds__(RT) k_lagr_frames(const float2 *__restrict__ f, const float *__restrict__ D,
+                                                    float dscale, size_t n, int model, double *__restrict__ work)
+{
+    double acc[1] = {0};
+    for (size_t i = (size_t)blockIdx.x * RT + threadIdx.x; i < n; i += (size_t)gridDim.x * RT) {
+        const float2 x = f[i];
+        const float dd = D[i] * dscale;
+        const float a = sqrtf(x.x * x.x + x.y * x.y);
+        if (model == 0) {
+            const float sq = sqrtf(dd);
+            acc[0] += (double)a * a - 2.0 * dd * (double)logf(fmaxf(a, 1e-32f)) -
+                      ((double)dd - 2.0 * dd * (double)logf(fmaxf(sq, 1e-32f)));
+        } else {
+            const double t = (double)a - (double)sqrtf(dd);
+            acc[0] += t * t;
+        }
+    }
+    block_reduce_store<1>(acc, work, blockIdx.x, gridDim.x);
+}
+
+// ---- elementwise ----------------------------------------------------------
+struct Lin4 {
+    const float2 *x[4];
+    float2 c[4];
+};
+
+// out = sum_{i<k} c_i x_i  (out may alias any x_i)
+__global__ void k_lincomb(float2 *__restrict__ out, size_t n, int k, Lin4 p)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float2 acc = czero();
+        for (int j = 0; j < k; ++j) acc = acc + cmul(p.c[j], p.x[j][i]);
+        out[i] = acc;
+    }
+}
+
+// mode 0: out = a * b;  mode 1: out = conj(a) * (b - c);  mode 2: out = conj(a) * b
+__global__ void k_cmul(float2 *__restrict__ out, const float2 *__restrict__ a, const float2 *__restrict__ b,
+                       const float2 *__restrict__ c, size_t n, int mode)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float2 x = a[i];
+        float2 y = b[i];
+        if (mode == 1) y = y - c[i];
+        out[i] = mode == 0 ? cmul(x, y) : cmulc(x, y);
+    }
+}
+
+// out = exp(i s x) * exp(i phi)   (exptomo, solver.py:59-60; h update, :322)
+__global__ void k_expmap(float2 *__restrict__ out, const float2 *__restrict__ x, size_t n, float s, float phi)
+{
+    float cp, sp;
+    sincosf(phi, &sp, &cp);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float2 v = x[i];
+        const float mag = expf(-s * v.y);
+        float sn, cs;
+        sincosf(s * v.x, &sn, &cs);
+        out[i] = cmul(make_float2(mag * cs, mag * sn), make_float2(cp, sp));
+    }
+}
+
+// out = c * mlog(x),  mlog: |x| < 1e-32 -> 1e-32, then complex log (solver.py:48-52)
+__global__ void k_logmap(float2 *__restrict__ out, const float2 *__restrict__ x, size_t n, float2 c)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float2 v = x[i];
+        const float a = hypotf(v.x, v.y);
+        if (a < 1e-32f) v = make_float2(1e-32f, 0.f);
+        const float2 l = make_float2(logf(fmaxf(a, 1e-32f)), a < 1e-32f ? 0.f : atan2f(v.y, v.x));
+        out[i] = cmul(c, l);
+    }
+}
+
+// takexi second half (solver.py:163-166) with t given and tmax = max|t|:
+//   K = i t / tmax;  xi0 = K * (-i mlog(t) / (voxel k)) * coeftomo
+__global__ void k_takexi(float2 *__restrict__ K, float2 *__restrict__ xi0, const float2 *__restrict__ t, size_t n,
+                         float inv_tmax, float cxi)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float2 v = t[i];
+        const float kx = -v.y * inv_tmax, ky = v.x * inv_tmax;   // i t / tmax
+        const float a = hypotf(v.x, v.y);
+        if (a < 1e-32f) v = make_float2(1e-32f, 0.f);
+        const float lr = logf(fmaxf(a, 1e-32f)), li = a < 1e-32f ? 0.f : atan2f(v.y, v.x);
+        // -i * log(t) * cxi = (li - i lr) * cxi
+        const float2 m = make_float2(li * cxi, -lr * cxi);
+        K[i] = make_float2(kx, ky);
+        xi0[i] = cmul(make_float2(kx, ky), m);
+    }
+}
+
+// gradient residual of the ptycho data term (solver.py:220-224), D scaled by dscale:
+//   Poisson  r = f - D f / (|f|^2 + 1e-32)
+//   Gaussian r = f - sqrt(D) exp(i angle(f))
+__global__ void k_residual(float2 *__restrict__ out, const float2 *__restrict__ f, const float *__restrict__ D,
+                           float dscale, size_t n, int model)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float2 x = f[i];
+        const float dd = D[i] * dscale;
+        float2 r;
+        if (model == 0) {
+            const float q = dd / (x.x * x.x + x.y * x.y + 1e-32f);
+            r = make_float2(x.x - q * x.x, x.y - q * x.y);
+        } else {
+            const float ang = atan2f(x.y, x.x);
+            float sn, cs;
+            sincosf(ang, &sn, &cs);
+            const float sq = sqrtf(dd);
+            r = make_float2(x.x - sq * cs, x.y - sq * sn);
+        }
+        out[i] = r;
+    }
+}
+
+// out = |x|^2 * scale   (fwd_ptycho_batch intensities, solver.py:115)
+__global__ void k_abs2(float *__restrict__ out, const float2 *__restrict__ x, size_t n, float scale)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float2 v = x[i];
+        out[i] = (v.x * v.x + v.y * v.y) * scale;
+    }
+}
+
+// ---- TV regulariser J, J* (solver.py:128-146) --------------------------------
+// u [nz][ny][nx]; res [3][nz][ny][nx]: forward differences along x, y, z times s
+__global__ void k_reg_fwd(float2 *__restrict__ res, const float2 *__restrict__ u, int nz, int ny, int nx, float s)
+{
+    const size_t vol = (size_t)nz * ny * nx;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < vol; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        const float2 c = u[i];
+        res[i] = x < nx - 1 ? s * (u[i + 1] - c) : czero();
+        res[vol + i] = y < ny - 1 ? s * (u[i + nx] - c) : czero();
+        res[2 * vol + i] = z < nz - 1 ? s * (u[i + (size_t)nx * ny] - c) : czero();
+    }
+}
+
+__global__ void k_reg_adj(float2 *__restrict__ res, const float2 *__restrict__ g, int nz, int ny, int nx, float s)
+{
+    const size_t vol = (size_t)nz * ny * nx;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < vol; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        const float2 *g0 = g, *g1 = g + vol, *g2 = g + 2 * vol;
+        float2 r = x > 0 ? g0[i] - g0[i - 1] : g0[i];
+        r = r + (y > 0 ? g1[i] - g1[i - nx] : g1[i]);
+        r = r + (z > 0 ? g2[i] - g2[i - (size_t)nx * ny] : g2[i]);
+        res[i] = s * r;
+    }
+}
+
+// solve_reg (solver.py:257-264): z = J u + mu/tau, isotropic soft threshold alpha/tau
+__global__ void k_solve_reg(float2 *__restrict__ z, const float2 *__restrict__ u, const float2 *__restrict__ mu,
+                            int nz, int ny, int nx, float s, float inv_tau, float thr)
+{
+    const size_t vol = (size_t)nz * ny * nx;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < vol; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), zz = (int)(i / ((size_t)nx * ny));
+        const float2 c = u[i];
+        float2 v0 = x < nx - 1 ? s * (u[i + 1] - c) : czero();
+        float2 v1 = y < ny - 1 ? s * (u[i + nx] - c) : czero();
+        float2 v2 = zz < nz - 1 ? s * (u[i + (size_t)nx * ny] - c) : czero();
+        v0 = v0 + inv_tau * mu[i];
+        v1 = v1 + inv_tau * mu[vol + i];
+        v2 = v2 + inv_tau * mu[2 * vol + i];
+        const float za = sqrtf(v0.x * v0.x + v0.y * v0.y + v1.x * v1.x + v1.y * v1.y + v2.x * v2.x + v2.y * v2.y);
+        if (za <= thr) {
+            v0 = v1 = v2 = czero();
+        } else {
+            const float f = thr / za;
+            v0 = v0 - f * v0;
+            v1 = v1 - f * v1;
+            v2 = v2 - f * v2;
+        }
+        z[i] = v0;
+        z[vol + i] = v1;
+        z[2 * vol + i] = v2;
+    }
+}
+
+unsigned ew_blocks(size_t n)
+{
+    size_t b = (n + 255) / 256;
+    return (unsigned)(b < 148 * 16 ? (b ? b : 1) : 148 * 16);
+}
+
+}  // namespace
+
+extern "C" size_t pt_reduce_workspace_bytes(void) { return (size_t)RB * MAXK * sizeof(double); }
+
+extern "C" int pt_reduce_c64(int op, const void *a, const void *b, size_t n, int c0, int c1, int ncol, void *work,
+                             void *out, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(op >= 0 && op <= 7, "reduce: unknown op %d", op);
+    PT_CHECK_ARG(a && work && out, "reduce: null pointer");
+    PT_CHECK_ARG((op != 1 && op != 2 && op != 5) || b, "reduce: op %d needs two arrays", op);
+    PT_CHECK_ARG(op != 4 || (ncol > 0 && c0 >= 0 && c1 <= ncol), "reduce: bad column band");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int K = op == 1 ? 2 : (op == 2 ? 3 : 1);
+    k_reduce<<<RB, RT, 0, st>>>(op, (const float2 *)a, (const float2 *)b, n, c0, c1, ncol, (double *)work);
+    PT_LAUNCHED("k_reduce");
+    k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, K, RB, op == 3 || op == 7);
+    PT_LAUNCHED("k_finish");
+    return PT_OK;
+}
+
+extern "C" int pt_ls_frames(const void *f, const void *d, const float *data, float dscale, size_t n, int model,
+                            const double *gammas, int J, void *work, void *out, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(f && d && data && gammas && work && out, "ls_frames: null pointer");
+    PT_CHECK_ARG(J >= 1 && J <= MAXK, "ls_frames: 1 <= J <= %d", MAXK);
+    PT_CHECK_ARG(model == 0 || model == 1, "ls_frames: model 0 (poisson) or 1 (gaussian)");
+    cudaStream_t st = (cudaStream_t)stream;
+    k_ls_frames<<<RB, RT, 0, st>>>((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J,
+                                   (double *)work);
+    PT_LAUNCHED("k_ls_frames");
+    k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, J, RB, 0);
+    PT_LAUNCHED("k_finish");
+    return PT_OK;
+}
+
+extern "C" int pt_lagr_frames(const void *f, const float *data, float dscale, size_t n, int model, void *work,
+                              void *out, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(f && data && work && out, "lagr_frames: null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    k_lagr_frames<<<RB, RT, 0, st>>>((const float2 *)f, data, dscale, n, model, (double *)work);
+    PT_LAUNCHED("k_lagr_frames");
+    k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, 1, RB, 0);
+    PT_LAUNCHED("k_finish");
+    return PT_OK;
+}
+
+extern "C" int pt_lincomb_c64(void *out, size_t n, int k, const void *const *x, const float *coef, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(out && x && coef && k >= 1 && k <= 4, "lincomb: 1..4 terms");
+    Lin4 p;
+    for (int j = 0; j < 4; ++j) {
+        p.x[j] = j < k ? (const float2 *)x[j] : nullptr;
+        p.c[j] = j < k ? make_float2(coef[2 * j], coef[2 * j + 1]) : czero();
+        PT_CHECK_ARG(j >= k || p.x[j], "lincomb: null term %d", j);
+    }
+    k_lincomb<<<ew_blocks(n), 256, 0, (cudaStream_t)stream>>>((float2 *)out, n, k, p);
+    PT_LAUNCHED("k_lincomb");
+    return PT_OK;
+}
+
+extern "C" int pt_cmul_c64(void *out, const void *a, const void *b, const void *c, size_t n, int mode, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(out && a && b && (mode != 1 || c) && mode >= 0 && mode <= 2, "cmul: bad arguments");
+    k_cmul<<<ew_blocks(n), 256, 0, (cudaStream_t)stream>>>((float2 *)out, (const float2 *)a, (const float2 *)b,
+                                                           (const float2 *)c, n, mode);
+    PT_LAUNCHED("k_cmul");
+    return PT_OK;
+}
+
+extern "C" int pt_expmap_c64(void *out, const void *x, size_t n, float s, float phi, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(out && x, "expmap: null pointer");
+    k_expmap<<<ew_blocks(n), 256, 0, (cudaStream_t)stream>>>((float2 *)out, (const float2 *)x, n, s, phi);
+    PT_LAUNCHED("k_expmap");
+    return PT_OK;
+}
+
+extern "C" int pt_logmap_c64(void *out, const void *x, size_t n, float cre, float cim, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(out && x, "logmap: null pointer");
+    k_logmap<<<ew_blocks(n), 256, 0, (cudaStream_t)stream>>>((float2 *)out, (const float2 *)x, n,
+                                                             make_float2(cre, cim));
+    PT_LAUNCHED("k_logmap");
+    return PT_OK;
+}
+
+extern "C" int pt_takexi_c64(void *K, void *xi0, const void *t, size_t n, float inv_tmax, float cxi, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(K && xi0 && t, "takexi: null pointer");
+    k_takexi<<<ew_blocks(n), 256, 0, (cudaStream_t)stream>>>((float2 *)K, (float2 *)xi0, (const float2 *)t, n,
+                                                             inv_tmax, cxi);
+    PT_LAUNCHED("k_takexi");
+    return PT_OK;
+}
+
+extern "C" int pt_reg_fwd_c64(void *res, const void *u, int nz, int ny, int nx, float s, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(res && u && nz > 0 && ny > 0 && nx > 0, "reg_fwd: bad arguments");
+    k_reg_fwd<<<ew_blocks((size_t)nz * ny * nx), 256, 0, (cudaStream_t)stream>>>((float2 *)res, (const float2 *)u,
+                                                                                  nz, ny, nx, s);
+    PT_LAUNCHED("k_reg_fwd");
+    return PT_OK;
+}
+
+extern "C" int pt_reg_adj_c64(void *res, const void *g, int nz, int ny, int nx, float s, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(res && g && nz > 0 && ny > 0 && nx > 0, "reg_adj: bad arguments");
+    k_reg_adj<<<ew_blocks((size_t)nz * ny * nx), 256, 0, (cudaStream_t)stream>>>((float2 *)res, (const float2 *)g,
+                                                                                  nz, ny, nx, s);
+    PT_LAUNCHED("k_reg_adj");
+    return PT_OK;
+}
+
+extern "C" int pt_solve_reg_c64(void *z, const void *u, const void *mu, int nz, int ny, int nx, float s,
+                                float inv_tau, float thr, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(z && u && mu && nz > 0 && ny > 0 && nx > 0, "solve_reg: bad arguments");
+    k_solve_reg<<<ew_blocks((size_t)nz * ny * nx), 256, 0, (cudaStream_t)stream>>>(
+        (float2 *)z, (const float2 *)u, (const float2 *)mu, nz, ny, nx, s, inv_tau, thr);
+    PT_LAUNCHED("k_solve_reg");
+    return PT_OK;
+}
+
+extern "C" int pt_residual_c64(void *out, const void *f, const float *data, float dscale, size_t n, int model,
+                               void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(out && f && data && (model == 0 || model == 1), "residual: bad arguments");
+    k_residual<<<ew_blocks(n), 256, 0, (cudaStream_t)stream>>>((float2 *)out, (const float2 *)f, data, dscale, n,
+                                                               model);
+    PT_LAUNCHED("k_residual");
+    return PT_OK;
+}
+
+extern "C" int pt_abs2_c64(float *out, const void *x, size_t n, float scale, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(out && x, "abs2: null pointer");
+    k_abs2<<<ew_blocks(n), 256, 0, (cudaStream_t)stream>>>(out, (const float2 *)x, n, scale);
+    PT_LAUNCHED("k_abs2");
+    return PT_OK;
+}

@@ -1,0 +1,363 @@
+"""Drop-in ADMM ptycho-tomography Solver on torch CUDA tensors.
+
+Same constructor and methods as the reference Solver
+(src/ptychotomo/solver.py:19-336); arrays are torch CUDA tensors
+(complex64 / float32) instead of CuPy arrays.  Every arithmetic step runs in
+libptychotomo_b200.so: the USFFT and ptycho operators, and the Solver
+kernels (linear combinations, TV, exp/log maps, FP64 reductions).  torch
+only allocates memory.
+
+Differences from the reference, all deliberate:
+* reductions (norms, inner products, the Poisson log-likelihood, the
+  Lagrangian) accumulate in FP64;
+* the line searches evaluate the decrease minf(x) - minf(x + g d) directly:
+  quadratic terms in closed form (||w + g d||^2 - ||w||^2 = 2 g Re<w, d> +
+  g^2 ||d||^2) and the Poisson / Gaussian term per element in FP64 for up to
+  16 step lengths per pass.  They take the halving decisions of
+  solver.py:171-177 exactly, except where the decrease is within FP32
+  rounding of zero (near convergence), where the reference's own float
+  atomics make it differ from run to run;
+* takexi uses r = prb.shape[0] // 2 (solver.py:151 slices with a float);
+* a CG loop stops once its line search returns gamma = 0 (gamma only
+  halves, so the iterate cannot change any more; the reference would divide
+  by an exactly-zero Dai-Yuan denominator next and return NaN), and a zero
+  Dai-Yuan denominator gives beta = 0;
+* fwd_ptycho_batch returns a device tensor; admm accepts data on the host
+  or the device and keeps it resident on the device;
+* all angles / slices of a *_batch call go through one operator launch
+  (the reference loops over ptheta / pnz chunks; results are identical).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import kernels as K
+from .operators import ptychofft, radonusfft
+
+PLANCK_CONSTANT = 6.58211928e-19  # [keV*s]  solver.py:15
+SPEED_OF_LIGHT = 299792458e+2    # [cm/s]   solver.py:16
+
+_MODELS = {"poisson": 0, "gaussian": 1}
+
+
+def _dev_tensor(x, dtype, device):
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.asarray(x), dtype=dtype, device=device).contiguous()
+
+
+class Solver:
+    def __init__(self, prb, scan, theta, det, voxelsize, energy, ntheta, nz, n, ptheta, pnz, device=None):
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        dev = self.device
+        self.voxelsize = voxelsize
+        self.energy = energy
+        self.scan = _dev_tensor(scan, torch.float32, dev)
+        self.prb = _dev_tensor(prb, torch.complex64, dev)
+        self.theta = _dev_tensor(theta, torch.float32, dev)
+        self.ntheta, self.nz, self.n = ntheta, nz, n
+        self.nscan = self.scan.shape[2]
+        self.ndety, self.ndetx = det[0], det[1]
+        self.nprb = self.prb.shape[0]
+        self.ptheta, self.pnz = ptheta, pnz
+        if ntheta % ptheta or nz % pnz:
+            raise ValueError("ptheta must divide ntheta and pnz must divide nz (solver.py:86,111)")
+        # tomography: the pnz-chunk operator of fwd_tomo/adj_tomo and one for whole batches
+        self.cl_tomo = radonusfft(ntheta, pnz, n)
+        self.cl_tomo.setobj(self.theta)
+        if pnz == nz:
+            self._tomo_all = self.cl_tomo
+        else:
+            self._tomo_all = radonusfft(ntheta, nz, n)
+            self._tomo_all.setobj(self.theta)
+        # ptychography: one operator per angle chunk, its scans set once
+        self._ptycho = []
+        for k in range(ntheta // ptheta):
+            op = ptychofft(ptheta, nz, n, ptheta, self.nscan, self.ndety, self.ndetx, self.nprb)
+            op.setobj(self.scan[:, k * ptheta:(k + 1) * ptheta].contiguous(), self.prb)
+            self._ptycho.append(op)
+        self.cl_ptycho = self._ptycho[0]
+        if ptheta != ntheta:
+            self._ptycho_all = ptychofft(ntheta, nz, n, ntheta, self.nscan, self.ndety, self.ndetx, self.nprb)
+            self._ptycho_all.setobj(self.scan, self.prb)
+        else:
+            self._ptycho_all = self.cl_ptycho
+        # normalization coefficients, solver.py:43-46 (float32 like the reference)
+        self.red = K.Reducer(dev)
+        amax = self.red.maxabs(self.prb)
+        self.coeftomo = float(np.float32(1 / np.float32(np.sqrt(ntheta * n / 2))))
+        self.coefptycho = float(np.float32(1 / np.float32(amax)))
+        self.coefdata = float(np.float32(1 / (self.ndetx * self.ndety * np.float32(amax) ** 2)))
+
+    # ---- helpers ----------------------------------------------------------
+    def _empty(self, shape, dtype=torch.complex64):
+        return torch.empty(shape, dtype=dtype, device=self.device)
+
+    def _ids(self, k):
+        return slice(k * self.ptheta, (k + 1) * self.ptheta)
+
+    # ---- maps, solver.py:48-64 --------------------------------------------
+    def mlog(self, psi):
+        return K.logmap(torch.empty_like(psi), psi, 1.0)
+
+    def wavenumber(self):
+        return 2 * np.pi / (2 * np.pi * PLANCK_CONSTANT * SPEED_OF_LIGHT / self.energy)
+
+    def exptomo(self, psi):
+        return K.expmap(torch.empty_like(psi), psi, self.voxelsize * self.wavenumber() / self.coeftomo)
+
+    def logtomo(self, psi):
+        c = -1j / self.wavenumber() / self.voxelsize * self.coeftomo
+        return K.logmap(torch.empty_like(psi), psi, c)
+
+    # ---- tomography, solver.py:67-97 --------------------------------------
+    def fwd_tomo(self, u):
+        res = self._empty([self.ntheta, self.pnz, self.n])
+        self.cl_tomo.fwd(res, u, scale=self.coeftomo)
+        return res
+
+    def adj_tomo(self, data):
+        res = self._empty([self.pnz, self.n, self.n])
+        self.cl_tomo.adj(res, data, scale=self.coeftomo)
+        return res
+
+    def fwd_tomo_batch(self, u):
+        res = self._empty([self.ntheta, self.nz, self.n])
+        self._tomo_all.fwd(res, u, scale=self.coeftomo)
+        return res
+
+    def adj_tomo_batch(self, data):
+        res = self._empty([self.nz, self.n, self.n])
+        self._tomo_all.adj(res, data, scale=self.coeftomo)
+        return res
+
+    # ---- ptychography, solver.py:100-125 ----------------------------------
+    def fwd_ptycho(self, psi):
+        """FQ psi on the current angle chunk (self.cl_ptycho)."""
+        res = self._empty([self.ptheta, self.nscan, self.ndety, self.ndetx])
+        self.cl_ptycho.fwd(res, psi, scale=self.coefptycho)
+        return res
+
+    def fwd_ptycho_batch(self, psi):
+        """|FQ psi|^2 / coefdata for all angles (a device float32 tensor)."""
+        frames = self._empty([self.ntheta, self.nscan, self.ndety, self.ndetx])
+        self._ptycho_all.fwd(frames, psi, scale=self.coefptycho)
+        data = self._empty(frames.shape, torch.float32)
+        return K.abs2(data, frames, 1.0 / self.coefdata)
+
+    def adj_ptycho(self, data):
+        res = self._empty([self.ptheta, self.nz, self.n])
+        self.cl_ptycho.adj(res, data, scale=self.coefptycho)
+        return res
+
+    # ---- TV, solver.py:128-146 --------------------------------------------
+    def fwd_reg(self, u):
+        return K.reg_fwd(self._empty([3, *u.shape]), u, np.float32(2 / np.sqrt(3)))
+
+    def adj_reg(self, gr):
+        return K.reg_adj(self._empty(gr.shape[1:]), gr, np.float32(-2 / np.sqrt(3)))
+
+    # ---- linearisation, solver.py:149-168 ---------------------------------
+    def takexi(self, psi, phi, lamd, mu, rho, tau):
+        r = self.prb.shape[0] // 2
+        ncols = psi.shape[2]
+        cnt = psi.numel() // ncols * r
+        m1 = self.red.angle_band_sum(psi, r, 2 * r) / cnt
+        m2 = self.red.angle_band_sum(psi, ncols - 2 * r, ncols - r) / cnt
+        pshift = (m1 + m2) / 2
+        e = complex(math.cos(-pshift), math.sin(-pshift))
+        t = K.lincomb(torch.empty_like(psi), [(e, psi), (-e / rho, lamd)])
+        tmax = self.red.maxabs(t)
+        Kt, xi0 = torch.empty_like(psi), torch.empty_like(psi)
+        K.takexi(Kt, xi0, t, tmax, self.coeftomo / (self.voxelsize * self.wavenumber()))
+        xi1 = K.lincomb(torch.empty_like(phi), [(1.0, phi), (-1.0 / tau, mu)])
+        return xi0, xi1, Kt, pshift
+
+    # ---- line search, solver.py:171-177 -----------------------------------
+    def line_search(self, minf, gamma, u, fu, d, fd):
+        """Generic backtracking with a user functional, as in the reference."""
+        while minf(u, fu) - minf(u + gamma * d, fu + gamma * fd) < 0 and gamma > 1e-12:
+            gamma *= 0.5
+        if gamma <= 1e-12:
+            gamma = 0
+        return gamma
+
+    trace = None   # list: records (kind, gamma) of every CG line search when set
+
+    @staticmethod
+    def _halve_until(gamma, decrease):
+        """Same decisions as solver.py:172-177 given decrease(g) = minf(0) - minf(g)."""
+        while decrease(gamma) < 0 and gamma > 1e-12:
+            gamma *= 0.5
+        return 0 if gamma <= 1e-12 else gamma
+
+    # ---- CG tomography, solver.py:180-203 ---------------------------------
+    def cg_tomo(self, xi0, xi1, Kt, init, rho, tau, titer):
+        red = self.red
+        u = init.clone()
+        gamma = 2
+        grad0 = d = None
+        a = torch.empty_like(xi0)
+        for i in range(titer):
+            KRu = K.cmul(torch.empty_like(xi0), Kt, self.fwd_tomo_batch(u))
+            gu = self.fwd_reg(u)
+            K.lincomb(a, [(1.0, KRu), (-1.0, xi0)])                       # K R u - xi0
+            b = K.lincomb(gu, [(1.0, gu), (-1.0, xi1)])                   # J u - xi1 (in place)
+            ga = self.adj_tomo_batch(K.cmul(torch.empty_like(a), Kt, a, mode=2))
+            grad = K.lincomb(ga, [(rho, ga), (tau, self.adj_reg(b))])
+            if i == 0:
+                d = K.lincomb(torch.empty_like(grad), [(-1.0, grad)])
+            else:
+                den = red.dot(d, grad) - red.dot(d, grad0)
+                beta = red.norm2(grad) / den if den != 0 else 0.0
+                K.lincomb(d, [(-1.0, grad), (beta, d)])
+            grad0 = grad
+            fd = K.cmul(torch.empty_like(xi0), Kt, self.fwd_tomo_batch(d))
+            gd = self.fwd_reg(d)
+            _, a_fd, fd2 = red.quad3(a, fd)
+            _, b_gd, gd2 = red.quad3(b, gd)
+            c1 = rho * a_fd + tau * b_gd
+            c2 = rho * fd2 + tau * gd2
+            gamma = self._halve_until(gamma, lambda g: -(2 * g * c1 + g * g * c2))
+            if self.trace is not None:
+                self.trace.append(("tomo", gamma))
+            K.lincomb(u, [(1.0, u), (gamma, d)])
+            if gamma == 0:
+                break   # gamma only halves: u can no longer change in this call
+        return u
+
+    # ---- CG ptychography, solver.py:206-254 -------------------------------
+    def cg_ptycho(self, data, init, h, lamd, rho, piter, model, dscale=1.0):
+        """CG on the current angle chunk; data are raw counts times dscale."""
+        red = self.red
+        mdl = _MODELS[model]
+        psi = init.clone()
+        gamma = 2
+        grad0 = d = None
+        w = torch.empty_like(psi)
+        for i in range(piter):
+            fpsi = self.fwd_ptycho(psi)
+            res = K.residual(torch.empty_like(fpsi), fpsi, data, dscale, mdl)
+            grad = self.adj_ptycho(res)
+            del res
+            K.lincomb(w, [(1.0, h), (-1.0, psi), (1.0 / rho, lamd)])     # h - psi + lamd/rho
+            K.lincomb(grad, [(1.0, grad), (-rho, w)])
+            if i == 0:
+                d = K.lincomb(torch.empty_like(grad), [(-1.0, grad)])
+            else:
+                den = red.dot(d, grad) - red.dot(d, grad0)
+                beta = red.norm2(grad) / den if den != 0 else 0.0
+                K.lincomb(d, [(-1.0, grad), (beta, d)])
+            grad0 = grad
+            fd = self.fwd_ptycho(d)
+            _, w_d, d2 = red.quad3(w, d)
+            # minf(psi) - minf(psi + g d) = data-term decrease (per element, FP64)
+            #   + rho (2 g Re<w, d> - g^2 ||d||^2)  for the penalty rho ||w - g d||^2
+            while True:
+                gs = [gamma * 0.5 ** j for j in range(16)]
+                vals = red.ls_frames(fpsi, fd, data, dscale, mdl, gs)
+                chosen = None
+                for g, dec_data in zip(gs, vals):
+                    dec = dec_data + rho * (2 * g * w_d - g * g * d2)
+                    if not (dec < 0 and g > 1e-12):
+                        chosen = g
+                        break
+                if chosen is not None:
+                    gamma = 0 if chosen <= 1e-12 else chosen
+                    break
+                gamma = gs[-1] * 0.5
+            if self.trace is not None:
+                self.trace.append(("ptycho", gamma))
+            K.lincomb(psi, [(1.0, psi), (gamma, d)])
+            del fpsi, fd
+            if gamma == 0:
+                break   # gamma only halves: psi can no longer change in this call
+        if red.maxangle(psi) > 3.14:
+            print("possible phase wrap, max computed angle", red.maxangle(psi))
+        return psi
+
+    def cg_ptycho_batch(self, data, init, h, lamd, rho, piter, model):
+        data = self._as_data(data)
+        if self.ptheta == self.ntheta:
+            self.cl_ptycho = self._ptycho[0]
+            return self.cg_ptycho(data, init, h, lamd, rho, piter, model, dscale=self.coefdata)
+        psi = init.clone()
+        for k in range(self.ntheta // self.ptheta):
+            ids = self._ids(k)
+            self.cl_ptycho = self._ptycho[k]
+            psi[ids] = self.cg_ptycho(data[ids], psi[ids].contiguous(), h[ids].contiguous(),
+                                      lamd[ids].contiguous(), rho, piter, model, dscale=self.coefdata)
+        return psi
+
+    def _as_data(self, data):
+        if isinstance(data, torch.Tensor) and data.is_cuda and data.dtype == torch.float32 and data.is_contiguous():
+            return data
+        return _dev_tensor(data, torch.float32, self.device)
+
+    # ---- regulariser, penalties, monitor, solver.py:257-305 ---------------
+    def solve_reg(self, u, mu, tau, alpha):
+        z = self._empty([3, *u.shape])
+        return K.solve_reg(z, u, mu, np.float32(2 / np.sqrt(3)), 1.0 / tau, alpha / tau)
+
+    def update_penalty(self, psi, h, h0, phi, e, e0, rho, tau):
+        r = self.red.norm2_diff(psi, h)
+        s = rho * rho * self.red.norm2_diff(h, h0)
+        if r > 10 * s:
+            rho *= 2
+        elif s > 10 * r:
+            rho *= 0.5
+        r = self.red.norm2_diff(phi, e)
+        s = tau * tau * self.red.norm2_diff(e, e0)
+        if r > 10 * s:
+            tau *= 2
+        elif s > 10 * r:
+            tau *= 0.5
+        return rho, tau
+
+    def take_lagr(self, psi, phi, data, h, e, lamd, mu, alpha, rho, tau, model):
+        data = self._as_data(data)
+        red = self.red
+        lagr = np.zeros(7)
+        for k in range(self.ntheta // self.ptheta):
+            ids = self._ids(k)
+            self.cl_ptycho = self._ptycho[k]
+            fpsi = self.fwd_ptycho(psi[ids].contiguous())
+            lagr[0] += red.lagr_frames(fpsi, data[ids], self.coefdata, _MODELS[model])
+        lagr[1] = alpha * red.tv(phi)
+        lagr[2] = 2 * (red.dot(lamd, h) - red.dot(lamd, psi)).real
+        lagr[3] = rho * red.norm2_diff(h, psi)
+        lagr[4] = 2 * (red.dot(mu, e) - red.dot(mu, phi)).real
+        lagr[5] = tau * red.norm2_diff(e, phi)
+        lagr[6] = np.sum(lagr[0:5])  # the reference sums terms 0..4 (solver.py:304)
+        return lagr
+
+    # ---- ADMM, solver.py:308-336 ------------------------------------------
+    def admm(self, data, h, e, psi, phi, lamd, mu, u, alpha, piter, titer, niter, model, verbose=True,
+             history=None):
+        data = self._as_data(data)
+        rho, tau = 0.5, 0.5
+        for m in range(niter):
+            h0, e0 = h, e
+            psi = self.cg_ptycho_batch(data, psi, h, lamd, rho, piter + (m < 2) * 32, model)
+            xi0, xi1, Kt, pshift = self.takexi(psi, phi, lamd, mu, rho, tau)
+            u = self.cg_tomo(xi0, xi1, Kt, u, rho, tau, titer)
+            phi = self.solve_reg(u, mu, tau, alpha)
+            h = K.expmap(torch.empty_like(psi), self.fwd_tomo_batch(u),
+                         self.voxelsize * self.wavenumber() / self.coeftomo, pshift)
+            e = self.fwd_reg(u)
+            lamd = K.lincomb(torch.empty_like(lamd), [(1.0, lamd), (rho, h), (-rho, psi)])
+            mu = K.lincomb(torch.empty_like(mu), [(1.0, mu), (tau, e), (-tau, phi)])
+            rho, tau = self.update_penalty(psi, h, h0, phi, e, e0, rho, tau)
+            if history is not None:
+                history.append(dict(m=m, rho=rho, tau=tau))
+            if np.mod(m, 10) == 0 and (verbose or history is not None):
+                lagr = self.take_lagr(psi, phi, data, h, e, lamd, mu, alpha, rho, tau, model)
+                if history is not None:
+                    history[-1]["lagr"] = lagr
+                if verbose:
+                    print("%d/%d) rho=%.2e, tau=%.2e, Lagrangian terms:  %.2e %.2e %.2e %.2e %.2e %.2e, Sum: %.2e" %
+                          (m, niter, rho, tau, *lagr))
+        return u, psi
