@@ -118,6 +118,19 @@ int pt_reduce_c64(int op, const void *a, const void *b, size_t n, int c0, int c1
  * formed per element in FP64.  gammas: device double[J], J <= 16. */
 int pt_ls_frames(const void *f, const void *d, const float *data, float dscale, size_t n, int model,
                  const double *gammas, int J, void *work, void *out, void *stream);
+/* pt_ls_frames without allocating anything and without a workspace argument.
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory at call time: a host application whose memory pool owns the device
+ * memory, or a latency-bound loop that must not call cudaMalloc (which can
+ * synchronise the device) after start-up.  The scratch (148 KiB: 1184
+ * blocks x 16 FP64 partials) is a static device array of the library, held
+ * on every GPU that loads it until the process exits.  The first call on a
+ * device looks up the array's address (cudaGetSymbolAddress) and should be
+ * made before any stream capture.  J > 16 is rejected with PT_ERR_ARG.
+ * All calls share the scratch: calls that overlap on the GPU (different
+ * streams, or concurrent host threads) race and give wrong sums. */
+int pt_ls_frames_noalloc(const void *f, const void *d, const float *data, float dscale, size_t n, int model,
+                         const double *gammas, int J, void *out, void *stream);
 /* Lagrangian data term, solver.py:294-298 (D = dscale * data). */
 int pt_lagr_frames(const void *f, const float *data, float dscale, size_t n, int model, void *work, void *out,
                    void *stream);

@@ -504,3 +504,60 @@ extern "C" int pt_abs2_c64(float *out, const void *x, size_t n, float scale, voi
     PT_LAUNCHED("k_abs2");
     return PT_OK;
 }
+
+// ---- pt_ls_frames without any allocation ------------------------------------
+// Scratch of the reduction (one FP64 partial per block and step length) in a
+// file-scope device array: 1184 blocks x 16 step lengths x 8 B = 148 KiB, held
+// by every GPU that loads this library until the process exits.  Host code
+// cannot use the array's name as a device address, so its address is looked
+// up once per device with cudaGetSymbolAddress and cached.
+#include <mutex>
+
+namespace {
+static __device__ __align__(256) double g_ls_scratch[RB * MAXK];
+
+constexpr int MAX_DEVICES = 64;
+double *g_ls_scratch_ptr[MAX_DEVICES] = {};
+std::mutex g_ls_scratch_mu;
+
+int ls_scratch_for_current_device(double **ptr)
+{
+    int dev = -1;
+    PT_CUDA(cudaGetDevice(&dev));
+    PT_CHECK_ARG(dev >= 0 && dev < MAX_DEVICES, "ls_frames_noalloc: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_ls_scratch_mu);
+    if (!g_ls_scratch_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_ls_scratch);
+        if (e != cudaSuccess || !p) {
+            pt::set_error("ls_frames_noalloc: cudaGetSymbolAddress of the static scratch failed on device %d: %s",
+                          dev, cudaGetErrorString(e));
+            return PT_ERR_CUDA;
+        }
+        g_ls_scratch_ptr[dev] = (double *)p;
+    }
+    *ptr = g_ls_scratch_ptr[dev];
+    return PT_OK;
+}
+}  // namespace
+
+extern "C" int pt_ls_frames_noalloc(const void *f, const void *d, const float *data, float dscale, size_t n,
+                                    int model, const double *gammas, int J, void *out, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(f && d && data && gammas && out, "ls_frames_noalloc: null pointer");
+    PT_CHECK_ARG(J >= 1 && J <= MAXK,
+                 "ls_frames_noalloc: J = %d step lengths exceeds the static scratch (1 <= J <= %d)", J, MAXK);
+    PT_CHECK_ARG(model == 0 || model == 1, "ls_frames_noalloc: model 0 (poisson) or 1 (gaussian)");
+    double *work = nullptr;
+    const int rc = ls_scratch_for_current_device(&work);
+    if (rc != PT_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    // every partial that k_finish reads (J x RB) is written by k_ls_frames in
+    // this call, so nothing in the shared scratch needs clearing first
+    k_ls_frames<<<RB, RT, 0, st>>>((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J, work);
+    PT_LAUNCHED("k_ls_frames");
+    k_finish<<<1, RT, 0, st>>>(work, (double *)out, J, RB, 0);
+    PT_LAUNCHED("k_finish");
+    return PT_OK;
+}
