@@ -230,17 +230,21 @@ __global__ void __launch_bounds__(ZC * 32)
 }
 
 // ---- A2: column gather (transpose of the forward gather) + column IFFT ----
-// grid (nzp / 16, G); block = 16 FFTs x T threads.  One warp per grid cell:
-// lanes 0-15 and 16-31 take alternate entries of the cell's list for 16
-// slices and are combined at the end (fixed order -> deterministic).
+// grid (nzp / 16, G); block = 16 FFTs x T threads.  A warp owns 4 consecutive
+// cells (a "cell group") of the column at a time; the group's list holds every
+// polar point whose kernel window covers any of the 4 cells, with the 4
+// weights (0 where the window misses a cell), in increasing point order.
+// Lanes 0-15 / 16-31 = 16 slices x 2 entry streams, combined at the end in a
+// fixed order -> deterministic.  Each loaded g value feeds 4 accumulators.
 constexpr int ZQ = 16;
+constexpr int CG = 4;  // cells per group
 template <int G>
-__global__ void __launch_bounds__(ZQ *fft_threads<G>())
-    k_adj_colgather(const float2 *__restrict__ lines, float2 *__restrict__ rbuf, const int *__restrict__ cell_off,
-                    const int2 *__restrict__ entries, const int *__restrict__ col_order, int nzp,
-                    const float2 *__restrict__ tw)
+__global__ void __launch_bounds__(ZQ *fft_threads<G>(), (G >= 1024 ? 1 : 2))
+    k_adj_colgather(const float2 *__restrict__ lines, float2 *__restrict__ rbuf, const int *__restrict__ goff,
+                    const int *__restrict__ gpt, const float4 *__restrict__ gw, const int *__restrict__ col_order,
+                    int nzp, const float2 *__restrict__ tw)
 {
-    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, PITCH = G + 1;
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, PITCH = G + 1, NG4 = G / CG;
     constexpr int Y0 = N / 2 + N / 6;
     constexpr int U = 4;  // entries in flight per lane
     extern __shared__ float2 sm[];
@@ -250,35 +254,60 @@ __global__ void __launch_bounds__(ZQ *fft_threads<G>())
     const int s = lane >> 4, zl = lane & 15;
     const int nwarps = blockDim.x >> 5;
     const float2 *lz = lines + z0 + zl;
-    for (int ky = warp; ky < G; ky += nwarps) {
-        const int cell = ky * G + kx;
-        const int beg = cell_off[cell], end = cell_off[cell + 1];
-        float2 acc = czero();
+    for (int gi = warp; gi < NG4; gi += nwarps) {
+        const int beg = goff[kx * NG4 + gi], end = goff[kx * NG4 + gi + 1];
+        float2 acc[CG];
+#pragma unroll
+        for (int c = 0; c < CG; ++c) acc[c] = czero();
         int e = beg + s;
         for (; e + 2 * (U - 1) < end; e += 2 * U) {
-            int2 en[U];
+            int pp[U];
+            float4 w[U];
             float2 v[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) en[u] = __ldg(&entries[e + 2 * u]);
+            for (int u = 0; u < U; ++u) {
+                pp[u] = __ldg(&gpt[e + 2 * u]);
+                w[u] = __ldg(&gw[e + 2 * u]);
+            }
 #pragma unroll
-            for (int u = 0; u < U; ++u) v[u] = __ldg(lz + (size_t)en[u].x * nzp);
+            for (int u = 0; u < U; ++u) v[u] = __ldg(lz + (size_t)pp[u] * nzp);
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const float w = __int_as_float(en[u].y);
-                acc.x = fmaf(w, v[u].x, acc.x);
-                acc.y = fmaf(w, v[u].y, acc.y);
+                acc[0].x = fmaf(w[u].x, v[u].x, acc[0].x);
+                acc[0].y = fmaf(w[u].x, v[u].y, acc[0].y);
+                acc[1].x = fmaf(w[u].y, v[u].x, acc[1].x);
+                acc[1].y = fmaf(w[u].y, v[u].y, acc[1].y);
+                acc[2].x = fmaf(w[u].z, v[u].x, acc[2].x);
+                acc[2].y = fmaf(w[u].z, v[u].y, acc[2].y);
+                acc[3].x = fmaf(w[u].w, v[u].x, acc[3].x);
+                acc[3].y = fmaf(w[u].w, v[u].y, acc[3].y);
             }
         }
         for (; e < end; e += 2) {
-            const int2 en = __ldg(&entries[e]);
-            const float w = __int_as_float(en.y);
-            const float2 v = __ldg(lz + (size_t)en.x * nzp);
-            acc.x = fmaf(w, v.x, acc.x);
-            acc.y = fmaf(w, v.y, acc.y);
+            const int pp = __ldg(&gpt[e]);
+            const float4 w = __ldg(&gw[e]);
+            const float2 v = __ldg(lz + (size_t)pp * nzp);
+            acc[0].x = fmaf(w.x, v.x, acc[0].x);
+            acc[0].y = fmaf(w.x, v.y, acc[0].y);
+            acc[1].x = fmaf(w.y, v.x, acc[1].x);
+            acc[1].y = fmaf(w.y, v.y, acc[1].y);
+            acc[2].x = fmaf(w.z, v.x, acc[2].x);
+            acc[2].y = fmaf(w.z, v.y, acc[2].y);
+            acc[3].x = fmaf(w.w, v.x, acc[3].x);
+            acc[3].y = fmaf(w.w, v.y, acc[3].y);
         }
-        acc.x += __shfl_down_sync(0xffffffffu, acc.x, 16);
-        acc.y += __shfl_down_sync(0xffffffffu, acc.y, 16);
-        if (s == 0) sm[zl * PITCH + ky] = ((kx + ky) & 1) ? -1.f * acc : acc;  // fftshiftc
+#pragma unroll
+        for (int c = 0; c < CG; ++c) {
+            acc[c].x += __shfl_down_sync(0xffffffffu, acc[c].x, 16);
+            acc[c].y += __shfl_down_sync(0xffffffffu, acc[c].y, 16);
+        }
+        if (s == 0) {
+#pragma unroll
+            for (int c = 0; c < CG; ++c) {
+                const int ky = gi * CG + c;
+                sm[zl * PITCH + ky] = ((kx + ky) & 1) ? -1.f * acc[c] : acc[c];  // fftshiftc
+            }
+        }
     }
     __syncthreads();
     const int f = threadIdx.x / T, t = threadIdx.x % T;
@@ -289,21 +318,34 @@ __global__ void __launch_bounds__(ZQ *fft_threads<G>())
     }
 }
 
-// setobj: the weight of every (cell, point) entry, same expression as the
-// forward gather (wx * wy, kernels.cuh:115-119 written separably)
+// setobj: the 4 weights of every (cell group, point) entry, with the forward
+// gather's expression (wx * wy, kernels.cuh:115-119 written separably).
+// key = point << 9 | i0 << 5 | (r0 + 3): window column i0, and the window row
+// r0 in [-3, 2M] of the group's first cell.
 template <int M>
-__global__ void k_make_entries(const int *__restrict__ keys, int2 *__restrict__ entries, size_t total,
-                               const int *__restrict__ fxy, const float *__restrict__ xt,
+__global__ void k_make_entries(const unsigned *__restrict__ keys, int *__restrict__ gpt, float4 *__restrict__ gw,
+                               size_t total, const int *__restrict__ fxy, const float *__restrict__ xt,
                                const float *__restrict__ yt, int G, float a)
 {
+    constexpr int W = 2 * M + 1;
     const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= total) return;
-    const int key = keys[e];
-    const int p = key >> 8, i1 = (key >> 4) & 15, i0 = key & 15;
+    const unsigned key = keys[e];
+    const int p = (int)(key >> 9), i0 = (int)((key >> 5) & 15), r0 = (int)(key & 31) - 3;
     const float w0 = (float)(fxy[2 * p] - M + i0) / (float)G - xt[p];
-    const float w1 = (float)(fxy[2 * p + 1] - M + i1) / (float)G - yt[p];
-    const float w = expf(-a * (w0 * w0)) * expf(-a * (w1 * w1));
-    entries[e] = make_int2(p, __float_as_int(w));
+    const float wx = expf(-a * (w0 * w0));
+    float w[CG];
+#pragma unroll
+    for (int c = 0; c < CG; ++c) {
+        const int i1 = r0 + c;
+        w[c] = 0.f;
+        if (i1 >= 0 && i1 < W) {
+            const float w1 = (float)(fxy[2 * p + 1] - M + i1) / (float)G - yt[p];
+            w[c] = wx * expf(-a * (w1 * w1));
+        }
+    }
+    gpt[e] = p;
+    gw[e] = make_float4(w[0], w[1], w[2], w[3]);
 }
 
 // ---- A4: row inverse FFT + fftshiftc + unpaddivphi + circ + crop -----------
@@ -358,8 +400,8 @@ struct pt_radon {
     float2 *rbuf = nullptr, *fgrid = nullptr;
     // adjoint (all slices, slice-minor with nzp lanes)
     float2 *lines = nullptr, *rbuf_adj = nullptr;
-    int *cell_off = nullptr, *col_order = nullptr;
-    int2 *entries = nullptr;
+    int *goff = nullptr, *col_order = nullptr, *gpt = nullptr;
+    float4 *gw = nullptr;
     size_t entries_cap = 0;
 };
 
@@ -368,7 +410,7 @@ namespace {
 void radon_free(pt_radon *h)
 {
     void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->rbuf, h->fgrid,
-                    h->lines, h->rbuf_adj, h->cell_off, h->col_order, h->entries};
+                    h->lines, h->rbuf_adj, h->goff, h->col_order, h->gpt, h->gw};
     for (void *p : bufs)
         if (p) cudaFree(p);
 }
@@ -442,7 +484,7 @@ int run_adj(pt_radon *h, float2 *f, const float2 *g, float scale, cudaStream_t s
     const int nzp = h->nzp;
     k_adj_lines<N><<<dim3(h->ntheta, nzp / ZC), ZC * 32, s3, st>>>(g, h->lines, h->nz, nzp, pre, h->tw_N);
     PT_LAUNCHED("k_adj_lines");
-    k_adj_colgather<G><<<dim3(nzp / ZQ, G), ZQ * T, s4, st>>>(h->lines, h->rbuf_adj, h->cell_off, h->entries,
+    k_adj_colgather<G><<<dim3(nzp / ZQ, G), ZQ * T, s4, st>>>(h->lines, h->rbuf_adj, h->goff, h->gpt, h->gw,
                                                              h->col_order, nzp, h->tw_G);
     PT_LAUNCHED("k_adj_colgather");
     k_adj_rows<G><<<dim3(n, nzp / ZC), ZC * T, s1, st>>>(h->rbuf_adj, f, h->nz, nzp, h->mu, scale, h->tw_G);
@@ -559,7 +601,7 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     const size_t nzp = h->nzp;
     if (rc == PT_OK) rc = dmalloc(&h->lines, ntheta * N * nzp);
     if (rc == PT_OK) rc = dmalloc(&h->rbuf_adj, n * (size_t)G * nzp);
-    if (rc == PT_OK) rc = dmalloc(&h->cell_off, (size_t)G * G + 1);
+    if (rc == PT_OK) rc = dmalloc(&h->goff, (size_t)G * (G / CG) + 1);
     if (rc == PT_OK) rc = dmalloc(&h->col_order, (size_t)G);
     if (rc == PT_OK) rc = radon_set_attrs(G);
     if (rc == PT_OK) {
@@ -626,62 +668,73 @@ extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
         fxy[2 * p + 1] = (int)floorf((float)G * ys[p]);
     }
     PT_CUDA(cudaMemcpy(h->fxy, fxy.data(), 2 * npts * sizeof(int), cudaMemcpyHostToDevice));
-    // cell -> (point, tap) lists for the adjoint: every point lists its
-    // (2M+1)^2 window cells (mod G: the reference's halo fold, kernels.cuh:67-82),
-    // in increasing point order, so each cell sums in a fixed order.
-    const size_t ncell = (size_t)G * G;
-    std::vector<int> off(ncell + 1, 0);
-    int cols[32], rows[32];
+    // cell-group lists for the adjoint: a group is CG consecutive rows of one
+    // grid column; every point is listed, in increasing point order, in each
+    // group that its (2M+1)^2 window (mod G: the reference's halo fold,
+    // kernels.cuh:67-82) touches, with the window column i0 and row offset r0.
+    const int NG4 = G / CG;
+    const size_t ngroups = (size_t)G * NG4;
+    std::vector<int> off(ngroups + 1, 0);
+    int cols[32], grp_first[8], ngrp = 0, oy = 0;
     auto window = [&](size_t p) {
         const int ox = ((N + fxy[2 * p] - M) % G + G) % G;
-        const int oy = ((N + fxy[2 * p + 1] - M) % G + G) % G;
+        oy = ((N + fxy[2 * p + 1] - M) % G + G) % G;
+        for (int i = 0; i < W; ++i) cols[i] = (ox + i) % G;
+        ngrp = 0;
         for (int i = 0; i < W; ++i) {
-            cols[i] = (ox + i) % G;
-            rows[i] = (oy + i) % G;
+            const int gi = ((oy + i) % G) / CG;
+            if (ngrp == 0 || grp_first[ngrp - 1] != gi) grp_first[ngrp++] = gi;
         }
     };
     for (size_t p = 0; p < npts; ++p) {
         window(p);
-        for (int i1 = 0; i1 < W; ++i1)
-            for (int i0 = 0; i0 < W; ++i0) off[(size_t)rows[i1] * G + cols[i0] + 1]++;
+        for (int i0 = 0; i0 < W; ++i0)
+            for (int k = 0; k < ngrp; ++k) off[(size_t)cols[i0] * NG4 + grp_first[k] + 1]++;
     }
-    for (size_t c = 0; c < ncell; ++c) off[c + 1] += off[c];
-    const size_t total = (size_t)off[ncell];
-    std::vector<int> keys(total);
+    for (size_t c = 0; c < ngroups; ++c) off[c + 1] += off[c];
+    const size_t total = (size_t)off[ngroups];
+    std::vector<unsigned> keys(total);
     {
         std::vector<int> pos(off.begin(), off.end() - 1);
         for (size_t p = 0; p < npts; ++p) {
             window(p);
-            for (int i1 = 0; i1 < W; ++i1)
+            for (int k = 0; k < ngrp; ++k) {
+                int r0 = ((grp_first[k] * CG - oy) % G + G) % G;  // row offset of the group's first cell
+                if (r0 > G - CG) r0 -= G;                          // in [-(CG-1), 2M]
                 for (int i0 = 0; i0 < W; ++i0)
-                    keys[pos[(size_t)rows[i1] * G + cols[i0]]++] = (int)((p << 8) | (i1 << 4) | i0);
+                    keys[pos[(size_t)cols[i0] * NG4 + grp_first[k]]++] =
+                        ((unsigned)p << 9) | ((unsigned)i0 << 5) | (unsigned)(r0 + 3);
+            }
         }
     }
     // columns ordered by decreasing work so the heavy centre columns start first
     std::vector<long long> colw(G, 0);
-    for (size_t c = 0; c < ncell; ++c) colw[c % G] += off[c + 1] - off[c];
+    for (int c = 0; c < G; ++c) colw[c] = off[(size_t)(c + 1) * NG4] - off[(size_t)c * NG4];
     std::vector<int> order(G);
     for (int i = 0; i < G; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int i, int j) { return colw[i] > colw[j]; });
     if (total > h->entries_cap) {
-        if (h->entries) cudaFree(h->entries);
-        h->entries = nullptr;
+        if (h->gpt) cudaFree(h->gpt);
+        if (h->gw) cudaFree(h->gw);
+        h->gpt = nullptr;
+        h->gw = nullptr;
         h->entries_cap = 0;
-        rc = dmalloc(&h->entries, total);
+        rc = dmalloc(&h->gpt, total);
+        if (rc == PT_OK) rc = dmalloc(&h->gw, total);
         if (rc != PT_OK) return rc;
         h->entries_cap = total;
     }
-    int *dkeys = nullptr;
+    unsigned *dkeys = nullptr;
     rc = dmalloc(&dkeys, total);
     if (rc != PT_OK) return rc;
-    cudaError_t e1 = cudaMemcpy(dkeys, keys.data(), total * sizeof(int), cudaMemcpyHostToDevice);
+    cudaError_t e1 = cudaMemcpy(dkeys, keys.data(), total * sizeof(unsigned), cudaMemcpyHostToDevice);
     if (e1 == cudaSuccess) {
         const float a = (float)(PI_REF * PI_REF / h->mu);
         const unsigned blocks = (unsigned)((total + 255) / 256);
         if (M == 7)
-            k_make_entries<7><<<blocks, 256, 0, st>>>(dkeys, h->entries, total, h->fxy, h->x, h->y, G, a);
+            k_make_entries<7><<<blocks, 256, 0, st>>>(dkeys, h->gpt, h->gw, total, h->fxy, h->x, h->y, G, a);
         else
-            k_make_entries<4><<<blocks, 256, 0, st>>>(dkeys, h->entries, total, h->fxy, h->x, h->y, G, a);
+            k_make_entries<4><<<blocks, 256, 0, st>>>(dkeys, h->gpt, h->gw, total, h->fxy, h->x, h->y, G, a);
         e1 = cudaGetLastError();
         if (e1 == cudaSuccess) e1 = cudaStreamSynchronize(st);
     }
@@ -690,7 +743,7 @@ extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
         pt::set_error("radonusfft.setobj: building the adjoint lists failed: %s", cudaGetErrorString(e1));
         return PT_ERR_CUDA;
     }
-    PT_CUDA(cudaMemcpy(h->cell_off, off.data(), (ncell + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    PT_CUDA(cudaMemcpy(h->goff, off.data(), (ngroups + 1) * sizeof(int), cudaMemcpyHostToDevice));
     PT_CUDA(cudaMemcpy(h->col_order, order.data(), G * sizeof(int), cudaMemcpyHostToDevice));
     h->ready = true;
     return PT_OK;
