@@ -19,6 +19,8 @@
 //  Detector 8x8 uses a plain shared-memory Stockham path.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstdint>
 #include <vector>
 
 #include "pt_common.cuh"
@@ -310,16 +312,255 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
             const int py = grp + F::NG * c - off;
             if (py < 0 || py >= P) continue;
             float2 *row = slab + (size_t)(sty + py) * n + stx;
+            float2 cur[F::N1];
 #pragma unroll
             for (int k2 = 0; k2 < F::N2; ++k2)
 #pragma unroll
                 for (int j = 0; j < F::KPT; ++j) {
                     const int px = t * F::KPT + j + F::N1 * k2 - off;
-                    if (px >= 0 && px < P) row[px] = row[px] + cmulc(__ldg(&prbT[py * P + px]), v[c][j * F::N2 + k2]);
+                    cur[j * F::N2 + k2] = (px >= 0 && px < P) ? row[px] : czero();
+                }
+#pragma unroll
+            for (int k2 = 0; k2 < F::N2; ++k2)
+#pragma unroll
+                for (int j = 0; j < F::KPT; ++j) {
+                    const int px = t * F::KPT + j + F::N1 * k2 - off;
+                    if (px >= 0 && px < P)
+                        row[px] = cur[j * F::N2 + k2] + cmulc(__ldg(&prbT[py * P + px]), v[c][j * F::N2 + k2]);
                 }
         }
         __syncthreads();
     }
+}
+
+// ---- det = 128: 16-byte shared-memory traffic ------------------------------
+// Transpose in a "pair" layout: a 16-byte slot holds rows 2q and 2q+1 of one
+// column; slot (q, c) lives at q * 128 + (c ^ (q & 7)), so the 8 threads of a
+// group hit 8 distinct 4-bank groups both when writing (q varies) and when
+// reading (c varies).  The group exchange uses the same trick.
+constexpr int P128_SMEM = (64 * 128) * 16 + 128 * 8;
+
+template <int DIR>
+__device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, const float2 *tws)
+{
+    ptfft::Dft<16, DIR>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) {
+        float2 w = tws[t * k1];
+        if (DIR > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) sc[t * 8 + ((q + t) & 7)] = make_float4(v[2 * q].x, v[2 * q].y, v[2 * q + 1].x, v[2 * q + 1].y);
+    __syncwarp();
+    float2 u0[8], u1[8];
+#pragma unroll
+    for (int n2 = 0; n2 < 8; ++n2) {
+        const float4 w = sc[n2 * 8 + ((t + n2) & 7)];
+        u0[n2] = make_float2(w.x, w.y);
+        u1[n2] = make_float2(w.z, w.w);
+    }
+    ptfft::Dft<8, DIR>::run(u0);
+    ptfft::Dft<8, DIR>::run(u1);
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) {
+        v[k2] = u0[k2];       // X[2t + 16 k2]
+        v[8 + k2] = u1[k2];   // X[2t + 1 + 16 k2]
+    }
+}
+
+template <bool FULL>
+__global__ void __launch_bounds__(512, 1)
+    k_ptycho_fwd128(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
+                    const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
+                    int nframes, int P, float scale, const float2 *__restrict__ tw)
+{
+    extern __shared__ float4 sm4[];
+    float4 *fr = sm4;
+    float2 *tws = reinterpret_cast<float2 *>(sm4 + 64 * 128);
+    for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
+    const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
+    float4 *sc = fr + grp * 64;
+    const int off = FULL ? 0 : (128 - P) / 2;
+    __syncthreads();
+    for (int fid = blockIdx.x; fid < nframes; fid += gridDim.x) {
+        const int th = fid / nscan;
+        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
+        float2 *out = g + (size_t)fid * 128 * 128;
+        if (stx < 0 || sty < 0) {
+            for (int e = threadIdx.x; e < 128 * 128 / 2; e += 512) reinterpret_cast<float4 *>(out)[e] = make_float4(0, 0, 0, 0);
+            continue;
+        }
+        const float2 *src = psi + ((size_t)th * nz + sty) * n + stx;
+        float2 v[2][16];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int py = grp + 64 * c - off;
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                const int px = t + 8 * m - off;
+                if (FULL) {
+                    v[c][m] = cmul(__ldg(&prbT[py * P + px]), __ldg(&src[(size_t)py * n + px]));
+                } else {
+                    float2 val = czero();
+                    if (py >= 0 && py < P && px >= 0 && px < P)
+                        val = cmul(__ldg(&prbT[py * P + px]), __ldg(&src[(size_t)py * n + px]));
+                    v[c][m] = val;
+                }
+            }
+            line_dft128<-1>(v[c], t, sc, tws);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int iy = grp + 64 * c;
+#pragma unroll
+            for (int k2 = 0; k2 < 8; ++k2) {
+                const int kp = t + 8 * k2;
+                fr[kp * 128 + (iy ^ (kp & 7))] = make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const float4 q = fr[grp * 128 + ((t + 8 * m) ^ (grp & 7))];
+            v[0][m] = make_float2(q.x, q.y);
+            v[1][m] = make_float2(q.z, q.w);
+        }
+        __syncthreads();
+        const float2 ph = scale * phase[fid];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            line_dft128<-1>(v[c], t, sc, tws);
+            float4 *row = reinterpret_cast<float4 *>(out + (2 * grp + c) * 128);
+#pragma unroll
+            for (int k2 = 0; k2 < 8; ++k2) {
+                const float2 a = cmul(v[c][k2], ph), b = cmul(v[c][8 + k2], ph);
+                row[t + 8 * k2] = make_float4(a.x, a.y, b.x, b.y);   // ky = 2t + 16 k2, +1
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// cp.async helpers (16-byte global -> shared copies, Ampere+ async copy)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// Rows 0..63 of frame `in` (64 KB) -> shared [row][64 chunks of 16 B], chunk
+// index XORed with (row & 1) << 2 so that Phase A reads are conflict-free.
+__device__ __forceinline__ void prefetch_half_frame(float4 *dst, const float2 *in)
+{
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int id = threadIdx.x + 512 * i;
+        const int row = id >> 6, c16 = id & 63;
+        cp_async16(dst + row * 64 + (c16 ^ ((row & 1) << 2)), in + row * 128 + 2 * c16);
+    }
+    cp_async_commit();
+}
+
+// grid (parts, ntheta): block (part, angle) owns slab dst[angle][part].
+// While the current frame finishes, the next frame's rows 0..63 are already
+// on their way into the idle half of the shared frame buffer.
+template <bool FULL>
+__global__ void __launch_bounds__(512, 1)
+    k_ptycho_adj128(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
+                    const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
+                    int P, float scale, const float2 *__restrict__ tw)
+{
+    extern __shared__ float4 sm4[];
+    float4 *fr = sm4;
+    float4 *pre = sm4 + 64 * 64;  // upper 64 KB of the frame buffer
+    float2 *tws = reinterpret_cast<float2 *>(sm4 + 64 * 128);
+    const int part = blockIdx.x, parts = gridDim.x, th = blockIdx.y;
+    float2 *slab = dst + ((size_t)th * parts + part) * nz * n;
+    for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
+    for (int e = threadIdx.x; e < nz * n; e += 512) slab[e] = czero();
+    const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
+    float4 *sc = fr + grp * 64;
+    const int off = FULL ? 0 : (128 - P) / 2;
+    const float2 *gth = g + (size_t)th * nscan * 128 * 128;
+    if (part < nscan) prefetch_half_frame(pre, gth + (size_t)part * 128 * 128);
+    for (int s = part; s < nscan; s += parts) {
+        const int fid = th * nscan + s;
+        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
+        const float2 *in = gth + (size_t)s * 128 * 128;
+        const float2 *in_next = s + parts < nscan ? in + (size_t)parts * 128 * 128 : nullptr;
+        cp_async_wait_all();
+        __syncthreads();
+        if (stx < 0 || sty < 0) {  // skipped scan: keep the prefetch chain going
+            __syncthreads();
+            if (in_next) prefetch_half_frame(pre, in_next);
+            continue;
+        }
+        const float2 ph = phase[fid];
+        float2 v[2][16];
+        // rows 64..127 from global first, so their latency hides behind row 0..63's work
+#pragma unroll
+        for (int m = 0; m < 16; ++m) v[1][m] = __ldg(&in[(grp + 64) * 128 + t + 8 * m]);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int ky = t + 8 * m;
+            const float4 q = pre[grp * 64 + ((ky >> 1) ^ ((grp & 1) << 2))];
+            v[0][m] = scale * cmulc(ph, (ky & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y));
+        }
+        line_dft128<+1>(v[0], t, sc, tws);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) v[1][m] = scale * cmulc(ph, v[1][m]);
+        line_dft128<+1>(v[1], t, sc, tws);
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int kx = grp + 64 * c;
+#pragma unroll
+            for (int k2 = 0; k2 < 8; ++k2) {
+                const int ip = t + 8 * k2;
+                fr[ip * 128 + (kx ^ (ip & 7))] = make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const float4 q = fr[grp * 128 + ((t + 8 * m) ^ (grp & 7))];
+            v[0][m] = make_float2(q.x, q.y);
+            v[1][m] = make_float2(q.z, q.w);
+        }
+        __syncthreads();
+        if (in_next) prefetch_half_frame(pre, in_next);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            line_dft128<+1>(v[c], t, sc, tws);
+            const int py = 2 * grp + c - off;
+            if (!FULL && (py < 0 || py >= P)) continue;
+            float2 *row = slab + (size_t)(sty + py) * n + stx;
+            // all 16 slab values are loaded before any is stored back, so the
+            // loads overlap instead of waiting on each other's stores
+            float2 cur[16];
+#pragma unroll
+            for (int k2 = 0; k2 < 8; ++k2)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int px = 2 * t + j + 16 * k2 - off;
+                    cur[j * 8 + k2] = (FULL || (px >= 0 && px < P)) ? row[px] : czero();
+                }
+#pragma unroll
+            for (int k2 = 0; k2 < 8; ++k2)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int px = 2 * t + j + 16 * k2 - off;
+                    if (FULL || (px >= 0 && px < P))
+                        row[px] = cur[j * 8 + k2] + cmulc(__ldg(&prbT[py * P + px]), v[c][j * 8 + k2]);
+                }
+        }
+    }
+    cp_async_wait_all();
 }
 
 // out[angle] = sum over parts of dst[angle][part], fixed order
@@ -366,6 +607,14 @@ int ptycho_attrs()
         const int s = DET * (DET + 1) * sizeof(float2);
         PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd_small<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
         PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj_small<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+    } else if constexpr (DET == 128) {
+        const int s = (int)PF<DET>::SMEM;
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd128<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, P128_SMEM));
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd128<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, P128_SMEM));
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj128<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, P128_SMEM));
+        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj128<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, P128_SMEM));
     } else {
         const int s = (int)PF<DET>::SMEM;
         PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
@@ -391,14 +640,44 @@ int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scal
     } else {
         using F = PF<DET>;
         const int nframes = h->ntheta * h->nscan;
+        const bool full = (h->P == DET);
         if (!adj) {
-            k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
-                                                              h->nscan, nframes, h->P, scale, h->tw);
+            // the det = 128 kernel writes frames with 16-byte stores
+            const bool aligned16 = ((uintptr_t)out % 16) == 0;
+            if constexpr (DET == 128) {
+                if (!aligned16)
+                    k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz,
+                                                                      h->n, h->nscan, nframes, h->P, scale, h->tw);
+                else if (full)
+                    k_ptycho_fwd128<true><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz,
+                                                                          h->n, h->nscan, nframes, h->P, scale, h->tw);
+                else
+                    k_ptycho_fwd128<false><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT,
+                                                                           h->nz, h->n, h->nscan, nframes, h->P, scale,
+                                                                           h->tw);
+            } else {
+                k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
+                                                                  h->nscan, nframes, h->P, scale, h->tw);
+            }
             PT_LAUNCHED("k_ptycho_fwd");
         } else {
             float2 *dst = h->parts > 1 ? h->partial : out;
-            k_ptycho_adj<DET><<<dim3(h->parts, h->ntheta), F::NT, F::SMEM, st>>>(
-                in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
+            // the det = 128 adjoint prefetches frames with 16-byte async copies
+            const bool in_aligned16 = ((uintptr_t)in % 16) == 0;
+            if constexpr (DET == 128) {
+                if (!in_aligned16)
+                    k_ptycho_adj<DET><<<dim3(h->parts, h->ntheta), F::NT, F::SMEM, st>>>(
+                        in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
+                else if (full)
+                    k_ptycho_adj128<true><<<dim3(h->parts, h->ntheta), 512, P128_SMEM, st>>>(
+                        in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
+                else
+                    k_ptycho_adj128<false><<<dim3(h->parts, h->ntheta), 512, P128_SMEM, st>>>(
+                        in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
+            } else {
+                k_ptycho_adj<DET><<<dim3(h->parts, h->ntheta), F::NT, F::SMEM, st>>>(
+                    in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
+            }
             PT_LAUNCHED("k_ptycho_adj");
             if (h->parts > 1) {
                 const size_t slab = (size_t)h->nz * h->n, total = slab * h->ntheta;
@@ -481,7 +760,23 @@ extern "C" int pt_ptycho_create(size_t ntheta, size_t nz, size_t n, size_t nthet
     // adjoint split: enough (part, angle) blocks to fill the GPU twice
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
-    h->parts = (detx >= 16 && (int)ntheta < 2 * nsm) ? (int)std::min<size_t>(nscan, (2 * nsm + ntheta - 1) / ntheta) : 1;
+    // waves x scans-per-block, with a 3% charge per extra part for the slab traffic;
+    // PT_PTYCHO_ADJ_PARTS=<k> overrides the choice (tuning)
+    h->parts = 1;
+    const char *env_parts = getenv("PT_PTYCHO_ADJ_PARTS");
+    if (env_parts && atoi(env_parts) >= 1) {
+        h->parts = std::min<int>(atoi(env_parts), (int)nscan);
+    } else if (detx >= 16) {
+        double best = 1e300;
+        for (int p = 1; p <= (int)std::min<size_t>(nscan, 16); ++p) {
+            const double waves = std::ceil((double)ntheta * p / nsm);
+            const double cost = waves * std::ceil((double)nscan / p) * (1.0 + 0.03 * (p - 1));
+            if (cost < best - 1e-9) {
+                best = cost;
+                h->parts = p;
+            }
+        }
+    }
     bool ok = cudaMalloc((void **)&h->tw, detx * sizeof(float2)) == cudaSuccess &&
               cudaMalloc((void **)&h->prb, nprb * nprb * sizeof(float2)) == cudaSuccess &&
               cudaMalloc((void **)&h->prbT, nprb * nprb * sizeof(float2)) == cudaSuccess &&

@@ -172,7 +172,7 @@ def p_adj(op, g):
 
 
 PTYCHO_SIZES = [(3, 32, 32, 7, 16, 16), (2, 24, 40, 5, 32, 16), (2, 64, 64, 9, 64, 64),
-                (2, 130, 140, 6, 128, 128), (4, 20, 20, 3, 8, 8)]
+                (2, 130, 140, 6, 128, 128), (3, 100, 110, 5, 128, 96), (4, 20, 20, 3, 8, 8)]
 
 
 @pytest.mark.parametrize("ntheta,nz,n,nscan,det,nprb", PTYCHO_SIZES)
@@ -221,3 +221,29 @@ def test_ptycho_vs_reference_cuda(ntheta, nz, n, nscan, det, nprb):
     ref.free()
     assert rel(p_fwd(op, f).cpu().numpy(), gr.cpu().numpy()) <= TOL
     assert rel(p_adj(op, g).cpu().numpy(), fr.cpu().numpy()) <= TOL
+
+
+def test_ptycho_det128_misaligned_output_pointer():
+    """A frame buffer that is only 8-byte aligned takes the generic kernel."""
+    rng = np.random.default_rng(17)
+    op, orc, _, _ = make_ptycho(2, 130, 130, 3, 128, 128, rng)
+    f = crand(rng, (2, 130, 130))
+    big = torch.zeros(2 * 3 * 128 * 128 + 1, dtype=torch.complex64, device="cuda")
+    out = big[1:]
+    assert out.data_ptr() % 16 == 8
+    op.fwd(out.data_ptr(), dev(f))
+    assert rel(out.view(2, 3, 128, 128).cpu().numpy(), orc.fwd(f)) <= TOL
+
+
+def test_ptycho_det128_misaligned_adjoint_input():
+    """An adjoint input that is only 8-byte aligned takes the generic kernel."""
+    rng = np.random.default_rng(19)
+    op, orc, _, _ = make_ptycho(2, 140, 130, 4, 128, 128, rng)
+    g = crand(rng, (2, 4, 128, 128))
+    big = torch.zeros(g.size + 1, dtype=torch.complex64, device="cuda")
+    big[1:] = dev(g.ravel())
+    src = big[1:]
+    assert src.data_ptr() % 16 == 8
+    out = torch.zeros((2, 140, 130), dtype=torch.complex64, device="cuda")
+    op.adj(out, src.data_ptr())
+    assert rel(out.cpu().numpy(), orc.adj(g)) <= TOL
