@@ -10,8 +10,9 @@
 //                     that are non-zero)                       [smem FFT]
 //    K2 k_fwd_cols    column FFT of length 2N (zero rows implicit) with the
 //                     post-FFT centring sign folded in          [smem FFT]
-//    K3 k_fwd_gather  Gaussian-kernel gather at the polar points, 1-D
-//                     centred inverse FFT along the detector, crop n of N
+//    K3a k_fwd_gather_pts  Gaussian-kernel gather at the polar points
+//                     (kernels.cuh:97-126), one 8-slice lane group per point
+//    K3b k_fwd_lines  1-D centred inverse FFT along the detector, crop n of N
 //  adjoint  R* g  (radonusfft.cu:94-139)
 //    A1 k_adj_lines     edge-replicating pad, centred 1-D FFT, written for all
 //                       slices as lines[point][slice]
@@ -138,57 +139,95 @@ __global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
     }
     __syncthreads();
     ptfft::fft<G, -1, T>(sm + f * PITCH, 1, t, tw);
+    // column-pair layout [ky][kx/2][z][kx&1]: one 128-byte line per (ky, pair)
+    static_assert(CK == 2, "the grid layout pairs two columns");
     for (int e = threadIdx.x; e < G * NF; e += blockDim.x) {
-        const int ky = e / NF, q = e % NF;
-        const int kx = kx0 + q / ZC;
-        float2 v = sm[q * PITCH + ky];
+        const int ky = e / NF, r = e % NF;
+        const int z = r >> 1, c = r & 1;
+        const int kx = kx0 + c;
+        float2 v = sm[(c * ZC + z) * PITCH + ky];
         if ((kx + ky) & 1) v = -1.f * v;
-        fg[((size_t)ky * G + kx0) * ZC + q] = v;
+        fg[((size_t)ky * (G / 2) + kx0 / 2) * (2 * ZC) + r] = v;
     }
 }
 
-// ---- K3: gather (kernels.cuh:97-126) + fftshift1c/IFFT/fftshift1c + crop ---
+// ---- K3a: gather only, many blocks --------------------------------------------
+// grid (ceil(N / GPB), ntheta); block = GPB points x ZC slice lanes.  The grid
+// is in column-pair layout, so a lane reads its slice's value at two
+// neighbouring window columns with one 16-byte load (the point's 8 lanes read
+// one 128-byte line).  The window's 15 columns are covered by 8 column pairs;
+// the one column outside the window gets weight 0.  Writes the gathered,
+// 1/N- and fftshift1c-scaled samples to lines[(theta N + k) ZC + z].
+constexpr int GPB = 32;
 template <int N, int M>
-__global__ void __launch_bounds__(ZC * 32)
-    k_fwd_gather(const float2 *__restrict__ fg, float2 *__restrict__ out, const float *__restrict__ xt,
-                 const float *__restrict__ yt, int nz, int z0, float a, float pre, float scale,
-                 const float2 *__restrict__ tw)
+__global__ void __launch_bounds__(GPB *ZC)
+    k_fwd_gather_pts(const float2 *__restrict__ fg, float2 *__restrict__ lines, const float *__restrict__ xt,
+                     const float *__restrict__ yt, float a, float pre)
 {
-    constexpr int G = 2 * N, n = 2 * N / 3, c0 = N / 6, W = 2 * M + 1, PITCH = N + 1, T = 32;
+    constexpr int G = 2 * N, W = 2 * M + 1, NP = (W + 2) / 2;  // column pairs covering the window
+    const int th = blockIdx.y;
+    const int lane = threadIdx.x % ZC;
+    const int k = blockIdx.x * GPB + threadIdx.x / ZC;
+    if (k >= N) return;
+    const float x0 = xt[th * N + k], y0 = yt[th * N + k];
+    // x0, y0 in [-1/2, 1/2) (validated at setobj); clamp keeps reads in bounds
+    const int fx = min(max((int)floorf((float)G * x0), -N), N - 1);
+    const int fy = min(max((int)floorf((float)G * y0), -N), N - 1);
+    const int c0 = wrapG(N + fx - M, G);  // first window column
+    const int odd = c0 & 1;               // window starts in the second column of a pair
+    float2 wxp[NP];                       // weights of the two columns of each pair
+    float wy[W];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        float w2[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i0 = 2 * j + h - odd;
+            const float w0 = (float)(fx - M + i0) / (float)G - x0;
+            w2[h] = (i0 >= 0 && i0 < W) ? expf(-a * (w0 * w0)) : 0.f;
+        }
+        wxp[j] = make_float2(w2[0], w2[1]);
+    }
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+        const float w1 = (float)(fy - M + i) / (float)G - y0;
+        wy[i] = expf(-a * (w1 * w1));
+    }
+    const int p0 = (c0 - odd) / 2;  // first column pair
+    const float4 *g4 = reinterpret_cast<const float4 *>(fg) + lane;
+    float2 acc = czero();
+#pragma unroll
+    for (int i1 = 0; i1 < W; ++i1) {
+        const float4 *rowp = g4 + (size_t)wrapG(N + fy - M + i1, G) * (G / 2) * ZC;
+        float2 rs = czero();
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            int pc = p0 + j;
+            pc -= pc >= G / 2 ? G / 2 : 0;
+            const float4 v = __ldg(rowp + pc * ZC);
+            rs.x = fmaf(wxp[j].x, v.x, rs.x);
+            rs.y = fmaf(wxp[j].x, v.y, rs.y);
+            rs.x = fmaf(wxp[j].y, v.z, rs.x);
+            rs.y = fmaf(wxp[j].y, v.w, rs.y);
+        }
+        acc.x = fmaf(wy[i1], rs.x, acc.x);
+        acc.y = fmaf(wy[i1], rs.y, acc.y);
+    }
+    lines[((size_t)th * N + k) * ZC + lane] = ((k & 1) ? pre : -pre) * acc;
+}
+
+// ---- K3b: fftshift1c / 1-D inverse FFT / fftshift1c + crop + scale --------
+template <int N>
+__global__ void __launch_bounds__(ZC * 32)
+    k_fwd_lines(const float2 *__restrict__ lines, float2 *__restrict__ out, int nz, int z0, float scale,
+                const float2 *__restrict__ tw)
+{
+    constexpr int n = 2 * N / 3, c0 = N / 6, PITCH = N + 1, T = 32;
     extern __shared__ float2 sm[];
     const int th = blockIdx.x;
-    const int lane = threadIdx.x % ZC, grp = threadIdx.x / ZC;
-    for (int k = grp; k < N; k += 32) {
-        const float x0 = xt[th * N + k], y0 = yt[th * N + k];
-        // x0, y0 in [-1/2, 1/2) (validated at setobj); clamp keeps reads in bounds
-        const int fx = min(max((int)floorf((float)G * x0), -N), N - 1);
-        const int fy = min(max((int)floorf((float)G * y0), -N), N - 1);
-        float wx[W], wy[W];
-        int col[W];
-#pragma unroll
-        for (int i = 0; i < W; ++i) {
-            const float w0 = (float)(fx - M + i) / (float)G - x0;
-            const float w1 = (float)(fy - M + i) / (float)G - y0;
-            wx[i] = expf(-a * (w0 * w0));
-            wy[i] = expf(-a * (w1 * w1));
-            col[i] = wrapG(N + fx - M + i, G) * ZC + lane;
-        }
-        float2 acc = czero();
-#pragma unroll
-        for (int i1 = 0; i1 < W; ++i1) {
-            const float2 *rowp = fg + (size_t)wrapG(N + fy - M + i1, G) * G * ZC;
-            float2 rs = czero();
-#pragma unroll
-            for (int i0 = 0; i0 < W; ++i0) {
-                const float2 v = __ldg(rowp + col[i0]);
-                rs.x = fmaf(wx[i0], v.x, rs.x);
-                rs.y = fmaf(wx[i0], v.y, rs.y);
-            }
-            acc.x = fmaf(wy[i1], rs.x, acc.x);
-            acc.y = fmaf(wy[i1], rs.y, acc.y);
-        }
-        // fftshift1c sign (1-2((k+1)%2)) and the 1/N of kernels.cuh:124-125
-        sm[lane * PITCH + k] = ((k & 1) ? pre : -pre) * acc;
+    for (int e = threadIdx.x; e < N * ZC; e += blockDim.x) {
+        const int k = e / ZC, q = e % ZC;
+        sm[q * PITCH + k] = lines[((size_t)th * N + k) * ZC + q];
     }
     __syncthreads();
     const int f = threadIdx.x / T, t = threadIdx.x % T;
@@ -446,8 +485,7 @@ int set_attrs()
     PT_CUDA(cudaFuncSetAttribute(k_adj_colgather<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s4));
     PT_CUDA(cudaFuncSetAttribute(k_adj_rows<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
     const int s3 = ZC * (N + 1) * sizeof(float2);
-    PT_CUDA(cudaFuncSetAttribute(k_fwd_gather<N, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
-    PT_CUDA(cudaFuncSetAttribute(k_fwd_gather<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    PT_CUDA(cudaFuncSetAttribute(k_fwd_lines<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     PT_CUDA(cudaFuncSetAttribute(k_adj_lines<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     return PT_OK;
 }
@@ -466,9 +504,11 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
         PT_LAUNCHED("k_fwd_rows");
         k_fwd_cols<G><<<G / CK, CK * ZC * T, s2, st>>>(h->rbuf, h->fgrid, h->tw_G);
         PT_LAUNCHED("k_fwd_cols");
-        k_fwd_gather<N, M><<<h->ntheta, ZC * 32, s3, st>>>(h->fgrid, g, h->x, h->y, h->nz, z0, a, pre,
-                                                           scale, h->tw_N);
-        PT_LAUNCHED("k_fwd_gather");
+        k_fwd_gather_pts<N, M><<<dim3((N + GPB - 1) / GPB, h->ntheta), GPB * ZC, 0, st>>>(h->fgrid, h->lines, h->x,
+                                                                                          h->y, a, pre);
+        PT_LAUNCHED("k_fwd_gather_pts");
+        k_fwd_lines<N><<<h->ntheta, ZC * 32, s3, st>>>(h->lines, g, h->nz, z0, scale, h->tw_N);
+        PT_LAUNCHED("k_fwd_lines");
     }
     return PT_OK;
 }
