@@ -69,6 +69,22 @@ def config_dict(c, extra=None):
     return d
 
 
+def dram_traffic(op):
+    """DRAM bytes (read + write) per call of `op` from the committed ncu summary
+    profiles/dram_traffic_bench_256cubed.md (rows `| op | bytes | ... |`)."""
+    path = ROOT / "profiles" / "dram_traffic_bench_256cubed.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) >= 2 and cells[0] == op:
+            try:
+                return int(float(cells[1]))
+            except ValueError:
+                return None
+    return None
+
+
 # ----------------------------------------------------------------------------
 # clocks sampler (nvidia-smi during the timed region)
 # ----------------------------------------------------------------------------
@@ -85,7 +101,7 @@ class Clocks:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -286,10 +302,7 @@ def run_ours(args, rank, world, local):
     peak = peak or 6650.0
     dom = max(per_op, key=per_op.get)
     achieved = bytes_op[dom] / (per_op[dom] * 1e-3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get(dom)
+    traffic = dram_traffic(dom)
 
     line = {"metric": "operator HBM GB/s (radonusfft fwd+adj + ptychofft fwd+adj, 256^3)",
             "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -451,8 +464,8 @@ def run_reference_cuda(args, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--ref-backend", choices=["cpu", "cuda"], default="cpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -96,6 +96,13 @@ int pt_ptycho_adj(pt_ptycho *h, void *f, const void *g, void *stream);
  * adj_ptycho apply coefptycho this way, solver.py:100-125). */
 int pt_ptycho_fwd_scaled(pt_ptycho *h, void *g, const void *f, float scale, void *stream);
 int pt_ptycho_adj_scaled(pt_ptycho *h, void *f, const void *g, float scale, void *stream);
+/* Gradient of the ptycho data term, solver.py:219-224: f = scale * Q* F* r
+ * with the residual r = fpsi - D fpsi / (|fpsi|^2 + 1e-32) (model 0, Poisson)
+ * or fpsi - sqrt(D) exp(i angle fpsi) (model 1, Gaussian), D = dscale * data,
+ * formed while the adjoint loads its frames (no residual array).  fpsi is
+ * not modified. */
+int pt_ptycho_adj_resid(pt_ptycho *h, void *f, const void *fpsi, const float *data, float dscale, int model,
+                        float scale, void *stream);
 
 
 /* ---- Solver arithmetic (src/ptychotomo/solver.py:48-336) -----------------
@@ -115,7 +122,8 @@ int pt_reduce_c64(int op, const void *a, const void *b, size_t n, int c0, int c1
  * (solver.py:208-214, :171-177), with D = dscale * data and t(x) =
  * |x|^2 - 2 D log max(|x|, 1e-32) (model 0, Poisson) or (|x| - sqrt D)^2
  * (model 1, Gaussian):  out[j] = sum over frames of t(f) - t(f + gammas[j] d),
- * formed per element in FP64.  gammas: device double[J], J <= 16. */
+ * formed per element without cancellation (log1p of the relative change)
+ * and summed in FP64.  gammas: device double[J], J <= 16. */
 int pt_ls_frames(const void *f, const void *d, const float *data, float dscale, size_t n, int model,
                  const double *gammas, int J, void *work, void *out, void *stream);
 /* pt_ls_frames without allocating anything and without a workspace argument.

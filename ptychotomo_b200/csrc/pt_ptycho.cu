@@ -30,6 +30,28 @@ namespace {
 
 constexpr double PI_REF = 3.1415926535;  // kernels.cuh:1
 
+// Residual of the ptycho data term applied to a frame value x on load
+// (solver.py:220-224, D = dscale * data): RESID 0 = none (plain adjoint),
+// 1 = Poisson x - D x / (|x|^2 + 1e-32), 2 = Gaussian x - sqrt(D) exp(i angle x).
+template <int RESID>
+__device__ __forceinline__ float2 resid(float2 x, const float *__restrict__ data, size_t idx, float dscale)
+{
+    if constexpr (RESID == 0) {
+        return x;
+    } else {
+        const float D = __ldg(&data[idx]) * dscale;
+        if constexpr (RESID == 1) {
+            const float q = D / (x.x * x.x + x.y * x.y + 1e-32f);
+            return make_float2(x.x - q * x.x, x.y - q * x.y);
+        } else {
+            float sn, cs;
+            sincosf(atan2f(x.y, x.x), &sn, &cs);
+            const float sq = sqrtf(D);
+            return make_float2(x.x - sq * cs, x.y - sq * sn);
+        }
+    }
+}
+
 template <int DET>
 constexpr int ptycho_fft_threads() { return (512 / DET) < 4 ? 4 : ((512 / DET) > 32 ? 32 : 512 / DET); }
 template <int DET>
@@ -89,11 +111,12 @@ __global__ void __launch_bounds__(ptycho_block<DET>(), 1)
     for (int e = threadIdx.x; e < DET * DET; e += NT) out[e] = cmul(fr[(e / DET) * PITCH + e % DET], ph);
 }
 
-template <int DET>
+template <int DET, int RESID>
 __global__ void __launch_bounds__(ptycho_block<DET>(), 1)
     k_ptycho_adj_small(const float2 *__restrict__ g, float2 *__restrict__ psi, const int *__restrict__ corner,
                  const float2 *__restrict__ phase, const float2 *__restrict__ prb, int nz, int n, int nscan,
-                 int P, float c, float scale, const float2 *__restrict__ tw)
+                 int P, float c, float scale, const float2 *__restrict__ tw, const float *__restrict__ data,
+                 float dscale)
 {
     constexpr int T = ptycho_fft_threads<DET>(), NT = ptycho_block<DET>(), PITCH = DET + 1;
     extern __shared__ float2 fr[];
@@ -110,7 +133,8 @@ __global__ void __launch_bounds__(ptycho_block<DET>(), 1)
         if (stx < 0 || sty < 0) continue;
         const float2 ph = phase[fid];
         const float2 *in = g + (size_t)fid * DET * DET;
-        for (int e = threadIdx.x; e < DET * DET; e += NT) fr[(e / DET) * PITCH + e % DET] = cmulc(ph, in[e]);
+        for (int e = threadIdx.x; e < DET * DET; e += NT)
+            fr[(e / DET) * PITCH + e % DET] = cmulc(ph, resid<RESID>(in[e], data, (size_t)fid * DET * DET + e, dscale));
         __syncthreads();
         ptfft::fft<DET, +1, T>(fr + f * PITCH, 1, t, tw);
         ptfft::fft<DET, +1, T>(fr + f, PITCH, t, tw);
@@ -252,11 +276,11 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
 }
 
 // grid (parts, ntheta): block (part, angle) owns slab dst[angle][part]
-template <int DET>
+template <int DET, int RESID>
 __global__ void __launch_bounds__(PF<DET>::NT, 1)
     k_ptycho_adj(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                  const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                 int P, float scale, const float2 *__restrict__ tw)
+                 int P, float scale, const float2 *__restrict__ tw, const float *__restrict__ data, float dscale)
 {
     using F = PF<DET>;
     extern __shared__ float2 sm[];
@@ -282,7 +306,10 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
         for (int c = 0; c < F::CPG; ++c) {
             const int kx = grp + F::NG * c;
 #pragma unroll
-            for (int m = 0; m < F::N1; ++m) v[c][m] = scale * cmulc(ph, __ldg(&in[kx * DET + t + F::N2 * m]));
+            for (int m = 0; m < F::N1; ++m) {
+                const int e = kx * DET + t + F::N2 * m;
+                v[c][m] = scale * cmulc(ph, resid<RESID>(__ldg(&in[e]), data, (size_t)fid * DET * DET + e, dscale));
+            }
             line_dft<DET, +1>(v[c], t, sc, tws);
         }
         __syncthreads();
@@ -469,11 +496,12 @@ __device__ __forceinline__ void prefetch_half_frame(float4 *dst, const float2 *i
 // grid (parts, ntheta): block (part, angle) owns slab dst[angle][part].
 // While the current frame finishes, the next frame's rows 0..63 are already
 // on their way into the idle half of the shared frame buffer.
-template <bool FULL>
+template <bool FULL, int RESID>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                    int P, float scale, const float2 *__restrict__ tw)
+                    int P, float scale, const float2 *__restrict__ tw, const float *__restrict__ data,
+                    float dscale)
 {
     extern __shared__ float4 sm4[];
     float4 *fr = sm4;
@@ -505,15 +533,18 @@ __global__ void __launch_bounds__(512, 1)
         // rows 64..127 from global first, so their latency hides behind row 0..63's work
 #pragma unroll
         for (int m = 0; m < 16; ++m) v[1][m] = __ldg(&in[(grp + 64) * 128 + t + 8 * m]);
+        const size_t fbase = (size_t)fid * 128 * 128;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int ky = t + 8 * m;
             const float4 q = pre[grp * 64 + ((ky >> 1) ^ ((grp & 1) << 2))];
-            v[0][m] = scale * cmulc(ph, (ky & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y));
+            const float2 x = (ky & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
+            v[0][m] = scale * cmulc(ph, resid<RESID>(x, data, fbase + grp * 128 + ky, dscale));
         }
         line_dft128<+1>(v[0], t, sc, tws);
 #pragma unroll
-        for (int m = 0; m < 16; ++m) v[1][m] = scale * cmulc(ph, v[1][m]);
+        for (int m = 0; m < 16; ++m)
+            v[1][m] = scale * cmulc(ph, resid<RESID>(v[1][m], data, fbase + (grp + 64) * 128 + t + 8 * m, dscale));
         line_dft128<+1>(v[1], t, sc, tws);
         __syncthreads();
 #pragma unroll
@@ -603,90 +634,100 @@ namespace {
 template <int DET>
 int ptycho_attrs()
 {
+#define PT_ATTR(K, S) PT_CUDA(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(S)))
     if constexpr (DET < 16) {
         const int s = DET * (DET + 1) * sizeof(float2);
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd_small<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj_small<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
-    } else if constexpr (DET == 128) {
-        const int s = (int)PF<DET>::SMEM;
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd128<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, P128_SMEM));
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd128<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, P128_SMEM));
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj128<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, P128_SMEM));
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj128<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, P128_SMEM));
+        PT_ATTR(k_ptycho_fwd_small<DET>, s);
+        PT_ATTR((k_ptycho_adj_small<DET, 0>), s);
+        PT_ATTR((k_ptycho_adj_small<DET, 1>), s);
+        PT_ATTR((k_ptycho_adj_small<DET, 2>), s);
     } else {
         const int s = (int)PF<DET>::SMEM;
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_fwd<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
-        PT_CUDA(cudaFuncSetAttribute(k_ptycho_adj<DET>, cudaFuncAttributeMaxDynamicSharedMemorySize, s));
+        PT_ATTR(k_ptycho_fwd<DET>, s);
+        PT_ATTR((k_ptycho_adj<DET, 0>), s);
+        PT_ATTR((k_ptycho_adj<DET, 1>), s);
+        PT_ATTR((k_ptycho_adj<DET, 2>), s);
+        if constexpr (DET == 128) {
+            PT_ATTR(k_ptycho_fwd128<true>, P128_SMEM);
+            PT_ATTR(k_ptycho_fwd128<false>, P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 0>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<false, 0>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 1>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<false, 1>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 2>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<false, 2>), P128_SMEM);
+        }
     }
+#undef PT_ATTR
     return PT_OK;
 }
 
-template <int DET>
-int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st)
+template <int DET, int RESID>
+int ptycho_adj_launch(pt_ptycho *h, float2 *out, const float2 *in, float scale, const float *data, float dscale,
+                      cudaStream_t st)
 {
     if constexpr (DET < 16) {
         const size_t s = DET * (DET + 1) * sizeof(float2);
-        if (!adj) {
-            k_ptycho_fwd_small<DET><<<dim3(h->nscan, h->ntheta), ptycho_block<DET>(), s, st>>>(
-                in, out, h->corner, h->phase, h->prb, h->nz, h->n, h->nscan, h->P, h->c, scale, h->tw);
-            PT_LAUNCHED("k_ptycho_fwd_small");
-        } else {
-            k_ptycho_adj_small<DET><<<h->ntheta, ptycho_block<DET>(), s, st>>>(
-                in, out, h->corner, h->phase, h->prb, h->nz, h->n, h->nscan, h->P, h->c, scale, h->tw);
-            PT_LAUNCHED("k_ptycho_adj_small");
-        }
+        k_ptycho_adj_small<DET, RESID><<<h->ntheta, ptycho_block<DET>(), s, st>>>(
+            in, out, h->corner, h->phase, h->prb, h->nz, h->n, h->nscan, h->P, h->c, scale, h->tw, data, dscale);
+        PT_LAUNCHED("k_ptycho_adj_small");
+        return PT_OK;
     } else {
         using F = PF<DET>;
-        const int nframes = h->ntheta * h->nscan;
-        const bool full = (h->P == DET);
-        if (!adj) {
-            // the det = 128 kernel writes frames with 16-byte stores
-            const bool aligned16 = ((uintptr_t)out % 16) == 0;
-            if constexpr (DET == 128) {
-                if (!aligned16)
-                    k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz,
-                                                                      h->n, h->nscan, nframes, h->P, scale, h->tw);
-                else if (full)
-                    k_ptycho_fwd128<true><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz,
-                                                                          h->n, h->nscan, nframes, h->P, scale, h->tw);
-                else
-                    k_ptycho_fwd128<false><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT,
-                                                                           h->nz, h->n, h->nscan, nframes, h->P, scale,
-                                                                           h->tw);
-            } else {
-                k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
-                                                                  h->nscan, nframes, h->P, scale, h->tw);
-            }
-            PT_LAUNCHED("k_ptycho_fwd");
-        } else {
-            float2 *dst = h->parts > 1 ? h->partial : out;
-            // the det = 128 adjoint prefetches frames with 16-byte async copies
-            const bool in_aligned16 = ((uintptr_t)in % 16) == 0;
-            if constexpr (DET == 128) {
-                if (!in_aligned16)
-                    k_ptycho_adj<DET><<<dim3(h->parts, h->ntheta), F::NT, F::SMEM, st>>>(
-                        in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
-                else if (full)
-                    k_ptycho_adj128<true><<<dim3(h->parts, h->ntheta), 512, P128_SMEM, st>>>(
-                        in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
-                else
-                    k_ptycho_adj128<false><<<dim3(h->parts, h->ntheta), 512, P128_SMEM, st>>>(
-                        in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
-            } else {
-                k_ptycho_adj<DET><<<dim3(h->parts, h->ntheta), F::NT, F::SMEM, st>>>(
-                    in, dst, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw);
-            }
-            PT_LAUNCHED("k_ptycho_adj");
-            if (h->parts > 1) {
-                const size_t slab = (size_t)h->nz * h->n, total = slab * h->ntheta;
-                const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
-                k_ptycho_reduce<<<blocks, 256, 0, st>>>(h->partial, out, slab, h->parts, total);
-                PT_LAUNCHED("k_ptycho_reduce");
-            }
+        float2 *dst = h->parts > 1 ? h->partial : out;
+        const dim3 grid(h->parts, h->ntheta);
+        // the det = 128 adjoint prefetches frames with 16-byte async copies
+        const bool fast128 = DET == 128 && ((uintptr_t)in % 16) == 0;
+        if (fast128 && h->P == DET)
+            k_ptycho_adj128<true, RESID><<<grid, 512, P128_SMEM, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz,
+                                                                      h->n, h->nscan, h->P, scale, h->tw, data, dscale);
+        else if (fast128)
+            k_ptycho_adj128<false, RESID><<<grid, 512, P128_SMEM, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz,
+                                                                       h->n, h->nscan, h->P, scale, h->tw, data,
+                                                                       dscale);
+        else
+            k_ptycho_adj<DET, RESID><<<grid, F::NT, F::SMEM, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz, h->n,
+                                                                  h->nscan, h->P, scale, h->tw, data, dscale);
+        PT_LAUNCHED("k_ptycho_adj");
+        if (h->parts > 1) {
+            const size_t slab = (size_t)h->nz * h->n, total = slab * h->ntheta;
+            const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+            k_ptycho_reduce<<<blocks, 256, 0, st>>>(h->partial, out, slab, h->parts, total);
+            PT_LAUNCHED("k_ptycho_reduce");
         }
+        return PT_OK;
     }
+}
+
+template <int DET>
+int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st, int resid_mode,
+               const float *data, float dscale)
+{
+    if (adj) {
+        if (resid_mode == 1) return ptycho_adj_launch<DET, 1>(h, out, in, scale, data, dscale, st);
+        if (resid_mode == 2) return ptycho_adj_launch<DET, 2>(h, out, in, scale, data, dscale, st);
+        return ptycho_adj_launch<DET, 0>(h, out, in, scale, data, dscale, st);
+    }
+    const int nframes = h->ntheta * h->nscan;
+    if constexpr (DET < 16) {
+        const size_t s = DET * (DET + 1) * sizeof(float2);
+        k_ptycho_fwd_small<DET><<<dim3(h->nscan, h->ntheta), ptycho_block<DET>(), s, st>>>(
+            in, out, h->corner, h->phase, h->prb, h->nz, h->n, h->nscan, h->P, h->c, scale, h->tw);
+    } else {
+        using F = PF<DET>;
+        // the det = 128 kernel writes frames with 16-byte stores
+        const bool fast128 = DET == 128 && ((uintptr_t)out % 16) == 0;
+        if (fast128 && h->P == DET)
+            k_ptycho_fwd128<true><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
+                                                                  h->nscan, nframes, h->P, scale, h->tw);
+        else if (fast128)
+            k_ptycho_fwd128<false><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz,
+                                                                   h->n, h->nscan, nframes, h->P, scale, h->tw);
+        else
+            k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
+                                                              h->nscan, nframes, h->P, scale, h->tw);
+    }
+    PT_LAUNCHED("k_ptycho_fwd");
     return PT_OK;
 }
 
@@ -708,10 +749,11 @@ int ptycho_set_attrs(int d)
     return PT_ERR_UNSUPPORTED;
 }
 
-int ptycho_dispatch(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st)
+int ptycho_dispatch(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st,
+                    int resid_mode = 0, const float *data = nullptr, float dscale = 1.f)
 {
 #define PT_CASE(D) \
-    if (h->det == D) return ptycho_run<D>(h, adj, out, in, scale, st);
+    if (h->det == D) return ptycho_run<D>(h, adj, out, in, scale, st, resid_mode, data, dscale);
     PT_PTYCHO_DETS(PT_CASE)
 #undef PT_CASE
     pt::set_error("ptychofft: detector size %d not compiled", h->det);
@@ -880,4 +922,22 @@ extern "C" int pt_ptycho_fwd_scaled(pt_ptycho *h, void *g, const void *f, float 
 extern "C" int pt_ptycho_adj_scaled(pt_ptycho *h, void *f, const void *g, float scale, void *stream)
 {
     return ptycho_call(h, true, f, g, scale, stream);
+}
+
+extern "C" int pt_ptycho_adj_resid(pt_ptycho *h, void *f, const void *fpsi, const float *data, float dscale,
+                                   int model, float scale, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h != nullptr, "ptychofft: null handle");
+    PT_CHECK_ARG(f != nullptr && fpsi != nullptr && data != nullptr, "ptychofft.adj_resid: null array pointer");
+    PT_CHECK_ARG(model == 0 || model == 1, "ptychofft.adj_resid: model 0 (poisson) or 1 (gaussian)");
+    if (!h->ready) {
+        pt::set_error("ptychofft.adj_resid: setobj(scan, prb) has not been called");
+        return PT_ERR_STATE;
+    }
+    int dev = -1;
+    PT_CUDA(cudaGetDevice(&dev));
+    PT_CHECK_ARG(dev == h->device, "ptychofft handle belongs to device %d, current device is %d", h->device, dev);
+    return ptycho_dispatch(h, true, (float2 *)f, (const float2 *)fpsi, scale, (cudaStream_t)stream, model + 1, data,
+                           dscale);
 }

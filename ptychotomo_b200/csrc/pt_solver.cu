@@ -123,42 +123,89 @@ __global__ void __launch_bounds__(RT) k_reduce(int op, const float2 *__restrict_
 }
 
 // ---- ptycho data terms over detector frames (solver.py:208-214, :294-298) ---
-// model 0 Poisson, 1 Gaussian.  With t(x) = |x|^2 - 2 D log(max(|x|, 1e-32))
-// (Poisson) or (|x| - sqrt D)^2 (Gaussian), out[j] = sum t(f) - t(f + g_j d):
-// the decrease of the data term for step g_j, formed per element in FP64 so
-// that it carries no cancellation of the (much larger) term itself.  |x| is
-// the float32 modulus, as np.abs / cp.abs of complex64.
-__device__ __forceinline__ double data_term(float a, float dd, int model)
+// model 0 Poisson, 1 Gaussian.  With t(y) = |y|^2 - 2 D log(max(|y|, 1e-32))
+// (Poisson) or (|y| - sqrt D)^2 (Gaussian), out[j] = sum t(f) - t(f + g_j d):
+// the decrease of the data term for step g_j.  It is formed per element in
+// FP32 without cancellation, then summed in FP64: with a2 = |f|^2 and
+//   delta = |f + g d|^2 - a2 = 2 g Re(conj(f) d) + g^2 |d|^2,
+// Poisson:  t(f) - t(f + g d) = -delta + D log1p(delta / a2),
+// Gaussian: t(f) - t(f + g d) = -delta / (|f| + |f + g d|) * (|f| + |f + g d| - 2 sqrt D);
+// moduli below the 1e-32 clamp take the direct formula.  Sums are FP64.
+// FP64 form, used for moduli below 1e-15 (where |f|^2 would underflow in FP32)
+__device__ __forceinline__ double ls_decrease_f64(float2 f, float2 d, float g, float D, int model)
 {
-    if (model == 0) return (double)a * a - 2.0 * (double)dd * log(fmax((double)a, 1e-32));
-    const double t = (double)a - (double)sqrtf(dd);
-    return t * t;
+    const double a2 = (double)f.x * f.x + (double)f.y * f.y;
+    const double fd = (double)f.x * d.x + (double)f.y * d.y;
+    const double d2 = (double)d.x * d.x + (double)d.y * d.y;
+    const double delta = 2.0 * g * fd + (double)g * g * d2;
+    const double b2 = a2 + delta;
+    if (model == 0) {
+        const double lim = 1e-64;  // (1e-32)^2: mlog's clamp
+        const double la = a2 >= lim ? 0.5 * log(a2) : -73.68272297580946;  // log 1e-32
+        const double lb = b2 >= lim ? 0.5 * log(b2) : -73.68272297580946;
+        return -delta - 2.0 * (double)D * (la - lb);
+    }
+    const double fa = sqrt(a2), fb = sqrt(fmax(b2, 0.0));
+    const double sum = fa + fb;
+    if (sum == 0.0) return 0.0;
+    return -delta / sum * (sum - 2.0 * (double)sqrtf(D));
 }
 
+// JB = accumulator bucket (2, 8 or 16 step lengths); J <= JB are used
+template <int JB>
 __global__ void __launch_bounds__(RT) k_ls_frames(const float2 *__restrict__ f, const float2 *__restrict__ d,
                                                   const float *__restrict__ D, float dscale, size_t n, int model,
                                                   const double *__restrict__ gam, int J, double *__restrict__ work)
 {
-    double acc[MAXK];
+    double acc[JB];
 #pragma unroll
-    for (int j = 0; j < MAXK; ++j) acc[j] = 0;
-    float gj[MAXK];
+    for (int j = 0; j < JB; ++j) acc[j] = 0;
+    float gj[JB];
 #pragma unroll
-    for (int j = 0; j < MAXK; ++j) gj[j] = j < J ? (float)gam[j] : 0.f;
+    for (int j = 0; j < JB; ++j) gj[j] = j < J ? (float)gam[j] : 0.f;
     for (size_t i = (size_t)blockIdx.x * RT + threadIdx.x; i < n; i += (size_t)gridDim.x * RT) {
         const float2 x = f[i];
         const float2 y = d[i];
         const float dd = D[i] * dscale;
-        const double t0 = data_term(hypotf(x.x, x.y), dd, model);
+        const float a2 = x.x * x.x + x.y * x.y;
+        const float fdot = x.x * y.x + x.y * y.y;
+        const float d2 = y.x * y.x + y.y * y.y;
+        const float sq = sqrtf(dd);
+        const float fa = sqrtf(a2);
+        const bool tiny = !(a2 >= 1e-30f);
 #pragma unroll
-        for (int j = 0; j < MAXK; ++j) {
+        for (int j = 0; j < JB; ++j) {
             if (j < J) {
-                const float2 v = make_float2(x.x + gj[j] * y.x, x.y + gj[j] * y.y);
-                acc[j] += t0 - data_term(hypotf(v.x, v.y), dd, model);
+                const float g = gj[j];
+                const float delta = g * (2.f * fdot + g * d2);
+                const float b2 = a2 + delta;
+                double dec;
+                if (tiny || !(b2 >= 1e-30f)) {
+                    dec = ls_decrease_f64(x, y, g, dd, model);
+                } else if (model == 0) {
+                    dec = (double)(dd * log1pf(delta / a2) - delta);
+                } else {
+                    const float s2 = fa + sqrtf(b2);
+                    dec = (double)(-delta / s2 * (s2 - 2.f * sq));
+                }
+                acc[j] += dec;
             }
         }
     }
-    block_reduce_store<MAXK>(acc, work, blockIdx.x, gridDim.x);
+    block_reduce_store<JB>(acc, work, blockIdx.x, gridDim.x);
+}
+
+int launch_ls_frames(const float2 *f, const float2 *d, const float *data, float dscale, size_t n, int model,
+                     const double *gammas, int J, double *work, cudaStream_t st)
+{
+    if (J <= 2)
+        k_ls_frames<2><<<RB, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
+    else if (J <= 8)
+        k_ls_frames<8><<<RB, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
+    else
+        k_ls_frames<16><<<RB, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
+    PT_LAUNCHED("k_ls_frames");
+    return PT_OK;
 }
 
 // Lagrangian data term, solver.py:294-298.  Poisson also subtracts the
@@ -379,9 +426,9 @@ extern "C" int pt_ls_frames(const void *f, const void *d, const float *data, flo
     PT_CHECK_ARG(J >= 1 && J <= MAXK, "ls_frames: 1 <= J <= %d", MAXK);
     PT_CHECK_ARG(model == 0 || model == 1, "ls_frames: model 0 (poisson) or 1 (gaussian)");
     cudaStream_t st = (cudaStream_t)stream;
-    k_ls_frames<<<RB, RT, 0, st>>>((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J,
-                                   (double *)work);
-    PT_LAUNCHED("k_ls_frames");
+    const int rc = launch_ls_frames((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J,
+                                    (double *)work, st);
+    if (rc != PT_OK) return rc;
     k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, J, RB, 0);
     PT_LAUNCHED("k_finish");
     return PT_OK;
@@ -555,8 +602,8 @@ extern "C" int pt_ls_frames_noalloc(const void *f, const void *d, const float *d
     cudaStream_t st = (cudaStream_t)stream;
     // every partial that k_finish reads (J x RB) is written by k_ls_frames in
     // this call, so nothing in the shared scratch needs clearing first
-    k_ls_frames<<<RB, RT, 0, st>>>((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J, work);
-    PT_LAUNCHED("k_ls_frames");
+    const int rc2 = launch_ls_frames((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J, work, st);
+    if (rc2 != PT_OK) return rc2;
     k_finish<<<1, RT, 0, st>>>(work, (double *)out, J, RB, 0);
     PT_LAUNCHED("k_finish");
     return PT_OK;

@@ -95,6 +95,11 @@ class ptychofft:  # noqa: N801 - reference class name
             check(lib().pt_ptycho_adj_scaled(self._h, as_ptr(f), as_ptr(g), float(scale), _s(stream)),
                   "ptychofft.adj")
 
+    def adj_resid(self, f, fpsi, data, dscale, model, scale=1.0, stream=None):
+        """Gradient of the data term: f = scale * Q* F* residual(fpsi, dscale * data)."""
+        check(lib().pt_ptycho_adj_resid(self._h, as_ptr(f), as_ptr(fpsi), as_ptr(data), float(dscale), int(model),
+                                        float(scale), _s(stream)), "ptychofft.adj_resid")
+
     def free(self):
         if getattr(self, "_h", None):
             lib().pt_ptycho_destroy(self._h)

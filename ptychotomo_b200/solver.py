@@ -12,8 +12,9 @@ Differences from the reference, all deliberate:
   Lagrangian) accumulate in FP64;
 * the line searches evaluate the decrease minf(x) - minf(x + g d) directly:
   quadratic terms in closed form (||w + g d||^2 - ||w||^2 = 2 g Re<w, d> +
-  g^2 ||d||^2) and the Poisson / Gaussian term per element in FP64 for up to
-  16 step lengths per pass.  They take the halving decisions of
+  g^2 ||d||^2) and the Poisson / Gaussian term per element without
+  cancellation (log1p of the relative change), summed in FP64, for 2, then
+  8, then 16 step lengths per pass.  They take the halving decisions of
   solver.py:171-177 exactly, except where the decrease is within FP32
   rounding of zero (near convergence), where the reference's own float
   atomics make it differ from run to run;
@@ -240,9 +241,8 @@ class Solver:
         w = torch.empty_like(psi)
         for i in range(piter):
             fpsi = self.fwd_ptycho(psi)
-            res = K.residual(torch.empty_like(fpsi), fpsi, data, dscale, mdl)
-            grad = self.adj_ptycho(res)
-            del res
+            grad = self._empty([self.ptheta, self.nz, self.n])   # Q*F*(residual), residual formed on load
+            self.cl_ptycho.adj_resid(grad, fpsi, data, dscale, mdl, scale=self.coefptycho)
             K.lincomb(w, [(1.0, h), (-1.0, psi), (1.0 / rho, lamd)])     # h - psi + lamd/rho
             K.lincomb(grad, [(1.0, grad), (-rho, w)])
             if i == 0:
@@ -256,8 +256,12 @@ class Solver:
             _, w_d, d2 = red.quad3(w, d)
             # minf(psi) - minf(psi + g d) = data-term decrease (per element, FP64)
             #   + rho (2 g Re<w, d> - g^2 ||d||^2)  for the penalty rho ||w - g d||^2
+            npass = 0
             while True:
-                gs = [gamma * 0.5 ** j for j in range(16)]
+                # gamma usually survives: try (g, g/2) first, then 8, then 16 halvings per pass
+                J = (2, 8, 16)[min(npass, 2)]
+                npass += 1
+                gs = [gamma * 0.5 ** j for j in range(J)]
                 vals = red.ls_frames(fpsi, fd, data, dscale, mdl, gs)
                 chosen = None
                 for g, dec_data in zip(gs, vals):

@@ -247,3 +247,21 @@ def test_ptycho_det128_misaligned_adjoint_input():
     out = torch.zeros((2, 140, 130), dtype=torch.complex64, device="cuda")
     op.adj(out, src.data_ptr())
     assert rel(out.cpu().numpy(), orc.adj(g)) <= TOL
+
+
+@pytest.mark.parametrize("ntheta,nz,n,nscan,det,nprb", [(2, 130, 140, 6, 128, 128), (2, 100, 110, 4, 128, 96),
+                                                       (2, 64, 64, 9, 64, 32), (3, 20, 20, 3, 8, 8)])
+@pytest.mark.parametrize("model", [0, 1])
+def test_ptycho_adjoint_with_fused_residual(ntheta, nz, n, nscan, det, nprb, model):
+    """adj_resid == adj(residual(fpsi, data)), the gradient of solver.py:220-224."""
+    from ptychotomo_b200 import kernels
+    rng = np.random.default_rng(det + model)
+    op, _, _, _ = make_ptycho(ntheta, nz, n, nscan, det, nprb, rng)
+    fpsi = dev(crand(rng, (ntheta, nscan, det, det)))
+    data = dev(rng.poisson(3.0, (ntheta, nscan, det, det)).astype(np.float32))
+    res = kernels.residual(torch.empty_like(fpsi), fpsi, data, 0.7, model)
+    ref = torch.zeros((ntheta, nz, n), dtype=torch.complex64, device="cuda")
+    op.adj(ref, res, scale=0.5)
+    out = torch.zeros_like(ref)
+    op.adj_resid(out, fpsi, data, 0.7, model, scale=0.5)
+    assert rel(out.cpu().numpy(), ref.cpu().numpy()) <= 1e-6
