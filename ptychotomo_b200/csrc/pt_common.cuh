@@ -23,6 +23,28 @@ __host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b)
 }
 __host__ __device__ __forceinline__ float2 czero() { return make_float2(0.f, 0.f); }
 
+// ---- data-term residual of the ptycho gradient (solver.py:220-224) ----------
+// D = measured intensity (already scaled).  Poisson: x - D x / (|x|^2 + 1e-32).
+// Gaussian: x - sqrt(D) exp(i angle(x)), formed as x (1 - sqrt(D) / |x|); for
+// |x|^2 < 1e-30 (and x = 0, where angle is 0) through atan2 as written.
+__device__ __forceinline__ float2 pt_residual_poisson(float2 x, float D)
+{
+    const float q = D / (x.x * x.x + x.y * x.y + 1e-32f);
+    return make_float2(x.x - q * x.x, x.y - q * x.y);
+}
+__device__ __forceinline__ float2 pt_residual_gaussian(float2 x, float D)
+{
+    const float sq = sqrtf(D);
+    const float a2 = x.x * x.x + x.y * x.y;
+    if (a2 >= 1e-30f) {
+        const float r = sq * rsqrtf(a2);
+        return make_float2(x.x - r * x.x, x.y - r * x.y);
+    }
+    float sn, cs;
+    sincosf(atan2f(x.y, x.x), &sn, &cs);
+    return make_float2(x.x - sq * cs, x.y - sq * sn);
+}
+
 namespace pt {
 
 // Thread-local last-error text (defined in pt_capi.cu).

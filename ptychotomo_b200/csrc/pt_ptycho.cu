@@ -33,23 +33,25 @@ constexpr double PI_REF = 3.1415926535;  // kernels.cuh:1
 // Residual of the ptycho data term applied to a frame value x on load
 // (solver.py:220-224, D = dscale * data): RESID 0 = none (plain adjoint),
 // 1 = Poisson x - D x / (|x|^2 + 1e-32), 2 = Gaussian x - sqrt(D) exp(i angle x).
+// RESID 0: the frame itself; 1: Poisson residual; 2: Gaussian residual, with
+// D = dscale * data (the gradient's input, solver.py:220-224)
+template <int RESID>
+__device__ __forceinline__ float2 resid_of(float2 x, float D)
+{
+    if constexpr (RESID == 1)
+        return pt_residual_poisson(x, D);
+    else if constexpr (RESID == 2)
+        return pt_residual_gaussian(x, D);
+    else
+        return x;
+}
 template <int RESID>
 __device__ __forceinline__ float2 resid(float2 x, const float *__restrict__ data, size_t idx, float dscale)
 {
-    if constexpr (RESID == 0) {
+    if constexpr (RESID == 0)
         return x;
-    } else {
-        const float D = __ldg(&data[idx]) * dscale;
-        if constexpr (RESID == 1) {
-            const float q = D / (x.x * x.x + x.y * x.y + 1e-32f);
-            return make_float2(x.x - q * x.x, x.y - q * x.y);
-        } else {
-            float sn, cs;
-            sincosf(atan2f(x.y, x.x), &sn, &cs);
-            const float sq = sqrtf(D);
-            return make_float2(x.x - sq * cs, x.y - sq * sn);
-        }
-    }
+    else
+        return resid_of<RESID>(x, __ldg(&data[idx]) * dscale);
 }
 
 template <int DET>
@@ -366,6 +368,8 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
 // group hit 8 distinct 4-bank groups both when writing (q varies) and when
 // reading (c varies).  The group exchange uses the same trick.
 constexpr int P128_SMEM = (64 * 128) * 16 + 128 * 8;
+// the fused-residual adjoint also stages the frame's 128 x 128 counts
+constexpr int P128_SMEM_RESID = P128_SMEM + 128 * 128 * 4;
 
 template <int DIR>
 __device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, const float2 *tws)
@@ -493,6 +497,24 @@ __device__ __forceinline__ void prefetch_half_frame(float4 *dst, const float2 *i
     cp_async_commit();
 }
 
+// The 128 x 128 counts of one frame (64 KB) -> shared [row][128], row r's
+// columns rotated by 8 (r & 3) so that four groups reading rows r..r+3 at
+// the same columns hit distinct banks.
+__device__ __forceinline__ void prefetch_counts(float *dst, const float *data)
+{
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int id = threadIdx.x + 512 * i;
+        const int row = id >> 5, c4 = (id & 31) * 4;
+        cp_async16(dst + row * 128 + ((c4 + 8 * (row & 3)) & 127), data + row * 128 + c4);
+    }
+    cp_async_commit();
+}
+__device__ __forceinline__ float staged_count(const float *cnt, int row, int col)
+{
+    return cnt[row * 128 + ((col + 8 * (row & 3)) & 127)];
+}
+
 // grid (parts, ntheta): block (part, angle) owns slab dst[angle][part].
 // While the current frame finishes, the next frame's rows 0..63 are already
 // on their way into the idle half of the shared frame buffer.
@@ -507,6 +529,7 @@ __global__ void __launch_bounds__(512, 1)
     float4 *fr = sm4;
     float4 *pre = sm4 + 64 * 64;  // upper 64 KB of the frame buffer
     float2 *tws = reinterpret_cast<float2 *>(sm4 + 64 * 128);
+    float *cnt = reinterpret_cast<float *>(sm4 + 64 * 128 + 64);  // RESID: this frame's counts
     const int part = blockIdx.x, parts = gridDim.x, th = blockIdx.y;
     float2 *slab = dst + ((size_t)th * parts + part) * nz * n;
     for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
@@ -515,17 +538,25 @@ __global__ void __launch_bounds__(512, 1)
     float4 *sc = fr + grp * 64;
     const int off = FULL ? 0 : (128 - P) / 2;
     const float2 *gth = g + (size_t)th * nscan * 128 * 128;
-    if (part < nscan) prefetch_half_frame(pre, gth + (size_t)part * 128 * 128);
+    const float *dth = RESID ? data + (size_t)th * nscan * 128 * 128 : nullptr;
+    if (part < nscan) {
+        prefetch_half_frame(pre, gth + (size_t)part * 128 * 128);
+        if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)part * 128 * 128);
+    }
     for (int s = part; s < nscan; s += parts) {
         const int fid = th * nscan + s;
         const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
         const float2 *in = gth + (size_t)s * 128 * 128;
-        const float2 *in_next = s + parts < nscan ? in + (size_t)parts * 128 * 128 : nullptr;
+        const bool more = s + parts < nscan;
+        const float2 *in_next = more ? in + (size_t)parts * 128 * 128 : nullptr;
         cp_async_wait_all();
         __syncthreads();
         if (stx < 0 || sty < 0) {  // skipped scan: keep the prefetch chain going
             __syncthreads();
-            if (in_next) prefetch_half_frame(pre, in_next);
+            if (more) {
+                prefetch_half_frame(pre, in_next);
+                if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
+            }
             continue;
         }
         const float2 ph = phase[fid];
@@ -533,18 +564,22 @@ __global__ void __launch_bounds__(512, 1)
         // rows 64..127 from global first, so their latency hides behind row 0..63's work
 #pragma unroll
         for (int m = 0; m < 16; ++m) v[1][m] = __ldg(&in[(grp + 64) * 128 + t + 8 * m]);
-        const size_t fbase = (size_t)fid * 128 * 128;
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             const int ky = t + 8 * m;
             const float4 q = pre[grp * 64 + ((ky >> 1) ^ ((grp & 1) << 2))];
             const float2 x = (ky & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
-            v[0][m] = scale * cmulc(ph, resid<RESID>(x, data, fbase + grp * 128 + ky, dscale));
+            float D = 0.f;
+            if constexpr (RESID != 0) D = staged_count(cnt, grp, ky) * dscale;
+            v[0][m] = scale * cmulc(ph, resid_of<RESID>(x, D));
         }
         line_dft128<+1>(v[0], t, sc, tws);
 #pragma unroll
-        for (int m = 0; m < 16; ++m)
-            v[1][m] = scale * cmulc(ph, resid<RESID>(v[1][m], data, fbase + (grp + 64) * 128 + t + 8 * m, dscale));
+        for (int m = 0; m < 16; ++m) {
+            float D = 0.f;
+            if constexpr (RESID != 0) D = staged_count(cnt, grp + 64, t + 8 * m) * dscale;
+            v[1][m] = scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
+        }
         line_dft128<+1>(v[1], t, sc, tws);
         __syncthreads();
 #pragma unroll
@@ -564,7 +599,10 @@ __global__ void __launch_bounds__(512, 1)
             v[1][m] = make_float2(q.z, q.w);
         }
         __syncthreads();
-        if (in_next) prefetch_half_frame(pre, in_next);
+        if (more) {
+            prefetch_half_frame(pre, in_next);
+            if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
+        }
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             line_dft128<+1>(v[c], t, sc, tws);
@@ -652,10 +690,10 @@ int ptycho_attrs()
             PT_ATTR(k_ptycho_fwd128<false>, P128_SMEM);
             PT_ATTR((k_ptycho_adj128<true, 0>), P128_SMEM);
             PT_ATTR((k_ptycho_adj128<false, 0>), P128_SMEM);
-            PT_ATTR((k_ptycho_adj128<true, 1>), P128_SMEM);
-            PT_ATTR((k_ptycho_adj128<false, 1>), P128_SMEM);
-            PT_ATTR((k_ptycho_adj128<true, 2>), P128_SMEM);
-            PT_ATTR((k_ptycho_adj128<false, 2>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 1>), P128_SMEM_RESID);
+            PT_ATTR((k_ptycho_adj128<false, 1>), P128_SMEM_RESID);
+            PT_ATTR((k_ptycho_adj128<true, 2>), P128_SMEM_RESID);
+            PT_ATTR((k_ptycho_adj128<false, 2>), P128_SMEM_RESID);
         }
     }
 #undef PT_ATTR
@@ -676,15 +714,15 @@ int ptycho_adj_launch(pt_ptycho *h, float2 *out, const float2 *in, float scale, 
         using F = PF<DET>;
         float2 *dst = h->parts > 1 ? h->partial : out;
         const dim3 grid(h->parts, h->ntheta);
-        // the det = 128 adjoint prefetches frames with 16-byte async copies
-        const bool fast128 = DET == 128 && ((uintptr_t)in % 16) == 0;
+        // the det = 128 adjoint prefetches frames (and counts) with 16-byte async copies
+        const bool fast128 = DET == 128 && ((uintptr_t)in % 16) == 0 && (RESID == 0 || (uintptr_t)data % 16 == 0);
+        const int smem = RESID ? P128_SMEM_RESID : P128_SMEM;
         if (fast128 && h->P == DET)
-            k_ptycho_adj128<true, RESID><<<grid, 512, P128_SMEM, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz,
-                                                                      h->n, h->nscan, h->P, scale, h->tw, data, dscale);
+            k_ptycho_adj128<true, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz, h->n,
+                                                                 h->nscan, h->P, scale, h->tw, data, dscale);
         else if (fast128)
-            k_ptycho_adj128<false, RESID><<<grid, 512, P128_SMEM, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz,
-                                                                       h->n, h->nscan, h->P, scale, h->tw, data,
-                                                                       dscale);
+            k_ptycho_adj128<false, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz,
+                                                                  h->n, h->nscan, h->P, scale, h->tw, data, dscale);
         else
             k_ptycho_adj<DET, RESID><<<grid, F::NT, F::SMEM, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz, h->n,
                                                                   h->nscan, h->P, scale, h->tw, data, dscale);

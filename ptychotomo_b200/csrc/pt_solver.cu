@@ -11,6 +11,7 @@
 // Reductions are deterministic: fixed grid, per-block partials in a caller
 // workspace, then one block sums the partials in order.
 #include <cmath>
+#include <cstdint>
 
 #include "pt_common.cuh"
 
@@ -125,13 +126,13 @@ __global__ void __launch_bounds__(RT) k_reduce(int op, const float2 *__restrict_
 // ---- ptycho data terms over detector frames (solver.py:208-214, :294-298) ---
 // model 0 Poisson, 1 Gaussian.  With t(y) = |y|^2 - 2 D log(max(|y|, 1e-32))
 // (Poisson) or (|y| - sqrt D)^2 (Gaussian), out[j] = sum t(f) - t(f + g_j d):
-// the decrease of the data term for step g_j.  It is formed per element in
-// FP32 without cancellation, then summed in FP64: with a2 = |f|^2 and
+// the decrease of the data term for step g_j, formed per element in FP32
+// without cancellation and summed in FP64: with a2 = |f|^2 and
 //   delta = |f + g d|^2 - a2 = 2 g Re(conj(f) d) + g^2 |d|^2,
 // Poisson:  t(f) - t(f + g d) = -delta + D log1p(delta / a2),
 // Gaussian: t(f) - t(f + g d) = -delta / (|f| + |f + g d|) * (|f| + |f + g d| - 2 sqrt D);
-// moduli below the 1e-32 clamp take the direct formula.  Sums are FP64.
-// FP64 form, used for moduli below 1e-15 (where |f|^2 would underflow in FP32)
+// moduli below ~1e-15 (|f|^2 underflows in FP32) take the FP64 direct
+// formula with mlog's 1e-32 clamp.
 __device__ __forceinline__ double ls_decrease_f64(float2 f, float2 d, float g, float D, int model)
 {
     const double a2 = (double)f.x * f.x + (double)f.y * f.y;
@@ -151,6 +152,38 @@ __device__ __forceinline__ double ls_decrease_f64(float2 f, float2 d, float g, f
     return -delta / sum * (sum - 2.0 * (double)sqrtf(D));
 }
 
+// Adds the decrease for each step gj[j], j < J, of one pixel (model 0 =
+// Poisson, 1 = Gaussian) to acc[j].  1/|f|^2 is formed once per pixel.
+template <int JB>
+__device__ __forceinline__ void ls_pixel(double (&acc)[JB], const float (&gj)[JB], int J, float2 x, float2 y, float D,
+                                         int model)
+{
+    const float a2 = x.x * x.x + x.y * x.y;
+    const float fdot = x.x * y.x + x.y * y.y;
+    const float d2 = y.x * y.x + y.y * y.y;
+    const bool tiny = !(a2 >= 1e-30f);
+    const float ia2 = tiny ? 0.f : 1.f / a2;
+    const float fa = sqrtf(a2), sq = sqrtf(D);
+#pragma unroll
+    for (int j = 0; j < JB; ++j) {
+        if (j < J) {
+            const float g = gj[j];
+            const float delta = g * (2.f * fdot + g * d2);
+            const float b2 = a2 + delta;
+            double dec;
+            if (tiny || !(b2 >= 1e-30f)) {
+                dec = ls_decrease_f64(x, y, g, D, model);
+            } else if (model == 0) {
+                dec = (double)(D * log1pf(delta * ia2) - delta);
+            } else {
+                const float s2 = fa + sqrtf(b2);  // >= 1e-15: __fdividef is within 2 ulp here
+                dec = (double)(-__fdividef(delta, s2) * (s2 - 2.f * sq));
+            }
+            acc[j] += dec;
+        }
+    }
+}
+
 // JB = accumulator bucket (2, 8 or 16 step lengths); J <= JB are used
 template <int JB>
 __global__ void __launch_bounds__(RT) k_ls_frames(const float2 *__restrict__ f, const float2 *__restrict__ d,
@@ -163,48 +196,57 @@ __global__ void __launch_bounds__(RT) k_ls_frames(const float2 *__restrict__ f, 
     float gj[JB];
 #pragma unroll
     for (int j = 0; j < JB; ++j) gj[j] = j < J ? (float)gam[j] : 0.f;
-    for (size_t i = (size_t)blockIdx.x * RT + threadIdx.x; i < n; i += (size_t)gridDim.x * RT) {
-        const float2 x = f[i];
-        const float2 y = d[i];
-        const float dd = D[i] * dscale;
-        const float a2 = x.x * x.x + x.y * x.y;
-        const float fdot = x.x * y.x + x.y * y.y;
-        const float d2 = y.x * y.x + y.y * y.y;
-        const float sq = sqrtf(dd);
-        const float fa = sqrtf(a2);
-        const bool tiny = !(a2 >= 1e-30f);
+    // U pixels a stride apart per trip, loads first: 20 U bytes in flight per thread
+    constexpr int U = JB <= 8 ? 4 : 1;
+    const size_t stride = (size_t)gridDim.x * RT;
+    size_t i = (size_t)blockIdx.x * RT + threadIdx.x;
+    for (; i + (U - 1) * stride < n; i += U * stride) {
+        float2 x[U], y[U];
+        float dd[U];
 #pragma unroll
-        for (int j = 0; j < JB; ++j) {
-            if (j < J) {
-                const float g = gj[j];
-                const float delta = g * (2.f * fdot + g * d2);
-                const float b2 = a2 + delta;
-                double dec;
-                if (tiny || !(b2 >= 1e-30f)) {
-                    dec = ls_decrease_f64(x, y, g, dd, model);
-                } else if (model == 0) {
-                    dec = (double)(dd * log1pf(delta / a2) - delta);
-                } else {
-                    const float s2 = fa + sqrtf(b2);
-                    dec = (double)(-delta / s2 * (s2 - 2.f * sq));
-                }
-                acc[j] += dec;
-            }
+        for (int u = 0; u < U; ++u) {
+            x[u] = f[i + u * stride];
+            y[u] = d[i + u * stride];
+            dd[u] = D[i + u * stride];
         }
+#pragma unroll
+        for (int u = 0; u < U; ++u) ls_pixel<JB>(acc, gj, J, x[u], y[u], dd[u] * dscale, model);
     }
+    for (; i < n; i += stride) ls_pixel<JB>(acc, gj, J, f[i], d[i], D[i] * dscale, model);
     block_reduce_store<JB>(acc, work, blockIdx.x, gridDim.x);
 }
 
-int launch_ls_frames(const float2 *f, const float2 *d, const float *data, float dscale, size_t n, int model,
-                     const double *gammas, int J, double *work, cudaStream_t st)
+// One wave of k_ls_frames<JB> on the current device (at most RB blocks, the
+// partials' capacity); fixed for a given device, so sums stay deterministic.
+template <int JB>
+int ls_grid()
 {
+    int dev = 0, nsm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ls_frames<JB>, RT, 0) != cudaSuccess)
+        return -1;
+    const int g = nsm * per_sm;
+    return g < 1 ? 1 : (g > RB ? RB : g);
+}
+
+// Launches k_ls_frames; *nblk receives the number of partials per step length.
+int launch_ls_frames(const float2 *f, const float2 *d, const float *data, float dscale, size_t n, int model,
+                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk)
+{
+    const int grid = J <= 2 ? ls_grid<2>() : J <= 8 ? ls_grid<8>() : ls_grid<16>();
+    if (grid < 0) {
+        pt::set_error("ls_frames: occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return PT_ERR_CUDA;
+    }
     if (J <= 2)
-        k_ls_frames<2><<<RB, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
+        k_ls_frames<2><<<grid, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
     else if (J <= 8)
-        k_ls_frames<8><<<RB, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
+        k_ls_frames<8><<<grid, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
     else
-        k_ls_frames<16><<<RB, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
+        k_ls_frames<16><<<grid, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
     PT_LAUNCHED("k_ls_frames");
+    *nblk = grid;
     return PT_OK;
 }
 
@@ -311,18 +353,7 @@ __global__ void k_residual(float2 *__restrict__ out, const float2 *__restrict__ 
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float2 x = f[i];
         const float dd = D[i] * dscale;
-        float2 r;
-        if (model == 0) {
-            const float q = dd / (x.x * x.x + x.y * x.y + 1e-32f);
-            r = make_float2(x.x - q * x.x, x.y - q * x.y);
-        } else {
-            const float ang = atan2f(x.y, x.x);
-            float sn, cs;
-            sincosf(ang, &sn, &cs);
-            const float sq = sqrtf(dd);
-            r = make_float2(x.x - sq * cs, x.y - sq * sn);
-        }
-        out[i] = r;
+        out[i] = model == 0 ? pt_residual_poisson(x, dd) : pt_residual_gaussian(x, dd);
     }
 }
 
@@ -426,10 +457,11 @@ extern "C" int pt_ls_frames(const void *f, const void *d, const float *data, flo
     PT_CHECK_ARG(J >= 1 && J <= MAXK, "ls_frames: 1 <= J <= %d", MAXK);
     PT_CHECK_ARG(model == 0 || model == 1, "ls_frames: model 0 (poisson) or 1 (gaussian)");
     cudaStream_t st = (cudaStream_t)stream;
+    int nblk = 0;
     const int rc = launch_ls_frames((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J,
-                                    (double *)work, st);
+                                    (double *)work, st, &nblk);
     if (rc != PT_OK) return rc;
-    k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, J, RB, 0);
+    k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, J, nblk, 0);
     PT_LAUNCHED("k_finish");
     return PT_OK;
 }
@@ -600,11 +632,13 @@ extern "C" int pt_ls_frames_noalloc(const void *f, const void *d, const float *d
     const int rc = ls_scratch_for_current_device(&work);
     if (rc != PT_OK) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    // every partial that k_finish reads (J x RB) is written by k_ls_frames in
+    // every partial that k_finish reads (J x nblk) is written by k_ls_frames in
     // this call, so nothing in the shared scratch needs clearing first
-    const int rc2 = launch_ls_frames((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J, work, st);
+    int nblk = 0;
+    const int rc2 =
+        launch_ls_frames((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J, work, st, &nblk);
     if (rc2 != PT_OK) return rc2;
-    k_finish<<<1, RT, 0, st>>>(work, (double *)out, J, RB, 0);
+    k_finish<<<1, RT, 0, st>>>(work, (double *)out, J, nblk, 0);
     PT_LAUNCHED("k_finish");
     return PT_OK;
 }

@@ -185,3 +185,38 @@ def test_admm_reconstruction_quality_tracks_oracle(problem):
     eg = np.linalg.norm(ug - obj) / np.linalg.norm(obj)
     eo = np.linalg.norm(uo - obj) / np.linalg.norm(obj)
     assert abs(eg - eo) < 5e-2 * eo, (eg, eo)
+
+
+@pytest.mark.parametrize("model", ["poisson", "gaussian"])
+def test_cg_ptycho_det128(model):
+    """The CG on 128 detectors (the det-128 operator kernels) tracks the oracle.
+
+    The start is the object at 0.8 times its contrast.  From psi = 1 the Poisson
+    step lengths are not determined by FP32 arithmetic: detector pixels where
+    |FQ psi| ~ 1e-9 of the frame's peak carry counts, the likelihood is steep
+    there, and noise of 3e-8 of the frame RMS in the oracle's own forward moves
+    its first step between 2^-11 and 2^-10."""
+    from ptychotomo_b200 import Solver
+    n = nz = 128
+    ntheta, nprb = 4, 96
+    theta = synthetic.angles(ntheta)
+    prb = synthetic.probe(nprb, seed=4)
+    scan = synthetic.raster_scan(ntheta, 3, n, nz, nprb)
+    scan[1] += np.float32(0.2)
+    obj = synthetic.phantom(n, nz, seed=5)
+    args = (prb, scan, theta, [128, 128], 1e-6, 5.0, ntheta, nz, n, ntheta // 2, nz // 2)
+    gs = Solver(*args)
+    x = torch.empty((ntheta, gs.cl_tomo.N), dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    gs._tomo_all.get_xy(x, y)
+    os_ = OSolver(*args, xy=(x.cpu().numpy(), y.cpu().numpy()))
+    data = os_.fwd_ptycho_batch(os_.exptomo(os_.fwd_tomo_batch(obj)))
+    data = np.random.default_rng(6).poisson(data * 1e3).astype(np.float32) / np.float32(1e3)
+    psi0 = os_.exptomo(os_.fwd_tomo_batch((0.8 * obj).astype(np.complex64)))
+    h, lamd = np.ones_like(psi0), np.zeros_like(psi0)
+    gs.trace, os_.trace = [], []
+    pg = gs.cg_ptycho_batch(T(data), T(psi0), T(h), T(lamd), 0.5, 4, model)
+    po = os_.cg_ptycho_batch(data, psi0, h, lamd, 0.5, 4, model)
+    assert [g for _, g in gs.trace] == [g for _, g in os_.trace]
+    gs.trace = None
+    assert rel(pg, po) < 1e-4
