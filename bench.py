@@ -16,6 +16,8 @@ Pass-model algorithmic bytes per call (complex64 = 8 B):
                   (read the probe-sized patch, write the detector frame)
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --admm        # ADMM wall time (128^3 run, 256^3 iterations)
+    python bench.py --cg-kernels  # the ptycho CG's frame kernels at the operator workload
 
 ``--impl reference`` times the reference's operators: by default the CPU
 restatement of the reference (oracle/, all host cores, a bounded sample of
@@ -203,21 +205,37 @@ class Ops:
         self.h_frames.copy_(self.frames.cpu())
         self.h_out = {k: pin(getattr(self, k)) for k in ("proj_out", "u_out", "frames", "psi_out")}
         self.d_frames_in = torch.empty_like(self.frames)
+        # uploads, kernels and downloads on three streams: the 8.5 GB frame
+        # download of ptychofft.fwd and the 8.5 GB frame upload of ptychofft.adj
+        # use the two PCIe directions at the same time
+        self.s_h2d = torch.cuda.Stream(self.dev)
+        self.s_d2h = torch.cuda.Stream(self.dev)
 
     def e2e_step(self):
+        torch = self.torch
         r, p = self.radon, self.ptycho
-        self.u.copy_(self.h_in["u"], non_blocking=True)
-        r.fwd(self.proj_out, self.u)
-        self.h_out["proj_out"].copy_(self.proj_out, non_blocking=True)
-        self.proj.copy_(self.h_in["proj"], non_blocking=True)
-        r.adj(self.u_out, self.proj)
-        self.h_out["u_out"].copy_(self.u_out, non_blocking=True)
-        self.psi.copy_(self.h_in["psi"], non_blocking=True)
-        p.fwd(self.frames, self.psi)
-        self.h_out["frames"].copy_(self.frames, non_blocking=True)
-        self.d_frames_in.copy_(self.h_frames, non_blocking=True)
-        p.adj(self.psi_out, self.d_frames_in)
-        self.h_out["psi_out"].copy_(self.psi_out, non_blocking=True)
+        cs, hs, ds = torch.cuda.current_stream(self.dev), self.s_h2d, self.s_d2h
+        cs.wait_stream(ds)   # the previous step's downloads finished before outputs are rewritten
+        hs.wait_stream(cs)   # ... and its kernels before inputs are overwritten
+        up = {}
+        with torch.cuda.stream(hs):
+            for k, dst, src in (("u", self.u, self.h_in["u"]), ("proj", self.proj, self.h_in["proj"]),
+                                ("psi", self.psi, self.h_in["psi"]), ("frames", self.d_frames_in, self.h_frames)):
+                dst.copy_(src, non_blocking=True)
+                up[k] = torch.cuda.Event()
+                up[k].record(hs)
+        for k, call, out in (("u", lambda: r.fwd(self.proj_out, self.u), "proj_out"),
+                             ("proj", lambda: r.adj(self.u_out, self.proj), "u_out"),
+                             ("psi", lambda: p.fwd(self.frames, self.psi), "frames"),
+                             ("frames", lambda: p.adj(self.psi_out, self.d_frames_in), "psi_out")):
+            cs.wait_event(up[k])
+            call()
+            done = torch.cuda.Event()
+            done.record(cs)
+            ds.wait_event(done)
+            with torch.cuda.stream(ds):
+                self.h_out[out].copy_(getattr(self, out), non_blocking=True)
+        cs.wait_stream(ds)   # the step ends when its results are on the host
 
     def e2e_bytes(self):
         bi = sum(v.numel() * v.element_size() for v in self.h_in.values()) + self.h_frames.numel() * 8
@@ -461,6 +479,176 @@ def run_reference_cuda(args, local):
             "e2e": {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# ---- ADMM wall time ----------------------------------------------------------
+# Small plain-ADMM problem: 128^3, 128 angles on [0, pi), 64^2 probe (sigma 12)
+# and detector, 7x7 raster with step 10 px, 5 keV, voxel 1e-6 cm, Poisson
+# counts at 1e3 mean photons per pixel, 4 ADMM iterations x 4 CG iterations
+# (the first two ADMM iterations run 4 + 32 ptycho CG iterations), TV 1e-3.
+ADMM_SMALL = dict(n=128, nz=128, ntheta=128, nprb=64, det=64, nside=7, step=10.0, photons=1e3, niter=4,
+                  piter=4, titer=4, alpha=1e-3, voxel=1e-6, energy=5.0)
+
+
+def _admm_problem(c, torch, dev, seed=0):
+    """Solver, device counts and the true object for an ADMM config."""
+    from ptychotomo_b200 import Solver, synthetic
+    n, nz, nt = c["n"], c["nz"], c["ntheta"]
+    theta = synthetic.angles(nt)
+    prb = synthetic.probe(c["nprb"], seed=seed + 1)
+    scan = synthetic.raster_scan(nt, c["nside"], n, nz, c["nprb"], step=c.get("step"))
+    obj = synthetic.phantom(n, nz, seed=seed + 2)
+    slv = Solver(prb, scan, theta, [c["det"], c["det"]], c["voxel"], c["energy"], nt, nz, n, nt, nz, device=dev)
+    u = torch.from_numpy(obj).to(dev)
+    inten = slv.fwd_ptycho_batch(slv.exptomo(slv.fwd_tomo_batch(u)))
+    scale = c["photons"] / float(inten.mean())
+    g = torch.Generator(device=dev).manual_seed(seed + 3)
+    data = torch.poisson(inten * scale, generator=g) / scale
+    return slv, data, u
+
+
+def _admm_run(slv, data, c, torch, dev, niter, history=None):
+    cplx = dict(dtype=torch.complex64, device=dev)
+    nt, nz, n = c["ntheta"], c["nz"], c["n"]
+    psi = torch.ones((nt, nz, n), **cplx)
+    z3 = lambda: torch.zeros((3, nz, n, n), **cplx)  # noqa: E731
+    return slv.admm(data, psi.clone(), z3(), psi, z3(), torch.zeros_like(psi), z3(), torch.zeros((nz, n, n), **cplx),
+                    c["alpha"], c["piter"], c["titer"], niter, "poisson", verbose=False, history=history)
+
+
+def _admm_cpu_estimate(c, data, psi_t):
+    """NumPy oracle on a bounded sample of the small ADMM, extrapolated to the full run.
+
+    Sample: 2 ptycho CG iterations at full size, one radonusfft fwd + adj on 2 of
+    the slices (per-slice cost x nz), and the elementwise ADMM steps once.  Full
+    run = sum over ADMM iterations of (piter_m / 2) x CG-ptycho(2) + titer x
+    (2 fwd + 1 adj) tomography passes + 1 fwd for h + the elementwise steps.
+    """
+    from oracle.solver import Solver as OSolver
+    from oracle.usfft import RadonUSFFT
+    from ptychotomo_b200 import synthetic
+    n, nz, nt = c["n"], c["nz"], c["ntheta"]
+    theta = synthetic.angles(nt)
+    prb = synthetic.probe(c["nprb"], seed=1)
+    scan = synthetic.raster_scan(nt, c["nside"], n, nz, c["nprb"], step=c.get("step"))
+    obj = synthetic.phantom(n, nz, seed=2)
+    osl = OSolver(prb, scan, theta, [c["det"], c["det"]], c["voxel"], c["energy"], nt, nz, n, nt, nz)
+    psi = np.ones((nt, nz, n), np.complex64)
+    t0 = time.perf_counter()
+    osl.cg_ptycho_batch(data, psi, psi.copy(), np.zeros_like(psi), 0.5, 2, "poisson")
+    t_cgp2 = time.perf_counter() - t0
+    r = RadonUSFFT(nt, 2, n)
+    r.setobj(theta)
+    f2 = obj[:2].astype(np.complex64)
+    t0 = time.perf_counter()
+    g2 = r.fwd(f2)
+    t_fwd = (time.perf_counter() - t0) / 2 * nz
+    t0 = time.perf_counter()
+    r.adj(g2)
+    t_adj = (time.perf_counter() - t0) / 2 * nz
+    z3 = np.zeros((3, nz, n, n), np.complex64)
+    t0 = time.perf_counter()
+    xi0, xi1, K, ps = osl.takexi(psi_t, z3, np.zeros_like(psi_t), z3, 0.5, 0.5)
+    osl.solve_reg(np.zeros((nz, n, n), np.complex64), z3, 0.5, c["alpha"])
+    osl.fwd_reg(np.zeros((nz, n, n), np.complex64))
+    osl.update_penalty(psi_t, psi_t, psi_t, z3, z3, z3, 0.5, 0.5)
+    t_rest = time.perf_counter() - t0
+    total = 0.0
+    for m in range(c["niter"]):
+        piter = c["piter"] + (m < 2) * 32
+        total += piter / 2 * t_cgp2 + c["titer"] * (2 * t_fwd + t_adj) + t_fwd + t_rest
+    sample = ("NumPy oracle, 1 process: 2 CG-ptycho iterations at full size (%.1f s), radonusfft fwd/adj on "
+              "2 of %d slices (%.2f / %.2f s per full call), elementwise ADMM steps (%.1f s); extrapolated to "
+              "%d ADMM iterations" % (t_cgp2, nz, t_fwd, t_adj, t_rest, c["niter"]))
+    return total, sample
+
+
+def run_admm(args, local):
+    """ADMM wall time on one GPU: the small plain-ADMM problem end to end, and the
+    steady-state ADMM iteration (piter = titer = 4) at 256^3 with 384 angles."""
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    c = dict(ADMM_SMALL)
+    slv, data, u_true = _admm_problem(c, torch, dev)
+    cpu_inputs = None
+    if not args.no_cpu_baseline:   # the same counts and true psi for the oracle sample
+        cpu_inputs = (data.cpu().numpy(), slv.exptomo(slv.fwd_tomo_batch(u_true)).cpu().numpy())
+    _admm_run(slv, data, c, torch, dev, 1)   # warm-up (allocator, tables)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    u, _ = _admm_run(slv, data, c, torch, dev, c["niter"])
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    err = float(torch.linalg.vector_norm(u - u_true) / torch.linalg.vector_norm(u_true))
+    del slv, data, u_true, u
+
+    class Stamps(list):
+        def append(self, x):
+            torch.cuda.synchronize()
+            x["t"] = time.perf_counter()
+            super().append(x)
+
+    big = dict(ADMM_SMALL, n=256, nz=256, ntheta=384, nprb=128, det=128, nside=13, step=None)
+    slv, data, _ = _admm_problem(big, torch, dev)
+    hist = Stamps()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _admm_run(slv, data, big, torch, dev, 4, history=hist)
+    it_ms = [1e3 * (b["t"] - a) for a, b in zip([t0] + [h["t"] for h in hist[:-1]], hist)]
+    line = {"metric": "plain Poisson ADMM wall time, 128^3 (4 ADMM x 4 CG iterations)", "value": round(wall, 3),
+            "unit": "s", "n_gpus": 1, "higher_is_better": False, "dtype": "c64 (fp32 complex), FP64 reductions",
+            "data": "synthetic", "config": {"workload": "plain ADMM: " + json.dumps(c)},
+            "recon_rel_err_vs_phantom": round(err, 4),
+            "iteration_ms_256cubed": {"workload": "384 angles, 13x13 scans, 128^2 probe/detector; iterations 0-1 "
+                                                  "run 36 ptycho CG iterations, 2-3 run 4",
+                                      "ms": [round(x, 1) for x in it_ms]}}
+    if not args.no_cpu_baseline:
+        est, sample = _admm_cpu_estimate(c, *cpu_inputs)
+        line["cpu_baseline"] = {"value": round(est, 1), "unit": "s", "cores": 1, "kind": "port", "sample": sample}
+    return line
+
+
+def run_cg_kernels(args, local):
+    """Device time of the ptycho CG's frame-sized kernels at the operator workload:
+    the gradient adjoint with the residual formed on load (Poisson, Gaussian) and
+    the line-search reduction for 2, 8 and 16 step lengths."""
+    import torch
+    from ptychotomo_b200 import kernels as K
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    c = dict(CFG)
+    ops = Ops(c, torch, dev)
+    p = ops.ptycho
+    g = torch.Generator(device=dev).manual_seed(5)
+    p.fwd(ops.frames, ops.psi)
+    data = (ops.frames.abs() ** 2 * (1 + 0.1 * torch.rand(ops.frames.shape, device=dev, generator=g))).float()
+    fd = 0.1 * ops.frames.roll(1, dims=-1)
+    red = K.Reducer(dev)
+    cases = {"adj_resid_poisson": lambda: p.adj_resid(ops.psi_out, ops.frames, data, 1.0, 0),
+             "adj_resid_gaussian": lambda: p.adj_resid(ops.psi_out, ops.frames, data, 1.0, 1),
+             "ptycho_adj": lambda: p.adj(ops.psi_out, ops.frames),
+             "ls_frames_J2": lambda: red.ls_frames(ops.frames, fd, data, 1.0, 0, [1.0, 0.5]),
+             "ls_frames_J8": lambda: red.ls_frames(ops.frames, fd, data, 1.0, 0, [0.5 ** j for j in range(8)]),
+             "ls_frames_J16": lambda: red.ls_frames(ops.frames, fd, data, 1.0, 0, [0.5 ** j for j in range(16)])}
+    out = {}
+    for name, fn in cases.items():
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = round(e0.elapsed_time(e1) / args.steps, 3)
+    S = c["ntheta"] * c["nside"] ** 2
+    frame = 8 * S * c["det"] ** 2
+    return {"metric": "ptycho CG frame kernels, ms per call", "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "data": "synthetic",
+            "config": config_dict(c), "ms": out,
+            "bytes_per_call": {"adj_resid": frame + frame // 2, "ls_frames": 2 * frame + frame // 2}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -472,6 +660,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--ntheta", type=int, default=None, help="override the angle count (small profiling cases)")
     ap.add_argument("--nz", type=int, default=None, help="override the slice count (small profiling cases)")
+    ap.add_argument("--admm", action="store_true", help="ADMM wall time instead of operator throughput")
+    ap.add_argument("--cg-kernels", action="store_true", help="device time of the ptycho CG's frame kernels")
     args = ap.parse_args()
     if args.ntheta:
         CFG["ntheta"] = args.ntheta
@@ -480,6 +670,11 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.admm or args.cg_kernels:
+        if rank == 0:
+            line = run_admm(args, local) if args.admm else run_cg_kernels(args, local)
+            print(json.dumps(line), flush=True)
+        return 0
     if args.impl == "reference":
         if rank != 0:
             return 0
