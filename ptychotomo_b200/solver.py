@@ -51,49 +51,70 @@ def _dev_tensor(x, dtype, device):
 
 
 class Solver:
-    def __init__(self, prb, scan, theta, det, voxelsize, energy, ntheta, nz, n, ptheta, pnz, device=None):
+    def __init__(self, prb, scan, theta, det, voxelsize, energy, ntheta, nz, n, ptheta, pnz, device=None,
+                 _held=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         dev = self.device
         self.voxelsize = voxelsize
         self.energy = energy
-        self.scan = _dev_tensor(scan, torch.float32, dev)
         self.prb = _dev_tensor(prb, torch.complex64, dev)
         self.theta = _dev_tensor(theta, torch.float32, dev)
         self.ntheta, self.nz, self.n = ntheta, nz, n
+        # the angles [th0, th1) and slices [z0, z1) this process holds: all of
+        # them here, one shard of each under ShardedSolver (angle-major arrays
+        # psi, h, lamd, data hold the angles; slice-major u, e, phi, mu the slices)
+        th0, th1, z0, z1 = _held if _held is not None else (0, ntheta, 0, nz)
+        self.theta_range, self.z_range = (th0, th1), (z0, z1)
+        self.ntheta_held, self.nz_held = th1 - th0, z1 - z0
+        self.scan = _dev_tensor(scan, torch.float32, dev)[:, th0:th1].contiguous()
         self.nscan = self.scan.shape[2]
         self.ndety, self.ndetx = det[0], det[1]
         self.nprb = self.prb.shape[0]
         self.ptheta, self.pnz = ptheta, pnz
-        if ntheta % ptheta or nz % pnz:
+        if self.ntheta_held % ptheta or self.nz_held % pnz:
             raise ValueError("ptheta must divide ntheta and pnz must divide nz (solver.py:86,111)")
         # tomography: the pnz-chunk operator of fwd_tomo/adj_tomo and one for whole batches
         self.cl_tomo = radonusfft(ntheta, pnz, n)
         self.cl_tomo.setobj(self.theta)
-        if pnz == nz:
+        if pnz == self.nz_held:
             self._tomo_all = self.cl_tomo
         else:
-            self._tomo_all = radonusfft(ntheta, nz, n)
+            self._tomo_all = radonusfft(ntheta, self.nz_held, n)
             self._tomo_all.setobj(self.theta)
         # ptychography: one operator per angle chunk, its scans set once
         self._ptycho = []
-        for k in range(ntheta // ptheta):
+        for k in range(self.ntheta_held // ptheta):
             op = ptychofft(ptheta, nz, n, ptheta, self.nscan, self.ndety, self.ndetx, self.nprb)
             op.setobj(self.scan[:, k * ptheta:(k + 1) * ptheta].contiguous(), self.prb)
             self._ptycho.append(op)
         self.cl_ptycho = self._ptycho[0]
-        if ptheta != ntheta:
-            self._ptycho_all = ptychofft(ntheta, nz, n, ntheta, self.nscan, self.ndety, self.ndetx, self.nprb)
+        if ptheta != self.ntheta_held:
+            self._ptycho_all = ptychofft(self.ntheta_held, nz, n, self.ntheta_held, self.nscan, self.ndety,
+                                         self.ndetx, self.nprb)
             self._ptycho_all.setobj(self.scan, self.prb)
         else:
             self._ptycho_all = self.cl_ptycho
         # normalization coefficients, solver.py:43-46 (float32 like the reference)
-        self.red = K.Reducer(dev)
+        self.red = self._reducer(K.Reducer(dev))
         amax = self.red.maxabs(self.prb)
         self.coeftomo = float(np.float32(1 / np.float32(np.sqrt(ntheta * n / 2))))
         self.coefptycho = float(np.float32(1 / np.float32(amax)))
         self.coefdata = float(np.float32(1 / (self.ndetx * self.ndety * np.float32(amax) ** 2)))
 
     # ---- helpers ----------------------------------------------------------
+    # Hooks for ShardedSolver: global reductions, angle <-> slice re-sharding.
+    # One process holds everything, so they are identities here.
+    def _reducer(self, red):
+        return red
+
+    def _theta_to_z(self, x):
+        """[angles held, nz, n] -> [ntheta, slices held, n]."""
+        return x
+
+    def _z_to_theta(self, x):
+        """[ntheta, slices held, n] -> [angles held, nz, n]."""
+        return x
+
     def _empty(self, shape, dtype=torch.complex64):
         return torch.empty(shape, dtype=dtype, device=self.device)
 
@@ -126,12 +147,12 @@ class Solver:
         return res
 
     def fwd_tomo_batch(self, u):
-        res = self._empty([self.ntheta, self.nz, self.n])
+        res = self._empty([self.ntheta, self.nz_held, self.n])
         self._tomo_all.fwd(res, u, scale=self.coeftomo)
         return res
 
     def adj_tomo_batch(self, data):
-        res = self._empty([self.nz, self.n, self.n])
+        res = self._empty([self.nz_held, self.n, self.n])
         self._tomo_all.adj(res, data, scale=self.coeftomo)
         return res
 
@@ -144,7 +165,7 @@ class Solver:
 
     def fwd_ptycho_batch(self, psi):
         """|FQ psi|^2 / coefdata for all angles (a device float32 tensor)."""
-        frames = self._empty([self.ntheta, self.nscan, self.ndety, self.ndetx])
+        frames = self._empty([self.ntheta_held, self.nscan, self.ndety, self.ndetx])
         self._ptycho_all.fwd(frames, psi, scale=self.coefptycho)
         data = self._empty(frames.shape, torch.float32)
         return K.abs2(data, frames, 1.0 / self.coefdata)
@@ -165,7 +186,7 @@ class Solver:
     def takexi(self, psi, phi, lamd, mu, rho, tau):
         r = self.prb.shape[0] // 2
         ncols = psi.shape[2]
-        cnt = psi.numel() // ncols * r
+        cnt = self.ntheta * self.nz * r   # elements in each column band over all angles
         m1 = self.red.angle_band_sum(psi, r, 2 * r) / cnt
         m2 = self.red.angle_band_sum(psi, ncols - 2 * r, ncols - r) / cnt
         pshift = (m1 + m2) / 2
@@ -285,11 +306,11 @@ class Solver:
 
     def cg_ptycho_batch(self, data, init, h, lamd, rho, piter, model):
         data = self._as_data(data)
-        if self.ptheta == self.ntheta:
+        if self.ptheta == self.ntheta_held:
             self.cl_ptycho = self._ptycho[0]
             return self.cg_ptycho(data, init, h, lamd, rho, piter, model, dscale=self.coefdata)
         psi = init.clone()
-        for k in range(self.ntheta // self.ptheta):
+        for k in range(self.ntheta_held // self.ptheta):
             ids = self._ids(k)
             self.cl_ptycho = self._ptycho[k]
             psi[ids] = self.cg_ptycho(data[ids], psi[ids].contiguous(), h[ids].contiguous(),
@@ -325,7 +346,7 @@ class Solver:
         data = self._as_data(data)
         red = self.red
         lagr = np.zeros(7)
-        for k in range(self.ntheta // self.ptheta):
+        for k in range(self.ntheta_held // self.ptheta):
             ids = self._ids(k)
             self.cl_ptycho = self._ptycho[k]
             fpsi = self.fwd_ptycho(psi[ids].contiguous())
@@ -347,9 +368,9 @@ class Solver:
             h0, e0 = h, e
             psi = self.cg_ptycho_batch(data, psi, h, lamd, rho, piter + (m < 2) * 32, model)
             xi0, xi1, Kt, pshift = self.takexi(psi, phi, lamd, mu, rho, tau)
-            u = self.cg_tomo(xi0, xi1, Kt, u, rho, tau, titer)
+            u = self.cg_tomo(self._theta_to_z(xi0), xi1, self._theta_to_z(Kt), u, rho, tau, titer)
             phi = self.solve_reg(u, mu, tau, alpha)
-            h = K.expmap(torch.empty_like(psi), self.fwd_tomo_batch(u),
+            h = K.expmap(torch.empty_like(psi), self._z_to_theta(self.fwd_tomo_batch(u)),
                          self.voxelsize * self.wavenumber() / self.coeftomo, pshift)
             e = self.fwd_reg(u)
             lamd = K.lincomb(torch.empty_like(lamd), [(1.0, lamd), (rho, h), (-rho, psi)])
