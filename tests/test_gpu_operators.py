@@ -265,3 +265,75 @@ def test_ptycho_adjoint_with_fused_residual(ntheta, nz, n, nscan, det, nprb, mod
     out = torch.zeros_like(ref)
     op.adj_resid(out, fpsi, data, 0.7, model, scale=0.5)
     assert rel(out.cpu().numpy(), ref.cpu().numpy()) <= 1e-6
+
+
+def test_operators_capture_in_a_cuda_graph():
+    """fwd/adj allocate nothing and never synchronise, so one CUDA graph holds a
+    whole operator step; replays equal eager calls bit for bit."""
+    rng = np.random.default_rng(21)
+    n, nz, nt = 64, 16, 24
+    theta = np.sort(rng.uniform(0, np.pi, nt)).astype(np.float32)
+    rop, _ = make_radon(n, nz, nt, theta)
+    pop, _, _, _ = make_ptycho(3, 140, 140, 5, 128, 128, rng)
+    f = dev(crand(rng, (nz, n, n)))
+    g = dev(crand(rng, (nt, nz, n)))
+    psi = dev(crand(rng, (3, 140, 140)))
+    frames_in = dev(crand(rng, (3, 5, 128, 128)))
+    data = dev(rng.poisson(2.0, (3, 5, 128, 128)).astype(np.float32))
+    outs = [torch.zeros((nt, nz, n), dtype=torch.complex64, device="cuda"),
+            torch.zeros((nz, n, n), dtype=torch.complex64, device="cuda"),
+            torch.zeros((3, 5, 128, 128), dtype=torch.complex64, device="cuda"),
+            torch.zeros((3, 140, 140), dtype=torch.complex64, device="cuda"),
+            torch.zeros((3, 140, 140), dtype=torch.complex64, device="cuda")]
+
+    def step():
+        rop.fwd(outs[0], f)
+        rop.adj(outs[1], g)
+        pop.fwd(outs[2], psi, scale=0.5)
+        pop.adj(outs[3], frames_in)
+        pop.adj_resid(outs[4], frames_in, data, 0.3, 0)
+
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        step()
+    torch.cuda.current_stream().wait_stream(s)
+    eager = [o.clone() for o in outs]
+    for o in outs:
+        o.zero_()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        step()
+    for _ in range(2):
+        for o in outs:
+            o.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        for o, e in zip(outs, eager):
+            assert torch.equal(o, e)
+
+
+@pytest.mark.parametrize("det,nprb", [(32, 32), (128, 96)])
+def test_ptycho_uneven_scan_counts(det, nprb):
+    """Per-angle scan counts drawn from [lo, hi] on a jittered spiral, padded to the
+    largest count with the -1 sentinel (kernels.cuh:256,280): every padded scan is
+    skipped by both transforms."""
+    from ptychotomo_b200 import ptychofft, synthetic
+    rng = np.random.default_rng(det)
+    nt, n, nz = 4, 160, 150
+    counts = rng.integers(5, 19, nt)
+    scan = synthetic.jittered_spiral_scan(nt, n, nz, nprb, counts, jitter=3.0, seed=det)
+    nscan = scan.shape[2]
+    assert (scan < 0).any()
+    prb = crand(rng, (nprb, nprb))
+    op = ptychofft(nt, nz, n, nt, nscan, det, det, nprb)
+    op.setobj(dev(scan), dev(prb))
+    orc = PtychoFFT(nt, nz, n, nt, nscan, det, det, nprb)
+    orc.setobj(scan, prb)
+    f = crand(rng, (nt, nz, n))
+    g = crand(rng, (nt, nscan, det, det))
+    got = p_fwd(op, dev(f)).cpu().numpy()
+    assert rel(got, orc.fwd(f)) <= TOL
+    for t in range(nt):   # padded scans leave their frames untouched (zero here)
+        assert not np.any(got[t, counts[t]:])
+    assert rel(p_adj(op, dev(g)).cpu().numpy(), orc.adj(g)) <= TOL
