@@ -24,13 +24,24 @@ __host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b)
 __host__ __device__ __forceinline__ float2 czero() { return make_float2(0.f, 0.f); }
 
 // ---- data-term residual of the ptycho gradient (solver.py:220-224) ----------
-// D = measured intensity (already scaled).  Poisson: x - D x / (|x|^2 + 1e-32).
-// Gaussian: x - sqrt(D) exp(i angle(x)), formed as x (1 - sqrt(D) / |x|); for
-// |x|^2 < 1e-30 (and x = 0, where angle is 0) through atan2 as written.
+// D = measured intensity (already scaled).  Poisson: x - D x / (|x|^2 + 1e-32),
+// the quotient as D times the correctly rounded reciprocal of the divisor (a
+// normal number >= 1e-32), so zero counts, which are common, take the same
+// path as the rest.  Gaussian: x - sqrt(D) exp(i angle(x)), formed as
+// x (1 - sqrt(D) / |x|) with rsqrtf for 1/|x| (within 2 ulp; the reference's
+// angle/exp pair is itself a few ulp from exact); for |x|^2 < 1e-30 (and
+// x = 0, where angle is 0) through atan2 as written.
 __device__ __forceinline__ float2 pt_residual_poisson(float2 x, float D)
 {
-    const float q = D / (x.x * x.x + x.y * x.y + 1e-32f);
+    const float q = D * __frcp_rn(x.x * x.x + x.y * x.y + 1e-32f);
     return make_float2(x.x - q * x.x, x.y - q * x.y);
+}
+// the rare |x|^2 < 1e-30 case, kept out of line so that unrolled callers stay small
+static __device__ __noinline__ float2 pt_residual_gaussian_tiny(float2 x, float sq)
+{
+    float sn, cs;
+    sincosf(atan2f(x.y, x.x), &sn, &cs);
+    return make_float2(x.x - sq * cs, x.y - sq * sn);
 }
 __device__ __forceinline__ float2 pt_residual_gaussian(float2 x, float D)
 {
@@ -40,9 +51,7 @@ __device__ __forceinline__ float2 pt_residual_gaussian(float2 x, float D)
         const float r = sq * rsqrtf(a2);
         return make_float2(x.x - r * x.x, x.y - r * x.y);
     }
-    float sn, cs;
-    sincosf(atan2f(x.y, x.x), &sn, &cs);
-    return make_float2(x.x - sq * cs, x.y - sq * sn);
+    return pt_residual_gaussian_tiny(x, sq);
 }
 
 namespace pt {

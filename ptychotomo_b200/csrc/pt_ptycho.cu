@@ -33,8 +33,6 @@ constexpr double PI_REF = 3.1415926535;  // kernels.cuh:1
 // Residual of the ptycho data term applied to a frame value x on load
 // (solver.py:220-224, D = dscale * data): RESID 0 = none (plain adjoint),
 // 1 = Poisson x - D x / (|x|^2 + 1e-32), 2 = Gaussian x - sqrt(D) exp(i angle x).
-// RESID 0: the frame itself; 1: Poisson residual; 2: Gaussian residual, with
-// D = dscale * data (the gradient's input, solver.py:220-224)
 template <int RESID>
 __device__ __forceinline__ float2 resid_of(float2 x, float D)
 {
@@ -368,7 +366,10 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
 // group hit 8 distinct 4-bank groups both when writing (q varies) and when
 // reading (c varies).  The group exchange uses the same trick.
 constexpr int P128_SMEM = (64 * 128) * 16 + 128 * 8;
-// the fused-residual adjoint also stages the frame's 128 x 128 counts
+// the fused-residual adjoint also stages the frame's 128 x 128 counts.  The
+// plain adjoint stays at P128_SMEM: the remaining ~125 KB of L1 keeps the
+// 128 KB probe table it rereads for every frame mostly resident (with 64 KB
+// more shared memory it ran at twice the time).
 constexpr int P128_SMEM_RESID = P128_SMEM + 128 * 128 * 4;
 
 template <int DIR>

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
 // 1/N- and fftshift1c-scaled samples to lines[(theta N + k) ZC + z].
 constexpr int GPB = 32;
 template <int N, int M>
-__global__ void __launch_bounds__(GPB *ZC)
+__global__ void __launch_bounds__(GPB *ZC, 4)
     k_fwd_gather_pts(const float2 *__restrict__ fg, float2 *__restrict__ lines, const float *__restrict__ xt,
                      const float *__restrict__ yt, float a, float pre)
 {
@@ -184,14 +184,14 @@ __global__ void __launch_bounds__(GPB *ZC)
         for (int h = 0; h < 2; ++h) {
             const int i0 = 2 * j + h - odd;
             const float w0 = (float)(fx - M + i0) / (float)G - x0;
-            w2[h] = (i0 >= 0 && i0 < W) ? expf(-a * (w0 * w0)) : 0.f;
+            w2[h] = (i0 >= 0 && i0 < W) ? __expf(-a * (w0 * w0)) : 0.f;
         }
         wxp[j] = make_float2(w2[0], w2[1]);
     }
 #pragma unroll
     for (int i = 0; i < W; ++i) {
         const float w1 = (float)(fy - M + i) / (float)G - y0;
-        wy[i] = expf(-a * (w1 * w1));
+        wy[i] = __expf(-a * (w1 * w1));
     }
     const int p0 = (c0 - odd) / 2;  // first column pair
     const float4 *g4 = reinterpret_cast<const float4 *>(fg) + lane;
@@ -372,7 +372,7 @@ __global__ void k_make_entries(const unsigned *__restrict__ keys, int *__restric
     const unsigned key = keys[e];
     const int p = (int)(key >> 9), i0 = (int)((key >> 5) & 15), r0 = (int)(key & 31) - 3;
     const float w0 = (float)(fxy[2 * p] - M + i0) / (float)G - xt[p];
-    const float wx = expf(-a * (w0 * w0));
+    const float wx = __expf(-a * (w0 * w0));
     float w[CG];
 #pragma unroll
     for (int c = 0; c < CG; ++c) {
@@ -380,7 +380,7 @@ __global__ void k_make_entries(const unsigned *__restrict__ keys, int *__restric
         w[c] = 0.f;
         if (i1 >= 0 && i1 < W) {
             const float w1 = (float)(fxy[2 * p + 1] - M + i1) / (float)G - yt[p];
-            w[c] = wx * expf(-a * (w1 * w1));
+            w[c] = wx * __expf(-a * (w1 * w1));
         }
     }
     gpt[e] = p;

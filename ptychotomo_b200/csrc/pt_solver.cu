@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(RT) k_reduce(int op, const float2 *__restrict_
 // Poisson:  t(f) - t(f + g d) = -delta + D log1p(delta / a2),
 // Gaussian: t(f) - t(f + g d) = -delta / (|f| + |f + g d|) * (|f| + |f + g d| - 2 sqrt D);
 // moduli below ~1e-15 (|f|^2 underflows in FP32) take the FP64 direct
-// formula with mlog's 1e-32 clamp.
-__device__ __forceinline__ double ls_decrease_f64(float2 f, float2 d, float g, float D, int model)
+// formula with mlog's 1e-32 clamp (out of line: rare, and its callers are unrolled).
+__device__ __noinline__ double ls_decrease_f64(float2 f, float2 d, float g, float D, int model)
 {
     const double a2 = (double)f.x * f.x + (double)f.y * f.y;
     const double fd = (double)f.x * d.x + (double)f.y * d.y;
@@ -152,18 +152,23 @@ __device__ __forceinline__ double ls_decrease_f64(float2 f, float2 d, float g, f
     return -delta / sum * (sum - 2.0 * (double)sqrtf(D));
 }
 
-// Adds the decrease for each step gj[j], j < J, of one pixel (model 0 =
-// Poisson, 1 = Gaussian) to acc[j].  1/|f|^2 is formed once per pixel.
-template <int JB>
-__device__ __forceinline__ void ls_pixel(double (&acc)[JB], const float (&gj)[JB], int J, float2 x, float2 y, float D,
-                                         int model)
+// Adds the decrease for each step gj[j], j < J, of one pixel to acc[j];
+// MODEL 0 = Poisson, 1 = Gaussian.  1/|f|^2 (Poisson) or |f| and sqrt D
+// (Gaussian) are formed once per pixel.
+template <int JB, int MODEL>
+__device__ __forceinline__ void ls_pixel(double (&acc)[JB], const float (&gj)[JB], int J, float2 x, float2 y, float D)
 {
     const float a2 = x.x * x.x + x.y * x.y;
     const float fdot = x.x * y.x + x.y * y.y;
     const float d2 = y.x * y.x + y.y * y.y;
     const bool tiny = !(a2 >= 1e-30f);
-    const float ia2 = tiny ? 0.f : 1.f / a2;
-    const float fa = sqrtf(a2), sq = sqrtf(D);
+    float ia2 = 0.f, fa = 0.f, sq = 0.f;
+    if (MODEL == 0) {
+        ia2 = tiny ? 0.f : 1.f / a2;
+    } else {
+        fa = sqrtf(a2);
+        sq = sqrtf(D);
+    }
 #pragma unroll
     for (int j = 0; j < JB; ++j) {
         if (j < J) {
@@ -172,8 +177,8 @@ __device__ __forceinline__ void ls_pixel(double (&acc)[JB], const float (&gj)[JB
             const float b2 = a2 + delta;
             double dec;
             if (tiny || !(b2 >= 1e-30f)) {
-                dec = ls_decrease_f64(x, y, g, D, model);
-            } else if (model == 0) {
+                dec = ls_decrease_f64(x, y, g, D, MODEL);
+            } else if (MODEL == 0) {
                 dec = (double)(D * log1pf(delta * ia2) - delta);
             } else {
                 const float s2 = fa + sqrtf(b2);  // >= 1e-15: __fdividef is within 2 ulp here
@@ -185,9 +190,9 @@ __device__ __forceinline__ void ls_pixel(double (&acc)[JB], const float (&gj)[JB
 }
 
 // JB = accumulator bucket (2, 8 or 16 step lengths); J <= JB are used
-template <int JB>
+template <int JB, int MODEL>
 __global__ void __launch_bounds__(RT) k_ls_frames(const float2 *__restrict__ f, const float2 *__restrict__ d,
-                                                  const float *__restrict__ D, float dscale, size_t n, int model,
+                                                  const float *__restrict__ D, float dscale, size_t n,
                                                   const double *__restrict__ gam, int J, double *__restrict__ work)
 {
     double acc[JB];
@@ -210,44 +215,54 @@ __global__ void __launch_bounds__(RT) k_ls_frames(const float2 *__restrict__ f, 
             dd[u] = D[i + u * stride];
         }
 #pragma unroll
-        for (int u = 0; u < U; ++u) ls_pixel<JB>(acc, gj, J, x[u], y[u], dd[u] * dscale, model);
+        for (int u = 0; u < U; ++u) ls_pixel<JB, MODEL>(acc, gj, J, x[u], y[u], dd[u] * dscale);
     }
-    for (; i < n; i += stride) ls_pixel<JB>(acc, gj, J, f[i], d[i], D[i] * dscale, model);
+    for (; i < n; i += stride) ls_pixel<JB, MODEL>(acc, gj, J, f[i], d[i], D[i] * dscale);
     block_reduce_store<JB>(acc, work, blockIdx.x, gridDim.x);
 }
 
-// One wave of k_ls_frames<JB> on the current device (at most RB blocks, the
-// partials' capacity); fixed for a given device, so sums stay deterministic.
-template <int JB>
-int ls_grid()
+// One wave of a k_ls_frames instance on the current device (at most RB
+// blocks, the partials' capacity); fixed for a given device, so sums stay
+// deterministic.
+template <typename Kern>
+int one_wave(Kern kern)
 {
     int dev = 0, nsm = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ls_frames<JB>, RT, 0) != cudaSuccess)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RT, 0) != cudaSuccess)
         return -1;
     const int g = nsm * per_sm;
     return g < 1 ? 1 : (g > RB ? RB : g);
+}
+
+template <int JB, int MODEL>
+int launch_ls_bucket(const float2 *f, const float2 *d, const float *data, float dscale, size_t n,
+                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk)
+{
+    const int grid = one_wave(k_ls_frames<JB, MODEL>);
+    if (grid < 0) {
+        pt::set_error("ls_frames: occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return PT_ERR_CUDA;
+    }
+    k_ls_frames<JB, MODEL><<<grid, RT, 0, st>>>(f, d, data, dscale, n, gammas, J, work);
+    PT_LAUNCHED("k_ls_frames");
+    *nblk = grid;
+    return PT_OK;
 }
 
 // Launches k_ls_frames; *nblk receives the number of partials per step length.
 int launch_ls_frames(const float2 *f, const float2 *d, const float *data, float dscale, size_t n, int model,
                      const double *gammas, int J, double *work, cudaStream_t st, int *nblk)
 {
-    const int grid = J <= 2 ? ls_grid<2>() : J <= 8 ? ls_grid<8>() : ls_grid<16>();
-    if (grid < 0) {
-        pt::set_error("ls_frames: occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
-        return PT_ERR_CUDA;
+    if (model == 0) {
+        if (J <= 2) return launch_ls_bucket<2, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk);
+        if (J <= 8) return launch_ls_bucket<8, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk);
+        return launch_ls_bucket<16, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk);
     }
-    if (J <= 2)
-        k_ls_frames<2><<<grid, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
-    else if (J <= 8)
-        k_ls_frames<8><<<grid, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
-    else
-        k_ls_frames<16><<<grid, RT, 0, st>>>(f, d, data, dscale, n, model, gammas, J, work);
-    PT_LAUNCHED("k_ls_frames");
-    *nblk = grid;
-    return PT_OK;
+    if (J <= 2) return launch_ls_bucket<2, 1>(f, d, data, dscale, n, gammas, J, work, st, nblk);
+    if (J <= 8) return launch_ls_bucket<8, 1>(f, d, data, dscale, n, gammas, J, work, st, nblk);
+    return launch_ls_bucket<16, 1>(f, d, data, dscale, n, gammas, J, work, st, nblk);
 }
 
 // Lagrangian data term, solver.py:294-298.  Poisson also subtracts the

@@ -220,3 +220,27 @@ def test_cg_ptycho_det128(model):
     assert [g for _, g in gs.trace] == [g for _, g in os_.trace]
     gs.trace = None
     assert rel(pg, po) < 1e-4
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_residual_edge_values(model):
+    """The gradient residual (solver.py:220-224) at zeros, tiny and subnormal
+    values and zero counts, against numpy's angle / exp form in float64."""
+    from ptychotomo_b200 import kernels
+    rng = np.random.default_rng(9)
+    mags = np.concatenate([np.zeros(4), 10.0 ** rng.uniform(-44, 3, 400)])
+    ph = rng.uniform(-np.pi, np.pi, mags.size)
+    x = (mags * np.exp(1j * ph)).astype(np.complex64)
+    x[1] = np.complex64(1e-45 + 0j)   # subnormal parts
+    x[2] = np.complex64(-3e-42 + 2e-43j)
+    D = np.where(rng.uniform(size=x.size) < 0.3, 0.0, 10.0 ** rng.uniform(-6, 4, x.size)).astype(np.float32)
+    out = kernels.residual(torch.empty(x.size, dtype=torch.complex64, device="cuda"), T(x), T(D), 1.0, model)
+    xd = x.astype(np.complex128)
+    if model == 0:
+        ref = xd - D * xd / (np.abs(xd) ** 2 + 1e-32)
+    else:
+        ref = xd - np.sqrt(D) * np.exp(1j * np.angle(xd))
+    got = out.cpu().numpy().astype(np.complex128)
+    scale = np.maximum(np.abs(ref), np.abs(xd)) + np.sqrt(D) + 1e-30
+    assert np.all(np.isfinite(got))
+    assert np.max(np.abs(got - ref) / scale) < 2e-6
