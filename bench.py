@@ -18,6 +18,7 @@ Pass-model algorithmic bytes per call (complex64 = 8 B):
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
     python bench.py --admm        # ADMM wall time (128^3 run, 256^3 iterations)
     python bench.py --cg-kernels  # the ptycho CG's frame kernels at the operator workload
+    python bench.py --precision   # operator errors vs direct sums, reconstruction errors
 
 ``--impl reference`` times the reference's operators: by default the CPU
 restatement of the reference (oracle/, all host cores, a bounded sample of
@@ -649,6 +650,108 @@ def run_cg_kernels(args, local):
             "bytes_per_call": {"adj_resid": frame + frame // 2, "ls_frames": 2 * frame + frame // 2}}
 
 
+def run_precision(args, local):
+    """Precision of the FP32 operators and reconstructions (one GPU + host cores).
+
+    Operators at 256^3 with 512 angles on [0, pi): the USFFT forward (M = 7 and
+    the M = 4 variant) on 2 slices x 16 angles against the complex128 direct
+    sum (oracle/nudft.py), beside the complex128 gridding of the oracle on the
+    same sample; the USFFT adjoint identity over the whole volume (FP64 dots);
+    the ptycho forward of 2 angles (169 frames each, 128^2) against dense
+    complex128 DFTs.  Reconstructions: 32^3, 16 angles, 4 ADMM iterations at
+    1e2, 1e3 and 1e4 mean photons per pixel, against the oracle Solver on the
+    same counts and against the phantom.
+    """
+    import torch
+    from oracle.nudft import ptycho_fwd_exact, radon_fwd_exact
+    from oracle.ptycho import PtychoFFT
+    from oracle.solver import Solver as OSolver
+    from oracle.usfft import RadonUSFFT
+    from ptychotomo_b200 import Solver, ptychofft, radonusfft, synthetic
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    out = {}
+    n = nz = 256
+    nt = 512
+    theta = synthetic.angles(nt)
+    obj = synthetic.phantom(n, nz, seed=4).astype(np.complex64)
+    rng = np.random.default_rng(5)
+    ang = np.sort(rng.choice(nt, 16, replace=False))
+    zs = [nz // 3, 2 * nz // 3]
+    for M in (7, 4):
+        op = radonusfft(nt, nz, n, m_override=0 if M == 7 else M)
+        op.setobj(torch.from_numpy(theta).to(dev))
+        f = torch.from_numpy(obj).to(dev)
+        g = torch.empty((nt, nz, n), dtype=torch.complex64, device=dev)
+        op.fwd(g, f)
+        x = torch.empty((nt, op.N), dtype=torch.float32, device=dev)
+        y = torch.empty_like(x)
+        op.get_xy(x, y)
+        xs, ys = x.cpu().numpy()[ang], y.cpu().numpy()[ang]
+        exact = radon_fwd_exact(obj[zs], theta[ang], n, xy=(xs, ys))
+        gpu = g.cpu().numpy()[ang][:, zs]
+        row = {"gpu_vs_direct_sum": rel(gpu, exact)}
+        if M == 7:
+            orc = RadonUSFFT(len(ang), len(zs), n)
+            orc.setobj(theta[ang], xy=(xs, ys))
+            row["oracle_c128_gridding_vs_direct_sum"] = rel(orc.fwd(obj[zs]), exact)
+            gg = torch.randn((nt, nz, n), dtype=torch.complex64, device=dev, generator=torch.Generator(
+                device=dev).manual_seed(6))
+            fa = torch.empty((nz, n, n), dtype=torch.complex64, device=dev)
+            op.adj(fa, gg)
+            a = torch.vdot(g.flatten().cdouble(), gg.flatten().cdouble()).item()
+            b = torch.vdot(f.flatten().cdouble(), fa.flatten().cdouble()).item()
+            row["adjoint_identity_mismatch"] = abs(a - b) / abs(a)
+        out["radon_fwd_M%d" % M] = row
+        del op, g
+    prb = synthetic.probe(128, seed=1)
+    scan = synthetic.raster_scan(2, 13, n, nz, 128)
+    psi = np.exp(1j * 0.3 * rng.standard_normal((2, nz, n))).astype(np.complex64)
+    pop = ptychofft(2, nz, n, 2, scan.shape[2], 128, 128, 128)
+    pop.setobj(torch.from_numpy(scan).to(dev), torch.from_numpy(prb).to(dev))
+    fr = torch.empty((2, scan.shape[2], 128, 128), dtype=torch.complex64, device=dev)
+    pop.fwd(fr, torch.from_numpy(psi).to(dev))
+    orc = PtychoFFT(2, nz, n, 2, scan.shape[2], 128, 128, 128)
+    orc.setobj(scan, prb)
+    out["ptycho_fwd_det128"] = {"gpu_vs_dense_dft": rel(fr.cpu().numpy(), ptycho_fwd_exact(orc, psi))}
+    # reconstructions
+    n, nz, nt = 32, 32, 16
+    theta = synthetic.angles(nt)
+    prb = synthetic.probe(16, seed=1)
+    scan = synthetic.raster_scan(nt, 3, n, nz, 16)
+    scan[0] += np.float32(0.3)
+    obj = synthetic.phantom(n, nz, seed=2)
+    args_ = (prb, scan, theta, [16, 16], 1e-6, 5.0, nt, nz, n, nt, nz)
+    gs = Solver(*args_, device=dev)
+    x = torch.empty((nt, gs.cl_tomo.N), dtype=torch.float32, device=dev)
+    y = torch.empty_like(x)
+    gs._tomo_all.get_xy(x, y)
+    os_ = OSolver(*args_, xy=(x.cpu().numpy(), y.cpu().numpy()))
+    inten = os_.fwd_ptycho_batch(os_.exptomo(os_.fwd_tomo_batch(obj)))
+    rec = {}
+    for photons in (1e2, 1e3, 1e4):
+        sc = photons / float(inten.mean())
+        data = (np.random.default_rng(7).poisson(inten * sc) / sc).astype(np.float32)
+        psi0 = np.ones((nt, nz, n), np.complex64)
+        z3 = np.zeros((3, nz, n, n), np.complex64)
+        u0 = np.zeros((nz, n, n), np.complex64)
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        ug, _ = gs.admm(T(data), T(psi0), T(z3), T(psi0), T(z3), T(np.zeros_like(psi0)), T(z3), T(u0), 1e-3, 4, 4, 4,
+                        "poisson", verbose=False)
+        uo, _ = os_.admm(data, psi0.copy(), z3.copy(), psi0.copy(), z3.copy(), np.zeros_like(psi0), z3.copy(),
+                         u0.copy(), 1e-3, 4, 4, 4, "poisson")
+        ug = ug.cpu().numpy()
+        rec["photons_%g" % photons] = {"u_vs_oracle_solver": rel(ug, uo), "u_vs_phantom": rel(ug, obj),
+                                       "oracle_u_vs_phantom": rel(uo, obj)}
+    out["reconstruction_32cubed_4iter"] = rec
+    return {"metric": "precision study (relative L2 errors)", "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": "operators 256^3 / 512 angles (sampled 2 slices x 16 angles for the USFFT "
+                                   "direct sums, 2 angles x 169 frames for ptycho); reconstructions 32^3, 16 "
+                                   "angles, 4 ADMM iterations"},
+            "errors": out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -662,6 +765,7 @@ def main():
     ap.add_argument("--nz", type=int, default=None, help="override the slice count (small profiling cases)")
     ap.add_argument("--admm", action="store_true", help="ADMM wall time instead of operator throughput")
     ap.add_argument("--cg-kernels", action="store_true", help="device time of the ptycho CG's frame kernels")
+    ap.add_argument("--precision", action="store_true", help="operator and reconstruction errors")
     args = ap.parse_args()
     if args.ntheta:
         CFG["ntheta"] = args.ntheta
@@ -670,10 +774,10 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
-    if args.admm or args.cg_kernels:
+    if args.admm or args.cg_kernels or args.precision:
         if rank == 0:
-            line = run_admm(args, local) if args.admm else run_cg_kernels(args, local)
-            print(json.dumps(line), flush=True)
+            fn = run_admm if args.admm else run_cg_kernels if args.cg_kernels else run_precision
+            print(json.dumps(fn(args, local)), flush=True)
         return 0
     if args.impl == "reference":
         if rank != 0:

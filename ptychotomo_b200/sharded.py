@@ -239,6 +239,10 @@ class ShardedSolver(Solver):
         mu_ext = torch.cat([mu, torch.zeros_like(mu[:, :1])], dim=1)
         return super().solve_reg(ext, mu_ext, tau, alpha)[:, :-1].contiguous()
 
+    def _checkpoint_file(self, path):
+        """Each rank keeps its own shards: <path>.rank<r>of<world>."""
+        return "%s.rank%dof%d" % (path, self.comm.rank, self.comm.world)
+
     # ---- shard helpers ----------------------------------------------------
     def theta_shard(self, x):
         """This rank's angles of a global angle-major array."""

@@ -31,6 +31,7 @@ Differences from the reference, all deliberate:
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 import torch
@@ -42,6 +43,10 @@ PLANCK_CONSTANT = 6.58211928e-19  # [keV*s]  solver.py:15
 SPEED_OF_LIGHT = 299792458e+2    # [cm/s]   solver.py:16
 
 _MODELS = {"poisson": 0, "gaussian": 1}
+
+
+def _as_tuple(x):
+    return tuple(x) if isinstance(x, (list, tuple)) else x
 
 
 def _dev_tensor(x, dtype, device):
@@ -359,12 +364,47 @@ class Solver:
         lagr[6] = np.sum(lagr[0:5])  # the reference sums terms 0..4 (solver.py:304)
         return lagr
 
+    # ---- checkpoint / resume (no counterpart in the reference) ------------
+    _STATE = ("u", "psi", "h", "e", "phi", "lamd", "mu")
+
+    def _checkpoint_file(self, path):
+        return str(path)
+
+    def save_state(self, path, m, rho, tau, **arrays):
+        """Write the ADMM state after iteration m (atomically: a temporary file, then rename)."""
+        path = self._checkpoint_file(path)
+        state = {"m": int(m), "rho": float(rho), "tau": float(tau),
+                 "held": (self.theta_range, self.z_range, self.ntheta, self.nz, self.n)}
+        state.update({k: arrays[k].detach().cpu() for k in self._STATE})
+        tmp = path + ".tmp"
+        torch.save(state, tmp)
+        os.replace(tmp, path)
+
+    def load_state(self, path):
+        """The state written by save_state, arrays on this Solver's device."""
+        state = torch.load(self._checkpoint_file(path), map_location="cpu", weights_only=True)
+        if tuple(map(_as_tuple, state["held"])) != tuple(map(_as_tuple, (
+                self.theta_range, self.z_range, self.ntheta, self.nz, self.n))):
+            raise ValueError("checkpoint %s was written for another problem or shard" % path)
+        for k in self._STATE:
+            state[k] = state[k].to(self.device)
+        return state
+
     # ---- ADMM, solver.py:308-336 ------------------------------------------
     def admm(self, data, h, e, psi, phi, lamd, mu, u, alpha, piter, titer, niter, model, verbose=True,
-             history=None):
+             history=None, checkpoint=None, checkpoint_every=1, resume=False):
+        """ADMM as solver.py:308-336.  With ``checkpoint`` (a file path) the state
+        is saved every ``checkpoint_every`` iterations and after the last one;
+        with ``resume`` a run continues from that file (iteration m + 1 of the
+        same schedule) instead of from the arrays passed in."""
         data = self._as_data(data)
         rho, tau = 0.5, 0.5
-        for m in range(niter):
+        m0 = 0
+        if resume and checkpoint is not None and os.path.exists(self._checkpoint_file(checkpoint)):
+            st = self.load_state(checkpoint)
+            m0, rho, tau = st["m"] + 1, st["rho"], st["tau"]
+            u, psi, h, e, phi, lamd, mu = (st[k] for k in self._STATE)
+        for m in range(m0, niter):
             h0, e0 = h, e
             psi = self.cg_ptycho_batch(data, psi, h, lamd, rho, piter + (m < 2) * 32, model)
             xi0, xi1, Kt, pshift = self.takexi(psi, phi, lamd, mu, rho, tau)
@@ -385,4 +425,6 @@ class Solver:
                 if verbose:
                     print("%d/%d) rho=%.2e, tau=%.2e, Lagrangian terms:  %.2e %.2e %.2e %.2e %.2e %.2e, Sum: %.2e" %
                           (m, niter, rho, tau, *lagr))
+            if checkpoint is not None and ((m + 1) % checkpoint_every == 0 or m == niter - 1):
+                self.save_state(checkpoint, m, rho, tau, u=u, psi=psi, h=h, e=e, phi=phi, lamd=lamd, mu=mu)
         return u, psi

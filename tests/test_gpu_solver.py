@@ -244,3 +244,38 @@ def test_residual_edge_values(model):
     scale = np.maximum(np.abs(ref), np.abs(xd)) + np.sqrt(D) + 1e-30
     assert np.all(np.isfinite(got))
     assert np.max(np.abs(got - ref) / scale) < 2e-6
+
+
+def test_admm_checkpoint_resume_is_bitwise(problem, tmp_path):
+    """An ADMM run saved after iteration 2 and resumed gives the same bits as
+    an uninterrupted run (deterministic kernels, same penalty schedule); a
+    checkpoint of another problem is refused."""
+    gs = problem["gs"]
+    data = T(problem["data"])
+    c = dict(dtype=torch.complex64, device="cuda")
+
+    def init():
+        psi = torch.ones((16, 32, 32), **c)
+        z3 = torch.zeros((3, 32, 32, 32), **c)
+        return dict(h=psi.clone(), e=z3.clone(), psi=psi, phi=z3.clone(), lamd=torch.zeros_like(psi),
+                    mu=z3.clone(), u=torch.zeros((32, 32, 32), **c))
+
+    def run(niter, **kw):
+        a = init()
+        hist = []
+        u, psi = gs.admm(data, a["h"], a["e"], a["psi"], a["phi"], a["lamd"], a["mu"], a["u"], 1e-3, 4, 4, niter,
+                         "poisson", verbose=False, history=hist, **kw)
+        return u, psi, [(x["rho"], x["tau"]) for x in hist]
+
+    u_ref, psi_ref, hist_ref = run(4)
+    ck = str(tmp_path / "admm.pt")
+    _, _, h1 = run(2, checkpoint=ck)
+    u, psi, h2 = run(4, checkpoint=ck, resume=True)
+    assert h1 + h2 == hist_ref
+    assert torch.equal(u, u_ref) and torch.equal(psi, psi_ref)
+    st = torch.load(ck, weights_only=True)
+    assert st["m"] == 3
+    st["held"] = ((0, 8), (0, 32), 16, 32, 32)
+    torch.save(st, ck)
+    with pytest.raises(ValueError, match="another problem"):
+        run(5, checkpoint=ck, resume=True)
