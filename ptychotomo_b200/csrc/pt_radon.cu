@@ -120,6 +120,14 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
     }
 }
 
+// The forward's Fourier grid carries a halo, like the reference's (G+2M)^2
+// grid (radonusfft.cu:16, wrap in kernels.cuh:50-65): rows 0..GH_ROWS-1 are
+// repeated after row G-1 and column pairs 0..GH_PAIRS-1 after pair G/2-1, so
+// every gather window is a plain rectangle (no index wraps) addressed from one
+// base pointer.  Layout [G + GH_ROWS][G/2 + GH_PAIRS][ZC][2].
+constexpr int GH_ROWS = 14;   // 2M for the largest compiled M (7)
+constexpr int GH_PAIRS = 8;   // (2M + 2) / 2 column pairs for M = 7
+
 // ---- K2: column FFT of the 2N grid, centring sign folded in ----------------
 template <int G>
 __global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
@@ -139,15 +147,21 @@ __global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
     }
     __syncthreads();
     ptfft::fft<G, -1, T>(sm + f * PITCH, 1, t, tw);
-    // column-pair layout [ky][kx/2][z][kx&1]: one 128-byte line per (ky, pair)
+    // column-pair layout [ky][kx/2][z][kx&1]: one 128-byte line per (ky, pair),
+    // plus the halo copies (rows < GH_ROWS again at G + ky, pairs < GH_PAIRS
+    // again at G/2 + pair)
     static_assert(CK == 2, "the grid layout pairs two columns");
-    for (int e = threadIdx.x; e < G * NF; e += blockDim.x) {
-        const int ky = e / NF, r = e % NF;
+    constexpr int PS = G / 2 + GH_PAIRS;
+    const int pr = kx0 / 2;
+    for (int e = threadIdx.x; e < (G + GH_ROWS) * NF; e += blockDim.x) {
+        const int kyh = e / NF, r = e % NF;
+        const int ky = kyh < G ? kyh : kyh - G;
         const int z = r >> 1, c = r & 1;
         const int kx = kx0 + c;
         float2 v = sm[(c * ZC + z) * PITCH + ky];
         if ((kx + ky) & 1) v = -1.f * v;
-        fg[((size_t)ky * (G / 2) + kx0 / 2) * (2 * ZC) + r] = v;
+        fg[((size_t)kyh * PS + pr) * (2 * ZC) + r] = v;
+        if (pr < GH_PAIRS) fg[((size_t)kyh * PS + G / 2 + pr) * (2 * ZC) + r] = v;
     }
 }
 
@@ -194,17 +208,18 @@ __global__ void __launch_bounds__(GPB *ZC, 4)
         wy[i] = __expf(-a * (w1 * w1));
     }
     const int p0 = (c0 - odd) / 2;  // first column pair
-    const float4 *g4 = reinterpret_cast<const float4 *>(fg) + lane;
+    constexpr int PS = G / 2 + GH_PAIRS;
+    static_assert(NP <= GH_PAIRS + 1 && 2 * M <= GH_ROWS, "the grid halo must cover the window");
+    // window rows r0 .. r0 + 2M and pairs p0 .. p0 + NP - 1 lie inside the haloed grid
+    const float4 *base = reinterpret_cast<const float4 *>(fg) + ((size_t)wrapG(N + fy - M, G) * PS + p0) * ZC + lane;
     float2 acc = czero();
 #pragma unroll
     for (int i1 = 0; i1 < W; ++i1) {
-        const float4 *rowp = g4 + (size_t)wrapG(N + fy - M + i1, G) * (G / 2) * ZC;
+        const float4 *rowp = base + (size_t)i1 * PS * ZC;
         float2 rs = czero();
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
-            int pc = p0 + j;
-            pc -= pc >= G / 2 ? G / 2 : 0;
-            const float4 v = __ldg(rowp + pc * ZC);
+            const float4 v = __ldg(rowp + j * ZC);
             rs.x = fmaf(wxp[j].x, v.x, rs.x);
             rs.y = fmaf(wxp[j].x, v.y, rs.y);
             rs.x = fmaf(wxp[j].y, v.z, rs.x);
@@ -636,7 +651,7 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     if (rc == PT_OK) rc = dmalloc(&h->y, ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->fxy, 2 * ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->rbuf, N * G * ZC);
-    if (rc == PT_OK) rc = dmalloc(&h->fgrid, (size_t)G * G * ZC);
+    if (rc == PT_OK) rc = dmalloc(&h->fgrid, (size_t)(G + GH_ROWS) * (G + 2 * GH_PAIRS) * ZC);
     h->nzp = (int)((nz + ZQ - 1) / ZQ * ZQ);
     const size_t nzp = h->nzp;
     if (rc == PT_OK) rc = dmalloc(&h->lines, ntheta * N * nzp);
