@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
 // 1/N- and fftshift1c-scaled samples to lines[(theta N + k) ZC + z].
 constexpr int GPB = 32;
 template <int N, int M>
-__global__ void __launch_bounds__(GPB *ZC, 4)
+__global__ void __launch_bounds__(GPB *ZC, 3)
     k_fwd_gather_pts(const float2 *__restrict__ fg, float2 *__restrict__ lines, const float *__restrict__ xt,
                      const float *__restrict__ yt, float a, float pre)
 {
