@@ -305,61 +305,71 @@ __global__ void __launch_bounds__(ZQ *fft_threads<G>(), (G >= 1024 ? 1 : 2))
     const int z0 = blockIdx.x * ZQ;
     const int kx = col_order[blockIdx.y];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s = lane >> 4, zl = lane & 15;
+    // 4 entry streams per warp; a stream's 8 lanes hold 2 slices each (one
+    // 16-byte load of a point's line covers 2 slices)
+    const int s = lane >> 3, zl = lane & 7;
     const int nwarps = blockDim.x >> 5;
-    const float2 *lz = lines + z0 + zl;
+    const float4 *lz = reinterpret_cast<const float4 *>(lines + z0) + zl;
+    const size_t lstride = (size_t)nzp / 2;  // float4 per point line
     for (int gi = warp; gi < NG4; gi += nwarps) {
         const int beg = goff[kx * NG4 + gi], end = goff[kx * NG4 + gi + 1];
-        float2 acc[CG];
+        float4 acc[CG];  // (re, im) of slices 2 zl and 2 zl + 1, per cell
 #pragma unroll
-        for (int c = 0; c < CG; ++c) acc[c] = czero();
+        for (int c = 0; c < CG; ++c) acc[c] = make_float4(0.f, 0.f, 0.f, 0.f);
         int e = beg + s;
-        for (; e + 2 * (U - 1) < end; e += 2 * U) {
+        for (; e + 4 * (U - 1) < end; e += 4 * U) {
             int pp[U];
-            float4 w[U];
-            float2 v[U];
+            float4 w[U], v[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                pp[u] = __ldg(&gpt[e + 2 * u]);
-                w[u] = __ldg(&gw[e + 2 * u]);
+                pp[u] = __ldg(&gpt[e + 4 * u]);
+                w[u] = __ldg(&gw[e + 4 * u]);
             }
 #pragma unroll
-            for (int u = 0; u < U; ++u) v[u] = __ldg(lz + (size_t)pp[u] * nzp);
+            for (int u = 0; u < U; ++u) v[u] = __ldg(lz + (size_t)pp[u] * lstride);
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                acc[0].x = fmaf(w[u].x, v[u].x, acc[0].x);
-                acc[0].y = fmaf(w[u].x, v[u].y, acc[0].y);
-                acc[1].x = fmaf(w[u].y, v[u].x, acc[1].x);
-                acc[1].y = fmaf(w[u].y, v[u].y, acc[1].y);
-                acc[2].x = fmaf(w[u].z, v[u].x, acc[2].x);
-                acc[2].y = fmaf(w[u].z, v[u].y, acc[2].y);
-                acc[3].x = fmaf(w[u].w, v[u].x, acc[3].x);
-                acc[3].y = fmaf(w[u].w, v[u].y, acc[3].y);
+                const float wc[CG] = {w[u].x, w[u].y, w[u].z, w[u].w};
+#pragma unroll
+                for (int c = 0; c < CG; ++c) {
+                    acc[c].x = fmaf(wc[c], v[u].x, acc[c].x);
+                    acc[c].y = fmaf(wc[c], v[u].y, acc[c].y);
+                    acc[c].z = fmaf(wc[c], v[u].z, acc[c].z);
+                    acc[c].w = fmaf(wc[c], v[u].w, acc[c].w);
+                }
             }
         }
-        for (; e < end; e += 2) {
+        for (; e < end; e += 4) {
             const int pp = __ldg(&gpt[e]);
             const float4 w = __ldg(&gw[e]);
-            const float2 v = __ldg(lz + (size_t)pp * nzp);
-            acc[0].x = fmaf(w.x, v.x, acc[0].x);
-            acc[0].y = fmaf(w.x, v.y, acc[0].y);
-            acc[1].x = fmaf(w.y, v.x, acc[1].x);
-            acc[1].y = fmaf(w.y, v.y, acc[1].y);
-            acc[2].x = fmaf(w.z, v.x, acc[2].x);
-            acc[2].y = fmaf(w.z, v.y, acc[2].y);
-            acc[3].x = fmaf(w.w, v.x, acc[3].x);
-            acc[3].y = fmaf(w.w, v.y, acc[3].y);
-        }
+            const float4 v = __ldg(lz + (size_t)pp * lstride);
+            const float wc[CG] = {w.x, w.y, w.z, w.w};
 #pragma unroll
-        for (int c = 0; c < CG; ++c) {
-            acc[c].x += __shfl_down_sync(0xffffffffu, acc[c].x, 16);
-            acc[c].y += __shfl_down_sync(0xffffffffu, acc[c].y, 16);
+            for (int c = 0; c < CG; ++c) {
+                acc[c].x = fmaf(wc[c], v.x, acc[c].x);
+                acc[c].y = fmaf(wc[c], v.y, acc[c].y);
+                acc[c].z = fmaf(wc[c], v.z, acc[c].z);
+                acc[c].w = fmaf(wc[c], v.w, acc[c].w);
+            }
+        }
+        // streams 0+2 and 1+3, then 0+1: a fixed order
+#pragma unroll
+        for (int o = 16; o >= 8; o >>= 1) {
+#pragma unroll
+            for (int c = 0; c < CG; ++c) {
+                acc[c].x += __shfl_down_sync(0xffffffffu, acc[c].x, o);
+                acc[c].y += __shfl_down_sync(0xffffffffu, acc[c].y, o);
+                acc[c].z += __shfl_down_sync(0xffffffffu, acc[c].z, o);
+                acc[c].w += __shfl_down_sync(0xffffffffu, acc[c].w, o);
+            }
         }
         if (s == 0) {
 #pragma unroll
             for (int c = 0; c < CG; ++c) {
                 const int ky = gi * CG + c;
-                sm[zl * PITCH + ky] = ((kx + ky) & 1) ? -1.f * acc[c] : acc[c];  // fftshiftc
+                const float sg = ((kx + ky) & 1) ? -1.f : 1.f;  // fftshiftc
+                sm[(2 * zl) * PITCH + ky] = make_float2(sg * acc[c].x, sg * acc[c].y);
+                sm[(2 * zl + 1) * PITCH + ky] = make_float2(sg * acc[c].z, sg * acc[c].w);
             }
         }
     }
