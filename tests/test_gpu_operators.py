@@ -337,3 +337,26 @@ def test_ptycho_uneven_scan_counts(det, nprb):
     for t in range(nt):   # padded scans leave their frames untouched (zero here)
         assert not np.any(got[t, counts[t]:])
     assert rel(p_adj(op, dev(g)).cpu().numpy(), orc.adj(g)) <= TOL
+
+
+@pytest.mark.parametrize("n,nz,ntheta", [(32, 8, 24), (64, 5, 40)])
+def test_radon_m4_variant_vs_oracle(n, nz, ntheta):
+    """The M = 4 precision variant (pt_radon_create_ex) against the oracle run with
+    the same N, M and mu: the gridding approximation is shared, so the two agree
+    to FP32 accuracy; fwd and adj stay adjoint."""
+    rng = np.random.default_rng(n + 4)
+    theta = np.sort(rng.uniform(0, np.pi, ntheta)).astype(np.float32)
+    from ptychotomo_b200 import radonusfft
+    op = radonusfft(ntheta, nz, n, m_override=4)
+    assert op.M == 4
+    op.setobj(dev(theta))
+    x = torch.empty((ntheta, op.N), dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    op.get_xy(x, y)
+    torch.cuda.synchronize()
+    orc = RadonUSFFT(ntheta, nz, n, params=(op.N, op.M, op.mu))
+    orc.setobj(theta, xy=(x.cpu().numpy(), y.cpu().numpy()))
+    f = crand(rng, (nz, n, n))
+    g = crand(rng, (ntheta, nz, n))
+    assert rel(radon_fwd(op, dev(f)).cpu().numpy(), orc.fwd(f)) <= TOL
+    assert rel(radon_adj(op, dev(g)).cpu().numpy(), orc.adj(g)) <= TOL
