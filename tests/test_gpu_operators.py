@@ -360,3 +360,33 @@ def test_radon_m4_variant_vs_oracle(n, nz, ntheta):
     g = crand(rng, (ntheta, nz, n))
     assert rel(radon_fwd(op, dev(f)).cpu().numpy(), orc.fwd(f)) <= TOL
     assert rel(radon_adj(op, dev(g)).cpu().numpy(), orc.adj(g)) <= TOL
+
+
+@pytest.mark.parametrize("det,nprb", [(32, 16), (128, 128)])
+def test_ptycho_every_scan_skipped(det, nprb):
+    """All scans carry the -1 sentinel (kernels.cuh:256,280): the forward leaves
+    zero frames and the adjoint a zero object."""
+    from ptychotomo_b200 import ptychofft
+    rng = np.random.default_rng(det)
+    nt, nz, n, nscan = 3, 130, 140, 4
+    scan = -np.ones((2, nt, nscan), np.float32)
+    op = ptychofft(nt, nz, n, nt, nscan, det, det, nprb)
+    op.setobj(dev(scan), dev(crand(rng, (nprb, nprb))))
+    g = torch.full((nt, nscan, det, det), 7.0 + 1j, dtype=torch.complex64, device="cuda")
+    op.fwd(g, dev(crand(rng, (nt, nz, n))))
+    f = torch.full((nt, nz, n), 7.0 + 1j, dtype=torch.complex64, device="cuda")
+    op.adj(f, dev(crand(rng, (nt, nscan, det, det))))
+    torch.cuda.synchronize()
+    assert not g.abs().any() and not f.abs().any()
+
+
+def test_radon_largest_width_vs_oracle():
+    """n = 512 (the largest compiled width, G = 1536) on a thin case."""
+    rng = np.random.default_rng(512)
+    n, nz, nt = 512, 3, 12
+    theta = np.sort(rng.uniform(0, np.pi, nt)).astype(np.float32)
+    op, orc = make_radon(n, nz, nt, theta)
+    f = crand(rng, (nz, n, n))
+    g = crand(rng, (nt, nz, n))
+    assert rel(radon_fwd(op, dev(f)).cpu().numpy(), orc.fwd(f)) <= TOL
+    assert rel(radon_adj(op, dev(g)).cpu().numpy(), orc.adj(g)) <= TOL
