@@ -66,6 +66,17 @@ __device__ __forceinline__ float deapod(int tx, int ty, int N, float mu)
     return __expf(-mu * (tx - N / 2) * (tx - N / 2) - mu * (ty - N / 2) * (ty - N / 2));
 }
 
+// fac[ty][tx] = circ / phi / (4 N^2) on the N x N padded slice, the factor that
+// unpaddivphi / divphi and circ apply (kernels.cuh:5-37, 160-172), evaluated once
+// per handle with the expressions above; the row passes multiply by it.
+__global__ void k_deap_table(float *__restrict__ fac, int N, float mu)
+{
+    const int tx = blockIdx.x * blockDim.x + threadIdx.x, ty = blockIdx.y;
+    if (tx >= N) return;
+    const float den = (float)(4 * N * N);
+    fac[(size_t)ty * N + tx] = circ_keep(tx, ty, N) / deapod(tx, ty, N, mu) / den;
+}
+
 __device__ __forceinline__ int wrapG(int c, int G) { return c < 0 ? c + G : (c >= G ? c - G : c); }
 
 // ---- geometry: takexy, kernels.cuh:84-95 (identical expression) -----------
@@ -85,8 +96,8 @@ __global__ void k_takexy(float *x, float *y, const float *theta, int N, int nthe
 // ---- K1: pad2 + circ + divphi + fftshiftc + row FFT ------------------------
 template <int G>
 __global__ void __launch_bounds__(ZC *fft_threads<G>())
-    k_fwd_rows(const float2 *__restrict__ u, float2 *__restrict__ rbuf, int nz, int z0, float mu,
-               const float2 *__restrict__ tw)
+    k_fwd_rows(const float2 *__restrict__ u, float2 *__restrict__ rbuf, int nz, int z0,
+               const float *__restrict__ fac, const float2 *__restrict__ tw)
 {
     constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, PITCH = G + 1;
     constexpr int c0 = N / 6, c1 = 5 * N / 6 - 1;
@@ -96,18 +107,13 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
     const int z = z0 + f;
     const int sr = min(max(y, c0), c1) - c0;
     const int Y = y + N / 2;
-    const float den = (float)(4 * N * N);
     float2 *b = sm + f * PITCH;
     for (int X = t; X < G; X += T) {
         float2 v = czero();
         const int tx = X - N / 2;
         if (tx >= 0 && tx < N && z < nz) {
             const int sc = min(max(tx, c0), c1) - c0;
-            v = u[((size_t)z * n + sr) * n + sc];
-            const float keep = circ_keep(tx, y, N);
-            const float phi = deapod(tx, y, N, mu);
-            v.x = v.x * keep / phi / den;
-            v.y = v.y * keep / phi / den;
+            v = __ldg(&fac[(size_t)y * N + tx]) * u[((size_t)z * n + sr) * n + sc];
             if ((X + Y) & 1) v = -1.f * v;
         }
         b[X] = v;
@@ -416,8 +422,8 @@ __global__ void k_make_entries(const unsigned *__restrict__ keys, int *__restric
 // grid (n, nzp / ZC); reads rbuf[(r * G + kx) * nzp + z]
 template <int G>
 __global__ void __launch_bounds__(ZC *fft_threads<G>())
-    k_adj_rows(const float2 *__restrict__ rbuf, float2 *__restrict__ out, int nz, int nzp, float mu, float scale,
-               const float2 *__restrict__ tw)
+    k_adj_rows(const float2 *__restrict__ rbuf, float2 *__restrict__ out, int nz, int nzp,
+               const float *__restrict__ fac, float scale, const float2 *__restrict__ tw)
 {
     constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, c0 = N / 6, PITCH = G + 1;
     extern __shared__ float2 sm[];
@@ -429,7 +435,6 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
     }
     __syncthreads();
     ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
-    const float den = (float)(4 * N * N);
     for (int e = threadIdx.x; e < ZC * n; e += blockDim.x) {
         const int q = e / n, c = e % n;
         const int z = z0 + q;
@@ -438,11 +443,7 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
             const int X = N / 2 + tx, Y = N / 2 + ty;
             float2 v = sm[q * PITCH + X];
             if ((X + Y) & 1) v = -1.f * v;
-            const float phi = deapod(tx, ty, N, mu);
-            v.x = v.x / phi / den;
-            v.y = v.y / phi / den;
-            const float keep = circ_keep(tx, ty, N);
-            out[((size_t)z * n + r) * n + c] = (keep * scale) * v;
+            out[((size_t)z * n + r) * n + c] = scale * (__ldg(&fac[(size_t)ty * N + tx]) * v);
         }
     }
 }
@@ -466,6 +467,7 @@ struct pt_radon {
     float2 *lines = nullptr, *rbuf_adj = nullptr;
     int *goff = nullptr, *col_order = nullptr, *gpt = nullptr;
     float4 *gw = nullptr;
+    float *deap = nullptr;  // N x N: circ / phi / (4 N^2)
     size_t entries_cap = 0;
 };
 
@@ -474,7 +476,7 @@ namespace {
 void radon_free(pt_radon *h)
 {
     void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->rbuf, h->fgrid,
-                    h->lines, h->rbuf_adj, h->goff, h->col_order, h->gpt, h->gw};
+                    h->lines, h->rbuf_adj, h->goff, h->col_order, h->gpt, h->gw, h->deap};
     for (void *p : bufs)
         if (p) cudaFree(p);
 }
@@ -525,7 +527,7 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
     const float a = (float)(PI_REF * PI_REF / h->mu);
     const float pre = (float)(PI_REF / std::fabs(h->mu)) / (float)N;
     for (int z0 = 0; z0 < h->nz; z0 += ZC) {
-        k_fwd_rows<G><<<N, ZC * T, s1, st>>>(f, h->rbuf, h->nz, z0, h->mu, h->tw_G);
+        k_fwd_rows<G><<<N, ZC * T, s1, st>>>(f, h->rbuf, h->nz, z0, h->deap, h->tw_G);
         PT_LAUNCHED("k_fwd_rows");
         k_fwd_cols<G><<<G / CK, CK * ZC * T, s2, st>>>(h->rbuf, h->fgrid, h->tw_G);
         PT_LAUNCHED("k_fwd_cols");
@@ -552,7 +554,7 @@ int run_adj(pt_radon *h, float2 *f, const float2 *g, float scale, cudaStream_t s
     k_adj_colgather<G><<<dim3(nzp / ZQ, G), ZQ * T, s4, st>>>(h->lines, h->rbuf_adj, h->goff, h->gpt, h->gw,
                                                              h->col_order, nzp, h->tw_G);
     PT_LAUNCHED("k_adj_colgather");
-    k_adj_rows<G><<<dim3(n, nzp / ZC), ZC * T, s1, st>>>(h->rbuf_adj, f, h->nz, nzp, h->mu, scale, h->tw_G);
+    k_adj_rows<G><<<dim3(n, nzp / ZC), ZC * T, s1, st>>>(h->rbuf_adj, f, h->nz, nzp, h->deap, scale, h->tw_G);
     PT_LAUNCHED("k_adj_rows");
     return PT_OK;
 }
@@ -661,6 +663,7 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     if (rc == PT_OK) rc = dmalloc(&h->y, ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->fxy, 2 * ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->rbuf, N * G * ZC);
+    if (rc == PT_OK) rc = dmalloc(&h->deap, (size_t)N * N);
     if (rc == PT_OK) rc = dmalloc(&h->fgrid, (size_t)(G + GH_ROWS) * (G + 2 * GH_PAIRS) * ZC);
     h->nzp = (int)((nz + ZQ - 1) / ZQ * ZQ);
     const size_t nzp = h->nzp;
@@ -716,6 +719,8 @@ extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
     PT_CUDA(cudaMemcpyAsync(h->theta, theta, ntheta * sizeof(float), cudaMemcpyDefault, st));
     k_takexy<<<dim3((N + 127) / 128, ntheta), 128, 0, st>>>(h->x, h->y, h->theta, N, ntheta);
     PT_LAUNCHED("k_takexy");
+    k_deap_table<<<dim3((N + 127) / 128, N), 128, 0, st>>>(h->deap, N, h->mu);
+    PT_LAUNCHED("k_deap_table");
     const size_t npts = (size_t)ntheta * N;
     std::vector<float> xs(npts), ys(npts);
     PT_CUDA(cudaMemcpyAsync(xs.data(), h->x, npts * sizeof(float), cudaMemcpyDeviceToHost, st));
