@@ -19,6 +19,11 @@ Differences from the reference, all deliberate:
   rounding of zero (near convergence), where the reference's own float
   atomics make it differ from run to run;
 * takexi uses r = prb.shape[0] // 2 (solver.py:151 slices with a float);
+* cg_tomo evaluates K R u - xi0 and J u - xi1 once per call and then advances
+  them with each step (+ gamma K R d, + gamma J d, which the line search has
+  formed already) instead of re-evaluating the Radon transform of the new
+  iterate (solver.py:189-190): the same quantities up to FP32 rounding, one
+  USFFT forward and one TV pass fewer per CG iteration;
 * a CG loop stops once its line search returns gamma = 0 (gamma only
   halves, so the iterate cannot change any more; the reference would divide
   by an exactly-zero Dai-Yuan denominator next and return NaN), and a zero
@@ -227,12 +232,14 @@ class Solver:
         u = init.clone()
         gamma = 2
         grad0 = d = None
-        a = torch.empty_like(xi0)
+        # residuals a = K R u - xi0 and b = J u - xi1: evaluated for the first
+        # iterate, then advanced with the step (u + g d gives a + g K R d and
+        # b + g J d, both already formed for the line search)
+        a = K.cmul(torch.empty_like(xi0), Kt, self.fwd_tomo_batch(u))
+        K.lincomb(a, [(1.0, a), (-1.0, xi0)])
+        b = self.fwd_reg(u)
+        K.lincomb(b, [(1.0, b), (-1.0, xi1)])
         for i in range(titer):
-            KRu = K.cmul(torch.empty_like(xi0), Kt, self.fwd_tomo_batch(u))
-            gu = self.fwd_reg(u)
-            K.lincomb(a, [(1.0, KRu), (-1.0, xi0)])                       # K R u - xi0
-            b = K.lincomb(gu, [(1.0, gu), (-1.0, xi1)])                   # J u - xi1 (in place)
             ga = self.adj_tomo_batch(K.cmul(torch.empty_like(a), Kt, a, mode=2))
             grad = K.lincomb(ga, [(rho, ga), (tau, self.adj_reg(b))])
             if i == 0:
@@ -254,6 +261,9 @@ class Solver:
             K.lincomb(u, [(1.0, u), (gamma, d)])
             if gamma == 0:
                 break   # gamma only halves: u can no longer change in this call
+            if i + 1 < titer:
+                K.lincomb(a, [(1.0, a), (gamma, fd)])
+                K.lincomb(b, [(1.0, b), (gamma, gd)])
         return u
 
     # ---- CG ptychography, solver.py:206-254 -------------------------------
