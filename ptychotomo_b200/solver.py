@@ -23,7 +23,8 @@ Differences from the reference, all deliberate:
   them with each step (+ gamma K R d, + gamma J d, which the line search has
   formed already) instead of re-evaluating the Radon transform of the new
   iterate (solver.py:189-190): the same quantities up to FP32 rounding, one
-  USFFT forward and one TV pass fewer per CG iteration;
+  USFFT forward and one TV pass fewer per CG iteration; admm takes R u for
+  h (solver.py:325) from the same running sum instead of a new transform;
 * a CG loop stops once its line search returns gamma = 0 (gamma only
   halves, so the iterate cannot change any more; the reference would divide
   by an exactly-zero Dai-Yuan denominator next and return NaN), and a zero
@@ -228,14 +229,19 @@ class Solver:
 
     # ---- CG tomography, solver.py:180-203 ---------------------------------
     def cg_tomo(self, xi0, xi1, Kt, init, rho, tau, titer):
+        return self._cg_tomo(xi0, xi1, Kt, init, rho, tau, titer)[0]
+
+    def _cg_tomo(self, xi0, xi1, Kt, init, rho, tau, titer):
+        """cg_tomo, also returning R u of the final iterate (for h in admm)."""
         red = self.red
         u = init.clone()
         gamma = 2
         grad0 = d = None
-        # residuals a = K R u - xi0 and b = J u - xi1: evaluated for the first
-        # iterate, then advanced with the step (u + g d gives a + g K R d and
-        # b + g J d, both already formed for the line search)
-        a = K.cmul(torch.empty_like(xi0), Kt, self.fwd_tomo_batch(u))
+        # R u, a = K R u - xi0 and b = J u - xi1: evaluated for the first
+        # iterate, then advanced with the step (u + g d gives R u + g R d,
+        # a + g K R d and b + g J d, all formed already for the line search)
+        Ru = self.fwd_tomo_batch(u)
+        a = K.cmul(torch.empty_like(xi0), Kt, Ru)
         K.lincomb(a, [(1.0, a), (-1.0, xi0)])
         b = self.fwd_reg(u)
         K.lincomb(b, [(1.0, b), (-1.0, xi1)])
@@ -249,7 +255,8 @@ class Solver:
                 beta = red.norm2(grad) / den if den != 0 else 0.0
                 K.lincomb(d, [(-1.0, grad), (beta, d)])
             grad0 = grad
-            fd = K.cmul(torch.empty_like(xi0), Kt, self.fwd_tomo_batch(d))
+            Rd = self.fwd_tomo_batch(d)
+            fd = K.cmul(torch.empty_like(xi0), Kt, Rd)
             gd = self.fwd_reg(d)
             _, a_fd, fd2 = red.quad3(a, fd)
             _, b_gd, gd2 = red.quad3(b, gd)
@@ -261,10 +268,11 @@ class Solver:
             K.lincomb(u, [(1.0, u), (gamma, d)])
             if gamma == 0:
                 break   # gamma only halves: u can no longer change in this call
+            K.lincomb(Ru, [(1.0, Ru), (gamma, Rd)])
             if i + 1 < titer:
                 K.lincomb(a, [(1.0, a), (gamma, fd)])
                 K.lincomb(b, [(1.0, b), (gamma, gd)])
-        return u
+        return u, Ru
 
     # ---- CG ptychography, solver.py:206-254 -------------------------------
     def cg_ptycho(self, data, init, h, lamd, rho, piter, model, dscale=1.0):
@@ -418,9 +426,9 @@ class Solver:
             h0, e0 = h, e
             psi = self.cg_ptycho_batch(data, psi, h, lamd, rho, piter + (m < 2) * 32, model)
             xi0, xi1, Kt, pshift = self.takexi(psi, phi, lamd, mu, rho, tau)
-            u = self.cg_tomo(self._theta_to_z(xi0), xi1, self._theta_to_z(Kt), u, rho, tau, titer)
+            u, Ru = self._cg_tomo(self._theta_to_z(xi0), xi1, self._theta_to_z(Kt), u, rho, tau, titer)
             phi = self.solve_reg(u, mu, tau, alpha)
-            h = K.expmap(torch.empty_like(psi), self._z_to_theta(self.fwd_tomo_batch(u)),
+            h = K.expmap(torch.empty_like(psi), self._z_to_theta(Ru),
                          self.voxelsize * self.wavenumber() / self.coeftomo, pshift)
             e = self.fwd_reg(u)
             lamd = K.lincomb(torch.empty_like(lamd), [(1.0, lamd), (rho, h), (-rho, psi)])
