@@ -126,6 +126,13 @@ int pt_reduce_c64(int op, const void *a, const void *b, size_t n, int c0, int c1
  * and summed in FP64.  gammas: device double[J], J <= 16. */
 int pt_ls_frames(const void *f, const void *d, const float *data, float dscale, size_t n, int model,
                  const double *gammas, int J, void *work, void *out, void *stream);
+/* pt_ls_frames, and then f <- f + gammas[0] * d in place.  With f = F Q psi
+ * and d = F Q dir, f becomes F Q (psi + gammas[0] dir) by linearity: the
+ * frames of the next CG iterate when the line search keeps its first step
+ * (solver.py:219 recomputes them with fwd_ptycho).  The returned sums are
+ * those of the unmodified f. */
+int pt_ls_frames_advance(void *f, const void *d, const float *data, float dscale, size_t n, int model,
+                         const double *gammas, int J, void *work, void *out, void *stream);
 /* pt_ls_frames without allocating anything and without a workspace argument.
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory at call time: a host application whose memory pool owns the device

@@ -63,6 +63,7 @@ SIGNATURES = {
     "pt_reduce_workspace_bytes": (_sz, []),
     "pt_reduce_c64": (_int, [_int, _vp, _vp, _sz, _int, _int, _int, _vp, _vp, _vp]),
     "pt_ls_frames": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp, _int, _vp, _vp, _vp]),
+    "pt_ls_frames_advance": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp, _int, _vp, _vp, _vp]),
     "pt_lagr_frames": (_int, [_vp, _vp, _f, _sz, _int, _vp, _vp, _vp]),
     "pt_ls_frames_noalloc": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp, _int, _vp, _vp]),
     "pt_residual_c64": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp]),

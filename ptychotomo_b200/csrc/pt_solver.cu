@@ -189,11 +189,14 @@ __device__ __forceinline__ void ls_pixel(double (&acc)[JB], const float (&gj)[JB
     }
 }
 
-// JB = accumulator bucket (2, 8 or 16 step lengths); J <= JB are used
-template <int JB, int MODEL>
+// JB = accumulator bucket (2, 8 or 16 step lengths); J <= JB are used.
+// ADV: also store f + gam[0] d over f (the frames of the step gam[0], by
+// linearity of F Q), in place: each pixel is read and written by one thread.
+template <int JB, int MODEL, bool ADV = false>
 __global__ void __launch_bounds__(RT) k_ls_frames(const float2 *__restrict__ f, const float2 *__restrict__ d,
                                                   const float *__restrict__ D, float dscale, size_t n,
-                                                  const double *__restrict__ gam, int J, double *__restrict__ work)
+                                                  const double *__restrict__ gam, int J, double *__restrict__ work,
+                                                  float2 *fo = nullptr)
 {
     double acc[JB];
 #pragma unroll
@@ -216,8 +219,17 @@ __global__ void __launch_bounds__(RT) k_ls_frames(const float2 *__restrict__ f, 
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) ls_pixel<JB, MODEL>(acc, gj, J, x[u], y[u], dd[u] * dscale);
+        if (ADV) {
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                fo[i + u * stride] = make_float2(fmaf(gj[0], y[u].x, x[u].x), fmaf(gj[0], y[u].y, x[u].y));
+        }
     }
-    for (; i < n; i += stride) ls_pixel<JB, MODEL>(acc, gj, J, f[i], d[i], D[i] * dscale);
+    for (; i < n; i += stride) {
+        const float2 x = f[i], y = d[i];
+        ls_pixel<JB, MODEL>(acc, gj, J, x, y, D[i] * dscale);
+        if (ADV) fo[i] = make_float2(fmaf(gj[0], y.x, x.x), fmaf(gj[0], y.y, x.y));
+    }
     block_reduce_store<JB>(acc, work, blockIdx.x, gridDim.x);
 }
 
@@ -236,25 +248,36 @@ int one_wave(Kern kern)
     return g < 1 ? 1 : (g > RB ? RB : g);
 }
 
-template <int JB, int MODEL>
+template <int JB, int MODEL, bool ADV = false>
 int launch_ls_bucket(const float2 *f, const float2 *d, const float *data, float dscale, size_t n,
-                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk)
+                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk, float2 *fo = nullptr)
 {
-    const int grid = one_wave(k_ls_frames<JB, MODEL>);
+    const int grid = one_wave(k_ls_frames<JB, MODEL, ADV>);
     if (grid < 0) {
         pt::set_error("ls_frames: occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
         return PT_ERR_CUDA;
     }
-    k_ls_frames<JB, MODEL><<<grid, RT, 0, st>>>(f, d, data, dscale, n, gammas, J, work);
+    k_ls_frames<JB, MODEL, ADV><<<grid, RT, 0, st>>>(f, d, data, dscale, n, gammas, J, work, fo);
     PT_LAUNCHED("k_ls_frames");
     *nblk = grid;
     return PT_OK;
 }
 
 // Launches k_ls_frames; *nblk receives the number of partials per step length.
+// fo != nullptr: the advancing variant (fo = f + gammas[0] d, fo may be f).
 int launch_ls_frames(const float2 *f, const float2 *d, const float *data, float dscale, size_t n, int model,
-                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk)
+                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk, float2 *fo = nullptr)
 {
+    if (fo != nullptr) {
+        if (model == 0) {
+            if (J <= 2) return launch_ls_bucket<2, 0, true>(f, d, data, dscale, n, gammas, J, work, st, nblk, fo);
+            if (J <= 8) return launch_ls_bucket<8, 0, true>(f, d, data, dscale, n, gammas, J, work, st, nblk, fo);
+            return launch_ls_bucket<16, 0, true>(f, d, data, dscale, n, gammas, J, work, st, nblk, fo);
+        }
+        if (J <= 2) return launch_ls_bucket<2, 1, true>(f, d, data, dscale, n, gammas, J, work, st, nblk, fo);
+        if (J <= 8) return launch_ls_bucket<8, 1, true>(f, d, data, dscale, n, gammas, J, work, st, nblk, fo);
+        return launch_ls_bucket<16, 1, true>(f, d, data, dscale, n, gammas, J, work, st, nblk, fo);
+    }
     if (model == 0) {
         if (J <= 2) return launch_ls_bucket<2, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk);
         if (J <= 8) return launch_ls_bucket<8, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk);
@@ -475,6 +498,23 @@ extern "C" int pt_ls_frames(const void *f, const void *d, const float *data, flo
     int nblk = 0;
     const int rc = launch_ls_frames((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J,
                                     (double *)work, st, &nblk);
+    if (rc != PT_OK) return rc;
+    k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, J, nblk, 0);
+    PT_LAUNCHED("k_finish");
+    return PT_OK;
+}
+
+extern "C" int pt_ls_frames_advance(void *f, const void *d, const float *data, float dscale, size_t n, int model,
+                                    const double *gammas, int J, void *work, void *out, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(f && d && data && gammas && work && out, "ls_frames_advance: null pointer");
+    PT_CHECK_ARG(J >= 1 && J <= MAXK, "ls_frames_advance: 1 <= J <= %d", MAXK);
+    PT_CHECK_ARG(model == 0 || model == 1, "ls_frames_advance: model 0 (poisson) or 1 (gaussian)");
+    cudaStream_t st = (cudaStream_t)stream;
+    int nblk = 0;
+    const int rc = launch_ls_frames((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J,
+                                    (double *)work, st, &nblk, (float2 *)f);
     if (rc != PT_OK) return rc;
     k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, J, nblk, 0);
     PT_LAUNCHED("k_finish");

@@ -75,13 +75,17 @@ class Reducer:
     def maxangle(self, a):
         return self._run(7, a)[0]
 
-    def ls_frames(self, f, d, data, dscale, model, gammas):
-        """Ptycho data term for each step length in `gammas` (<= 16)."""
+    def ls_frames(self, f, d, data, dscale, model, gammas, advance=False):
+        """Ptycho data term for each step length in `gammas` (<= 16).
+
+        ``advance``: afterwards f <- f + gammas[0] d in place (pt_ls_frames_advance).
+        """
         J = len(gammas)
         self.gam[:J].copy_(torch.tensor(gammas, dtype=torch.float64), non_blocking=False)
-        check(lib().pt_ls_frames(_c64(f), _c64(d) if d is not None else None, _p(data), float(dscale),
-                                 f.numel(), model, _p(self.gam), J, _p(self.work), _p(self.out),
-                                 current_stream()), "ls_frames")
+        fn = lib().pt_ls_frames_advance if advance else lib().pt_ls_frames
+        check(fn(_c64(f), _c64(d) if d is not None else None, _p(data), float(dscale),
+                 f.numel(), model, _p(self.gam), J, _p(self.work), _p(self.out),
+                 current_stream()), "ls_frames")
         return self.out[:J].tolist()
 
     def lagr_frames(self, f, data, dscale, model):

@@ -25,6 +25,10 @@ Differences from the reference, all deliberate:
   iterate (solver.py:189-190): the same quantities up to FP32 rounding, one
   USFFT forward and one TV pass fewer per CG iteration; admm takes R u for
   h (solver.py:325) from the same running sum instead of a new transform;
+* likewise cg_ptycho takes F Q psi of the next iterate as F Q psi + gamma
+  F Q d, stored by the line-search kernel for its first candidate step,
+  whenever that step is the one taken (solver.py:219 recomputes it); the
+  forward is recomputed otherwise;
 * a CG loop stops once its line search returns gamma = 0 (gamma only
   halves, so the iterate cannot change any more; the reference would divide
   by an exactly-zero Dai-Yuan denominator next and return NaN), and a zero
@@ -219,6 +223,9 @@ class Solver:
         return gamma
 
     trace = None   # list: records (kind, gamma) of every CG line search when set
+    # ptycho CG: the line search also advances the frames by its first step, and
+    # the next iteration reuses them instead of a new forward when that step is taken
+    advance_frames = True
 
     @staticmethod
     def _halve_until(gamma, decrease):
@@ -283,8 +290,10 @@ class Solver:
         gamma = 2
         grad0 = d = None
         w = torch.empty_like(psi)
+        fpsi = None
         for i in range(piter):
-            fpsi = self.fwd_ptycho(psi)
+            if fpsi is None:
+                fpsi = self.fwd_ptycho(psi)
             grad = self._empty([self.ptheta, self.nz, self.n])   # Q*F*(residual), residual formed on load
             self.cl_ptycho.adj_resid(grad, fpsi, data, dscale, mdl, scale=self.coefptycho)
             K.lincomb(w, [(1.0, h), (-1.0, psi), (1.0 / rho, lamd)])     # h - psi + lamd/rho
@@ -301,12 +310,19 @@ class Solver:
             # minf(psi) - minf(psi + g d) = data-term decrease (per element, FP64)
             #   + rho (2 g Re<w, d> - g^2 ||d||^2)  for the penalty rho ||w - g d||^2
             npass = 0
+            advanced = None   # the step by which the first pass advanced fpsi
             while True:
                 # gamma usually survives: try (g, g/2) first, then 8, then 16 halvings per pass
                 J = (2, 8, 16)[min(npass, 2)]
-                npass += 1
                 gs = [gamma * 0.5 ** j for j in range(J)]
-                vals = red.ls_frames(fpsi, fd, data, dscale, mdl, gs)
+                adv = self.advance_frames and npass == 0 and i + 1 < piter
+                if advanced is not None:   # a later pass needs the frames of psi itself
+                    fpsi = self.fwd_ptycho(psi)
+                    advanced = None
+                npass += 1
+                vals = red.ls_frames(fpsi, fd, data, dscale, mdl, gs, advance=adv)
+                if adv:
+                    advanced = gs[0]
                 chosen = None
                 for g, dec_data in zip(gs, vals):
                     dec = dec_data + rho * (2 * g * w_d - g * g * d2)
@@ -320,7 +336,11 @@ class Solver:
             if self.trace is not None:
                 self.trace.append(("ptycho", gamma))
             K.lincomb(psi, [(1.0, psi), (gamma, d)])
-            del fpsi, fd
+            # fpsi + gamma fd = F Q (psi + gamma d): kept when the step taken is
+            # the one the line search advanced the frames by
+            if advanced is None or gamma != advanced:
+                fpsi = None
+            del fd
             if gamma == 0:
                 break   # gamma only halves: psi can no longer change in this call
         if red.maxangle(psi) > 3.14:

@@ -279,3 +279,41 @@ def test_admm_checkpoint_resume_is_bitwise(problem, tmp_path):
     torch.save(st, ck)
     with pytest.raises(ValueError, match="another problem"):
         run(5, checkpoint=ck, resume=True)
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_ls_frames_advance(model):
+    """pt_ls_frames_advance returns pt_ls_frames's sums (same kernel and order)
+    and leaves f + gammas[0] d in f."""
+    from ptychotomo_b200 import kernels
+    rng = np.random.default_rng(31 + model)
+    n = 5 * 7 * 32 * 32 + 3
+    f = T(crand(rng, (n,)))
+    d = T(0.1 * crand(rng, (n,)))
+    data = T(rng.poisson(3.0, n).astype(np.float32))
+    gs = [0.75, 0.375]
+    red = kernels.Reducer("cuda")
+    ref = red.ls_frames(f, d, data, 0.8, model, gs)
+    f2 = f.clone()
+    got = red.ls_frames(f2, d, data, 0.8, model, gs, advance=True)
+    assert got == ref
+    want = f + np.float32(0.75) * d
+    assert torch.allclose(f2, want, rtol=1e-6, atol=1e-7)
+
+
+@pytest.mark.parametrize("model", ["poisson", "gaussian"])
+def test_cg_ptycho_advanced_frames_match_recomputed(problem, model):
+    """The ptycho CG with frames advanced by the line search takes the same steps
+    as the CG that recomputes F Q psi every iteration."""
+    gs = problem["gs"]
+    data = problem["data"]
+    psi0 = np.ones((16, 32, 32), np.complex64)
+    h, lamd = np.ones_like(psi0), np.zeros_like(psi0)
+    out = []
+    for adv in (True, False):
+        gs.advance_frames, gs.trace = adv, []
+        p = gs.cg_ptycho_batch(T(data), T(psi0), T(h), T(lamd), 0.5, 8, model)
+        out.append(([g for _, g in gs.trace], p.cpu().numpy()))
+    gs.advance_frames, gs.trace = True, None
+    assert out[0][0] == out[1][0]
+    assert rel(out[0][1], out[1][1]) < 1e-5
