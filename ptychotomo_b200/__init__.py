@@ -5,9 +5,11 @@ classes :class:`radonusfft` and :class:`ptychofft` (same constructor and
 method signatures as the reference's SWIG classes) and the ADMM
 :class:`Solver` (same methods as src/ptychotomo/solver.py) on torch CUDA
 tensors.  All arithmetic runs in the sm_100a library
-``libptychotomo_b200.so``; there is no CPU fallback.
+``libptychotomo_b200.so``; there is no CPU fallback.  The reference's host
+helpers :func:`probe` and :func:`scanner3` (NumPy) are provided too.
 """
 from ._lib import PtychotomoArgError, PtychotomoError, lib  # noqa: F401
+from .objects import probe, scanner3  # noqa: F401
 from .operators import ptychofft, radonusfft  # noqa: F401
 
 __version__ = "0.1.0"
