@@ -103,6 +103,21 @@ int pt_ptycho_adj_scaled(pt_ptycho *h, void *f, const void *g, float scale, void
  * not modified. */
 int pt_ptycho_adj_resid(pt_ptycho *h, void *f, const void *fpsi, const float *data, float dscale, int model,
                         float scale, void *stream);
+/* Probe retrieval: the operator as a linear map of the probe.  No counterpart
+ * in the reference, which keeps the probe fixed.
+ *   pt_ptycho_adj_probe:       gprb[P][P] = scale * c * sum over frames of
+ *       conj(psi patch) * (inverse 2-D DFT of conj(phase) * g), the adjoint of
+ *       fwd with respect to the probe for the object psi [Ntheta][Nz][N];
+ *   pt_ptycho_adj_probe_resid: the same with g = the data-term residual of
+ *       fpsi (as pt_ptycho_adj_resid): the data term's probe gradient;
+ *   pt_ptycho_fwd_probe:       fwd(g, psi) with the probe prb [P][P] instead
+ *       of the one given to setobj (which stays in place).
+ * Deterministic (fixed-order sum of per-block partials).  Detectors 16..128;
+ * PT_ERR_UNSUPPORTED for 8. */
+int pt_ptycho_adj_probe(pt_ptycho *h, void *gprb, const void *g, const void *psi, float scale, void *stream);
+int pt_ptycho_adj_probe_resid(pt_ptycho *h, void *gprb, const void *psi, const void *fpsi, const float *data,
+                              float dscale, int model, float scale, void *stream);
+int pt_ptycho_fwd_probe(pt_ptycho *h, void *g, const void *psi, const void *prb, float scale, void *stream);
 
 
 /* ---- Solver arithmetic (src/ptychotomo/solver.py:48-336) -----------------

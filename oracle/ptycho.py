@@ -92,3 +92,32 @@ class PtychoFFT:
                     continue
                 f[t, y0:y0 + P, x0:x0 + P] += (cp * g[t, s, rs:rs + P, cs:cs + P]).T
         return f
+
+    # ---- adjoint with respect to the probe (no counterpart in the reference) --
+    def adj_probe(self, g, f):
+        """gprb[ix, iy] = c sum_frames conj(f[t, y0 + iy, x0 + ix]) G[t, s, rs + ix, cs + iy],
+        G = unnormalised inverse DFT of conj(phase) g: the adjoint of fwd as a
+        linear map of the probe, for the object f."""
+        P, dx, dy = self.nprb, self.detx, self.dety
+        g = np.asarray(g).reshape(self.ntheta, self.nscan, dx, dy).astype(np.complex128)
+        f = np.asarray(f).reshape(self.ntheta, self.nz, self.n)
+        rs, cs = (dx - P) // 2, (dy - P) // 2
+        G = np.fft.ifft2(g * np.conj(self.phase)[:, :, None, None], axes=(-2, -1)) * (dx * dy)
+        gp = np.zeros((P, P), np.complex128)
+        for t in range(self.ntheta):
+            for s in range(self.nscan):
+                x0, y0 = self.stx[t, s], self.sty[t, s]
+                if x0 < 0 or y0 < 0:
+                    continue
+                patch = f[t, y0:y0 + P, x0:x0 + P].astype(np.complex128).T   # [ix, iy]
+                gp += np.conj(patch) * G[t, s, rs:rs + P, cs:cs + P]
+        return self.c * gp
+
+    def fwd_probe(self, f, prb):
+        """fwd with the probe prb instead of the one given to setobj."""
+        own = self.prb
+        self.prb = np.asarray(prb).astype(np.complex128).reshape(self.nprb, self.nprb)
+        try:
+            return self.fwd(f)
+        finally:
+            self.prb = own

@@ -60,6 +60,9 @@ SIGNATURES = {
     "pt_ptycho_fwd_scaled": (_int, [_vp, _vp, _vp, _f, _vp]),
     "pt_ptycho_adj_scaled": (_int, [_vp, _vp, _vp, _f, _vp]),
     "pt_ptycho_adj_resid": (_int, [_vp, _vp, _vp, _vp, _f, _int, _f, _vp]),
+    "pt_ptycho_adj_probe": (_int, [_vp, _vp, _vp, _vp, _f, _vp]),
+    "pt_ptycho_adj_probe_resid": (_int, [_vp, _vp, _vp, _vp, _vp, _f, _int, _f, _vp]),
+    "pt_ptycho_fwd_probe": (_int, [_vp, _vp, _vp, _vp, _f, _vp]),
     "pt_reduce_workspace_bytes": (_sz, []),
     "pt_reduce_c64": (_int, [_int, _vp, _vp, _sz, _int, _int, _int, _vp, _vp, _vp]),
     "pt_ls_frames": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp, _int, _vp, _vp, _vp]),

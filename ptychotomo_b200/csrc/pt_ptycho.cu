@@ -655,6 +655,102 @@ __global__ void k_probe_t(const float2 *__restrict__ prb, float2 *__restrict__ p
     prbT[i] = c * prb[ix * P + iy];
 }
 
+// ---- adjoint with respect to the probe (no counterpart in the reference) ----
+// The forward is linear in the probe too: with c prbT[py][px] = c prb[px P + py]
+// multiplying psi[th][sty + py][stx + px] (ptychofft.cu:58-76, kernels.cuh:
+// 243-265), the adjoint maps frames g to
+//   gprb[px P + py] = c sum_frames conj(psi[th][sty + py][stx + px]) G[py][px],
+// G = scale x inverse DFT of conj(phase) g (the same transform as the object
+// adjoint).  Block b walks frames b, b + gridDim.x, ... and accumulates into
+// its own P x P partial part[b] (prbT layout); every (py, px) of the window
+// belongs to one thread, so no atomics; k_probe_reduce sums the partials in
+// block order.  RESID: the frames are the data-term residual of g (as
+// k_ptycho_adj).
+template <int DET, int RESID>
+__global__ void __launch_bounds__(PF<DET>::NT, 1)
+    k_ptycho_adj_probe(const float2 *__restrict__ g, float2 *__restrict__ part, const float2 *__restrict__ psi,
+                       const int *__restrict__ corner, const float2 *__restrict__ phase, int nz, int n, int nscan,
+                       int nframes, int P, float scale, const float2 *__restrict__ tw, const float *__restrict__ data,
+                       float dscale)
+{
+    using F = PF<DET>;
+    extern __shared__ float2 sm[];
+    float2 *fr = sm;
+    float2 *tws = sm + DET * F::P;
+    float2 *acc = part + (size_t)blockIdx.x * P * P;
+    for (int i = threadIdx.x; i < DET; i += F::NT) tws[i] = tw[i];
+    for (int e = threadIdx.x; e < P * P; e += F::NT) acc[e] = czero();
+    const int t = threadIdx.x % F::N2, grp = threadIdx.x / F::N2;
+    float2 *sc = fr + grp * (DET + 1);
+    const int off = (DET - P) / 2;
+    __syncthreads();
+    for (int fid = blockIdx.x; fid < nframes; fid += gridDim.x) {
+        const int th = fid / nscan;
+        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
+        if (stx < 0 || sty < 0) continue;
+        const float2 ph = phase[fid];
+        const float2 *in = g + (size_t)fid * DET * DET;
+        float2 v[F::CPG][F::N1];
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            const int kx = grp + F::NG * c;
+#pragma unroll
+            for (int m = 0; m < F::N1; ++m) {
+                const int e = kx * DET + t + F::N2 * m;
+                v[c][m] = scale * cmulc(ph, resid<RESID>(__ldg(&in[e]), data, (size_t)fid * DET * DET + e, dscale));
+            }
+            line_dft<DET, +1>(v[c], t, sc, tws);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            const int kx = grp + F::NG * c;
+#pragma unroll
+            for (int j = 0; j < F::KPT; ++j)
+#pragma unroll
+                for (int k2 = 0; k2 < F::N2; ++k2) {
+                    const int iy = t * F::KPT + j + F::N1 * k2;
+                    fr[iy * F::P + (kx ^ fswz<DET>(iy))] = v[c][j * F::N2 + k2];
+                }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            const int iy = grp + F::NG * c;
+            const int sw = fswz<DET>(iy);
+#pragma unroll
+            for (int m = 0; m < F::N1; ++m) v[c][m] = fr[iy * F::P + ((t + F::N2 * m) ^ sw)];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < F::CPG; ++c) {
+            line_dft<DET, +1>(v[c], t, sc, tws);
+            const int py = grp + F::NG * c - off;
+            if (py < 0 || py >= P) continue;
+            const float2 *orow = psi + ((size_t)th * nz + sty + py) * n + stx;
+            float2 *arow = acc + (size_t)py * P;
+#pragma unroll
+            for (int k2 = 0; k2 < F::N2; ++k2)
+#pragma unroll
+                for (int j = 0; j < F::KPT; ++j) {
+                    const int px = t * F::KPT + j + F::N1 * k2 - off;
+                    if (px >= 0 && px < P) arow[px] = arow[px] + cmulc(__ldg(&orow[px]), v[c][j * F::N2 + k2]);
+                }
+        }
+    }
+}
+
+// gprb[px P + py] = c sum_b part[b][py P + px], blocks in order
+__global__ void k_probe_reduce(const float2 *__restrict__ part, float2 *__restrict__ gprb, int nblk, int P, float c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P * P) return;
+    float2 s = part[i];
+    for (int b = 1; b < nblk; ++b) s = s + part[(size_t)b * P * P + i];
+    const int py = i / P, px = i % P;
+    gprb[px * P + py] = c * s;
+}
+
 }  // namespace
 
 struct pt_ptycho {
@@ -664,6 +760,10 @@ struct pt_ptycho {
     float c = 0.f;
     float2 *tw = nullptr, *prb = nullptr, *prbT = nullptr, *phase = nullptr, *partial = nullptr;
     int *corner = nullptr;
+    // probe retrieval: a second transposed probe table (forward with a given
+    // probe) and one P x P partial per block of the probe adjoint
+    float2 *prbT2 = nullptr, *prb_part = nullptr;
+    int prb_blocks = 0;
 };
 
 namespace {
@@ -686,6 +786,9 @@ int ptycho_attrs()
         PT_ATTR((k_ptycho_adj<DET, 0>), s);
         PT_ATTR((k_ptycho_adj<DET, 1>), s);
         PT_ATTR((k_ptycho_adj<DET, 2>), s);
+        PT_ATTR((k_ptycho_adj_probe<DET, 0>), s);
+        PT_ATTR((k_ptycho_adj_probe<DET, 1>), s);
+        PT_ATTR((k_ptycho_adj_probe<DET, 2>), s);
         if constexpr (DET == 128) {
             PT_ATTR(k_ptycho_fwd128<true>, P128_SMEM);
             PT_ATTR(k_ptycho_fwd128<false>, P128_SMEM);
@@ -799,9 +902,44 @@ int ptycho_dispatch(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float
     return PT_ERR_UNSUPPORTED;
 }
 
+template <int DET, int RESID>
+int probe_adj_launch(pt_ptycho *h, float2 *gprb, const float2 *in, const float2 *psi, float scale, const float *data,
+                     float dscale, cudaStream_t st)
+{
+    if constexpr (DET < 16) {
+        pt::set_error("ptychofft.adj_probe: not compiled for detector %d (16 to 128)", DET);
+        return PT_ERR_UNSUPPORTED;
+    } else {
+        using F = PF<DET>;
+        const int nframes = h->ntheta * h->nscan;
+        k_ptycho_adj_probe<DET, RESID><<<h->prb_blocks, F::NT, F::SMEM, st>>>(
+            in, h->prb_part, psi, h->corner, h->phase, h->nz, h->n, h->nscan, nframes, h->P, scale, h->tw, data,
+            dscale);
+        PT_LAUNCHED("k_ptycho_adj_probe");
+        k_probe_reduce<<<(h->P * h->P + 255) / 256, 256, 0, st>>>(h->prb_part, gprb, h->prb_blocks, h->P, h->c);
+        PT_LAUNCHED("k_probe_reduce");
+        return PT_OK;
+    }
+}
+
+int probe_adj_dispatch(pt_ptycho *h, float2 *gprb, const float2 *in, const float2 *psi, float scale, int resid_mode,
+                       const float *data, float dscale, cudaStream_t st)
+{
+#define PT_CASE(D)                                                                               \
+    if (h->det == D) {                                                                           \
+        if (resid_mode == 1) return probe_adj_launch<D, 1>(h, gprb, in, psi, scale, data, dscale, st); \
+        if (resid_mode == 2) return probe_adj_launch<D, 2>(h, gprb, in, psi, scale, data, dscale, st); \
+        return probe_adj_launch<D, 0>(h, gprb, in, psi, scale, data, dscale, st);                \
+    }
+    PT_PTYCHO_DETS(PT_CASE)
+#undef PT_CASE
+    pt::set_error("ptychofft: detector size %d not compiled", h->det);
+    return PT_ERR_UNSUPPORTED;
+}
+
 void ptycho_free(pt_ptycho *h)
 {
-    void *bufs[] = {h->tw, h->prb, h->prbT, h->phase, h->partial, h->corner};
+    void *bufs[] = {h->tw, h->prb, h->prbT, h->phase, h->partial, h->corner, h->prbT2, h->prb_part};
     for (void *p : bufs)
         if (p) cudaFree(p);
 }
@@ -864,7 +1002,11 @@ extern "C" int pt_ptycho_create(size_t ntheta, size_t nz, size_t n, size_t nthet
               (h->parts == 1 || cudaMalloc((void **)&h->partial, (size_t)h->parts * ntheta * nz * n * sizeof(float2)) ==
                                     cudaSuccess) &&
               cudaMalloc((void **)&h->phase, ntheta * nscan * sizeof(float2)) == cudaSuccess &&
-              cudaMalloc((void **)&h->corner, 2 * ntheta * nscan * sizeof(int)) == cudaSuccess;
+              cudaMalloc((void **)&h->corner, 2 * ntheta * nscan * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&h->prbT2, nprb * nprb * sizeof(float2)) == cudaSuccess;
+    // probe adjoint: one block per SM (two below 64x64 detectors), one partial each
+    h->prb_blocks = (int)std::min<size_t>((size_t)nsm * (detx >= 64 ? 1 : 2), ntheta * nscan);
+    ok = ok && cudaMalloc((void **)&h->prb_part, (size_t)h->prb_blocks * nprb * nprb * sizeof(float2)) == cudaSuccess;
     if (!ok) {
         ptycho_free(h);
         delete h;
@@ -979,4 +1121,61 @@ extern "C" int pt_ptycho_adj_resid(pt_ptycho *h, void *f, const void *fpsi, cons
     PT_CHECK_ARG(dev == h->device, "ptychofft handle belongs to device %d, current device is %d", h->device, dev);
     return ptycho_dispatch(h, true, (float2 *)f, (const float2 *)fpsi, scale, (cudaStream_t)stream, model + 1, data,
                            dscale);
+}
+
+// ---- probe retrieval (no counterpart in the reference) -----------------------
+namespace {
+int probe_checks(pt_ptycho *h, const char *what)
+{
+    PT_CHECK_ARG(h != nullptr, "ptychofft.%s: null handle", what);
+    if (!h->ready) {
+        pt::set_error("ptychofft.%s: setobj(scan, prb) has not been called", what);
+        return PT_ERR_STATE;
+    }
+    int dev = -1;
+    PT_CUDA(cudaGetDevice(&dev));
+    PT_CHECK_ARG(dev == h->device, "ptychofft handle belongs to device %d, current device is %d", h->device, dev);
+    return PT_OK;
+}
+}  // namespace
+
+extern "C" int pt_ptycho_adj_probe(pt_ptycho *h, void *gprb, const void *g, const void *psi, float scale,
+                                   void *stream)
+{
+    pt::clear_error();
+    const int rc = probe_checks(h, "adj_probe");
+    if (rc != PT_OK) return rc;
+    PT_CHECK_ARG(gprb && g && psi, "ptychofft.adj_probe: null array pointer");
+    return probe_adj_dispatch(h, (float2 *)gprb, (const float2 *)g, (const float2 *)psi, scale, 0, nullptr, 1.f,
+                              (cudaStream_t)stream);
+}
+
+extern "C" int pt_ptycho_adj_probe_resid(pt_ptycho *h, void *gprb, const void *psi, const void *fpsi,
+                                         const float *data, float dscale, int model, float scale, void *stream)
+{
+    pt::clear_error();
+    const int rc = probe_checks(h, "adj_probe_resid");
+    if (rc != PT_OK) return rc;
+    PT_CHECK_ARG(gprb && psi && fpsi && data, "ptychofft.adj_probe_resid: null array pointer");
+    PT_CHECK_ARG(model == 0 || model == 1, "ptychofft.adj_probe_resid: model 0 (poisson) or 1 (gaussian)");
+    return probe_adj_dispatch(h, (float2 *)gprb, (const float2 *)fpsi, (const float2 *)psi, scale, model + 1, data,
+                              dscale, (cudaStream_t)stream);
+}
+
+extern "C" int pt_ptycho_fwd_probe(pt_ptycho *h, void *g, const void *psi, const void *prb, float scale,
+                                   void *stream)
+{
+    pt::clear_error();
+    const int rc = probe_checks(h, "fwd_probe");
+    if (rc != PT_OK) return rc;
+    PT_CHECK_ARG(g && psi && prb, "ptychofft.fwd_probe: null array pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    k_probe_t<<<(h->P * h->P + 255) / 256, 256, 0, st>>>((const float2 *)prb, h->prbT2, h->P, h->c);
+    PT_LAUNCHED("k_probe_t");
+    // the forward kernels read the handle's table: point it at this probe for one launch
+    float2 *own = h->prbT;
+    h->prbT = h->prbT2;
+    const int rc2 = ptycho_dispatch(h, false, (float2 *)g, (const float2 *)psi, scale, st);
+    h->prbT = own;
+    return rc2;
 }

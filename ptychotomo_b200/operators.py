@@ -100,6 +100,23 @@ class ptychofft:  # noqa: N801 - reference class name
         check(lib().pt_ptycho_adj_resid(self._h, as_ptr(f), as_ptr(fpsi), as_ptr(data), float(dscale), int(model),
                                         float(scale), _s(stream)), "ptychofft.adj_resid")
 
+    # ---- probe retrieval (no counterpart in the reference) -----------------
+    def adj_probe(self, gprb, g, psi, scale=1.0, stream=None):
+        """gprb [Nprb, Nprb] = adjoint of fwd as a map of the probe, for the object psi."""
+        check(lib().pt_ptycho_adj_probe(self._h, as_ptr(gprb), as_ptr(g), as_ptr(psi), float(scale), _s(stream)),
+              "ptychofft.adj_probe")
+
+    def adj_probe_resid(self, gprb, psi, fpsi, data, dscale, model, scale=1.0, stream=None):
+        """Probe gradient of the data term: adj_probe of residual(fpsi, dscale * data)."""
+        check(lib().pt_ptycho_adj_probe_resid(self._h, as_ptr(gprb), as_ptr(psi), as_ptr(fpsi), as_ptr(data),
+                                              float(dscale), int(model), float(scale), _s(stream)),
+              "ptychofft.adj_probe_resid")
+
+    def fwd_probe(self, g, psi, prb, scale=1.0, stream=None):
+        """fwd(g, psi) with the probe prb instead of the one given to setobj."""
+        check(lib().pt_ptycho_fwd_probe(self._h, as_ptr(g), as_ptr(psi), as_ptr(prb), float(scale), _s(stream)),
+              "ptychofft.fwd_probe")
+
     def free(self):
         if getattr(self, "_h", None):
             lib().pt_ptycho_destroy(self._h)

@@ -80,6 +80,16 @@ class ShardComm:
         dist.all_reduce(t, op=dist.ReduceOp.SUM if op == "sum" else dist.ReduceOp.MAX, group=self.group)
         return t.tolist()
 
+    def allreduce_tensor(self, x):
+        """Sum of a (complex) tensor over the ranks; every rank receives it."""
+        if self.world == 1:
+            return x
+        xr = torch.view_as_real(x) if x.is_complex() else x
+        buf = self._out(xr.contiguous())
+        dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=self.group)
+        buf = self._back(buf, x)
+        return torch.view_as_complex(buf.contiguous()) if x.is_complex() else buf
+
     # ---- angle <-> slice re-sharding --------------------------------------
     def theta_to_z(self, x):
         """[angles held, nz, n] -> [ntheta, slices held, n] (complex64)."""
@@ -212,6 +222,9 @@ class ShardedSolver(Solver):
 
     def _theta_to_z(self, x):
         return self.comm.theta_to_z(x)
+
+    def _sum_probe(self, g):
+        return self.comm.allreduce_tensor(g)
 
     def _z_to_theta(self, x):
         return self.comm.z_to_theta(x)

@@ -110,6 +110,7 @@ class Solver:
         else:
             self._ptycho_all = self.cl_ptycho
         # normalization coefficients, solver.py:43-46 (float32 like the reference)
+        self._red_local = K.Reducer(dev)   # for quantities every process holds whole (the probe)
         self.red = self._reducer(K.Reducer(dev))
         amax = self.red.maxabs(self.prb)
         self.coeftomo = float(np.float32(1 / np.float32(np.sqrt(ntheta * n / 2))))
@@ -121,6 +122,10 @@ class Solver:
     # One process holds everything, so they are identities here.
     def _reducer(self, red):
         return red
+
+    def _sum_probe(self, g):
+        """Sum of per-process probe gradients (one process: itself)."""
+        return g
 
     def _theta_to_z(self, x):
         """[angles held, nz, n] -> [ntheta, slices held, n]."""
@@ -347,6 +352,72 @@ class Solver:
             print("possible phase wrap, max computed angle", red.maxangle(psi))
         return psi
 
+    # ---- probe retrieval (no counterpart in the reference) -----------------
+    def set_probe(self, prb):
+        """Use the probe prb [Nprb, Nprb] in every ptycho operator from now on
+        (coefptycho and coefdata keep the values of the first probe)."""
+        self.prb = _dev_tensor(prb, torch.complex64, self.device)
+        for k, op in enumerate(self._ptycho):
+            op.setobj(self.scan[:, k * self.ptheta:(k + 1) * self.ptheta].contiguous(), self.prb)
+        if self._ptycho_all is not self.cl_ptycho:
+            self._ptycho_all.setobj(self.scan, self.prb)
+
+    def cg_probe(self, data, psi, prb, piter, model):
+        """Dai-Yuan CG on the probe with psi fixed: minimises the ptycho data
+        term of solver.py:208-214 over the probe, with the line search of
+        cg_ptycho.  data [angles held, Nscan, det, det] raw counts, psi
+        [angles held, Nz, N]; returns the new probe [Nprb, Nprb]."""
+        data = self._as_data(data)
+        red, loc = self.red, self._red_local
+        mdl = _MODELS[model]
+        p = _dev_tensor(prb, torch.complex64, self.device).clone()
+        chunks = [(self._ids(k), op) for k, op in enumerate(self._ptycho)]
+        frames = [self.ptheta, self.nscan, self.ndety, self.ndetx]
+
+        def fwd(q, ids, op):
+            out = self._empty(frames)
+            op.fwd_probe(out, psi[ids].contiguous(), q, scale=self.coefptycho)
+            return out
+
+        gamma = 2
+        grad0 = d = None
+        for i in range(piter):
+            fp = [fwd(p, ids, op) for ids, op in chunks]
+            grad = torch.zeros_like(p)
+            gk = torch.empty_like(p)
+            for (ids, op), f in zip(chunks, fp):
+                op.adj_probe_resid(gk, psi[ids].contiguous(), f, data[ids], self.coefdata, mdl, scale=self.coefptycho)
+                K.lincomb(grad, [(1.0, grad), (1.0, gk)])
+            grad = self._sum_probe(grad)
+            if i == 0:
+                d = K.lincomb(torch.empty_like(grad), [(-1.0, grad)])
+            else:
+                den = loc.dot(d, grad) - loc.dot(d, grad0)
+                beta = loc.norm2(grad) / den if den != 0 else 0.0
+                K.lincomb(d, [(-1.0, grad), (beta, d)])
+            grad0 = grad
+            fd = [fwd(d, ids, op) for ids, op in chunks]
+            npass = 0
+            while True:
+                J = (2, 8, 16)[min(npass, 2)]
+                npass += 1
+                gs = [gamma * 0.5 ** j for j in range(J)]
+                vals = np.zeros(J)
+                for (ids, _), f, fdk in zip(chunks, fp, fd):
+                    vals += np.asarray(red.ls_frames(f, fdk, data[ids], self.coefdata, mdl, gs))
+                chosen = next((g for g, dec in zip(gs, vals) if not (dec < 0 and g > 1e-12)), None)
+                if chosen is not None:
+                    gamma = 0 if chosen <= 1e-12 else chosen
+                    break
+                gamma = gs[-1] * 0.5
+            if self.trace is not None:
+                self.trace.append(("probe", gamma))
+            K.lincomb(p, [(1.0, p), (gamma, d)])
+            del fp, fd
+            if gamma == 0:
+                break
+        return p
+
     def cg_ptycho_batch(self, data, init, h, lamd, rho, piter, model):
         data = self._as_data(data)
         if self.ptheta == self.ntheta_held:
@@ -414,6 +485,7 @@ class Solver:
         state = {"m": int(m), "rho": float(rho), "tau": float(tau),
                  "held": (self.theta_range, self.z_range, self.ntheta, self.nz, self.n)}
         state.update({k: arrays[k].detach().cpu() for k in self._STATE})
+        state["prb"] = self.prb.detach().cpu()
         tmp = path + ".tmp"
         torch.save(state, tmp)
         os.replace(tmp, path)
@@ -430,11 +502,13 @@ class Solver:
 
     # ---- ADMM, solver.py:308-336 ------------------------------------------
     def admm(self, data, h, e, psi, phi, lamd, mu, u, alpha, piter, titer, niter, model, verbose=True,
-             history=None, checkpoint=None, checkpoint_every=1, resume=False):
+             history=None, checkpoint=None, checkpoint_every=1, resume=False, probe_iter=0):
         """ADMM as solver.py:308-336.  With ``checkpoint`` (a file path) the state
         is saved every ``checkpoint_every`` iterations and after the last one;
         with ``resume`` a run continues from that file (iteration m + 1 of the
-        same schedule) instead of from the arrays passed in."""
+        same schedule) instead of from the arrays passed in.  With ``probe_iter``
+        > 0 the probe is retrieved too: after each ptycho subproblem, that many
+        cg_probe iterations update it (``self.prb`` holds the result)."""
         data = self._as_data(data)
         rho, tau = 0.5, 0.5
         m0 = 0
@@ -442,9 +516,13 @@ class Solver:
             st = self.load_state(checkpoint)
             m0, rho, tau = st["m"] + 1, st["rho"], st["tau"]
             u, psi, h, e, phi, lamd, mu = (st[k] for k in self._STATE)
+            if "prb" in st and not torch.equal(st["prb"], self.prb.cpu()):
+                self.set_probe(st["prb"])
         for m in range(m0, niter):
             h0, e0 = h, e
             psi = self.cg_ptycho_batch(data, psi, h, lamd, rho, piter + (m < 2) * 32, model)
+            if probe_iter > 0:
+                self.set_probe(self.cg_probe(data, psi, self.prb, probe_iter, model))
             xi0, xi1, Kt, pshift = self.takexi(psi, phi, lamd, mu, rho, tau)
             u, Ru = self._cg_tomo(self._theta_to_z(xi0), xi1, self._theta_to_z(Kt), u, rho, tau, titer)
             phi = self.solve_reg(u, mu, tau, alpha)

@@ -60,6 +60,11 @@ def _worker(rank, world, port, ntheta, nz, n, errq):
         assert abs(tot - float(A.abs().double().pow(2).sum())) <= 1e-12 * tot
         mx, = comm.allreduce([float(A[th0:th1].abs().max())], op="max")
         assert mx == float(A.abs().max())
+        # tensor sum (probe gradients)
+        pr = _crand(torch.Generator().manual_seed(rank), (5, 5))
+        tot_t = comm.allreduce_tensor(pr.clone())
+        want = sum(_crand(torch.Generator().manual_seed(r), (5, 5)) for r in range(world))
+        assert torch.allclose(tot_t, want, rtol=1e-6, atol=1e-6)
         # gather
         assert torch.equal(comm.gather(A[th0:th1].contiguous(), 0, comm.theta_ranges), A)
         assert torch.equal(comm.gather(U[:, z0:z1].contiguous(), 1, comm.z_ranges), U)
