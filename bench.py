@@ -492,6 +492,11 @@ ADMM_SMALL = dict(n=128, nz=128, ntheta=128, nprb=64, det=64, nside=7, step=10.0
                   piter=4, titer=4, alpha=1e-3, voxel=1e-6, energy=5.0)
 
 
+def synthetic_phantom(c, seed=0):
+    from ptychotomo_b200 import synthetic
+    return synthetic.phantom(c["n"], c["nz"], seed=seed + 2)
+
+
 def _admm_problem(c, torch, dev, seed=0):
     """Solver, device counts and the true object for an ADMM config."""
     from ptychotomo_b200 import Solver, synthetic
@@ -598,13 +603,21 @@ def run_admm(args, local):
     t0 = time.perf_counter()
     _admm_run(slv, data, big, torch, dev, 4, history=hist)
     it_ms = [1e3 * (b["t"] - a) for a, b in zip([t0] + [h["t"] for h in hist[:-1]], hist)]
+    # probe retrieval at the same size: 4 CG iterations on the probe for the current psi
+    psi_b = slv.exptomo(slv.fwd_tomo_batch(torch.from_numpy(synthetic_phantom(big)).to(dev)))
+    torch.cuda.synchronize()
+    tp = time.perf_counter()
+    slv.cg_probe(data, psi_b, slv.prb, 4, "poisson")
+    torch.cuda.synchronize()
+    probe_ms = 1e3 * (time.perf_counter() - tp)
     line = {"metric": "plain Poisson ADMM wall time, 128^3 (4 ADMM x 4 CG iterations)", "value": round(wall, 3),
             "unit": "s", "n_gpus": 1, "higher_is_better": False, "dtype": "c64 (fp32 complex), FP64 reductions",
             "data": "synthetic", "config": {"workload": "plain ADMM: " + json.dumps(c)},
             "recon_rel_err_vs_phantom": round(err, 4),
             "iteration_ms_256cubed": {"workload": "384 angles, 13x13 scans, 128^2 probe/detector; iterations 0-1 "
                                                   "run 36 ptycho CG iterations, 2-3 run 4",
-                                      "ms": [round(x, 1) for x in it_ms]}}
+                                      "ms": [round(x, 1) for x in it_ms]},
+            "probe_cg_4iter_ms_256cubed": round(probe_ms, 1)}
     if not args.no_cpu_baseline:
         est, sample = _admm_cpu_estimate(c, *cpu_inputs)
         line["cpu_baseline"] = {"value": round(est, 1), "unit": "s", "cores": 1, "kind": "port", "sample": sample}
@@ -627,12 +640,17 @@ def run_cg_kernels(args, local):
     data = (ops.frames.abs() ** 2 * (1 + 0.1 * torch.rand(ops.frames.shape, device=dev, generator=g))).float()
     fd = 0.1 * ops.frames.roll(1, dims=-1)
     red = K.Reducer(dev)
+    P = c["nprb"]
+    gprb = torch.empty((P, P), dtype=torch.complex64, device=dev)
+    prb2 = torch.randn((P, P), dtype=torch.complex64, device=dev, generator=g)
     cases = {"adj_resid_poisson": lambda: p.adj_resid(ops.psi_out, ops.frames, data, 1.0, 0),
              "adj_resid_gaussian": lambda: p.adj_resid(ops.psi_out, ops.frames, data, 1.0, 1),
              "ptycho_adj": lambda: p.adj(ops.psi_out, ops.frames),
              "ls_frames_J2": lambda: red.ls_frames(ops.frames, fd, data, 1.0, 0, [1.0, 0.5]),
              "ls_frames_J8": lambda: red.ls_frames(ops.frames, fd, data, 1.0, 0, [0.5 ** j for j in range(8)]),
-             "ls_frames_J16": lambda: red.ls_frames(ops.frames, fd, data, 1.0, 0, [0.5 ** j for j in range(16)])}
+             "ls_frames_J16": lambda: red.ls_frames(ops.frames, fd, data, 1.0, 0, [0.5 ** j for j in range(16)]),
+             "adj_probe_resid_poisson": lambda: p.adj_probe_resid(gprb, ops.psi, ops.frames, data, 1.0, 0),
+             "fwd_probe": lambda: p.fwd_probe(fd, ops.psi, prb2)}
     out = {}
     for name, fn in cases.items():
         for _ in range(args.warmup):
@@ -647,7 +665,8 @@ def run_cg_kernels(args, local):
         out[name] = round(e0.elapsed_time(e1) / args.steps, 3)
     S = c["ntheta"] * c["nside"] ** 2
     frame = 8 * S * c["det"] ** 2
-    return {"metric": "ptycho CG frame kernels, ms per call", "unit": "ms", "n_gpus": 1, "steps": args.steps,
+    return {"metric": "ptycho CG frame kernels (and the probe-retrieval ones), ms per call", "unit": "ms",
+            "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": False, "data": "synthetic",
             "config": config_dict(c), "ms": out,
             "bytes_per_call": {"adj_resid": frame + frame // 2, "ls_frames": 2 * frame + frame // 2}}

@@ -41,22 +41,24 @@ def _data(slv, obj):
     return torch.poisson(d * 1e3, generator=g) / 1e3
 
 
-def _admm(slv, data, niter, th, zs):
+def _admm(slv, data, niter, th, zs, probe_iter=0):
     c = dict(dtype=torch.complex64, device="cuda")
     psi = torch.ones((th, NZ, N), **c)
     z3 = lambda: torch.zeros((3, zs, N, N), **c)  # noqa: E731
     hist = []
     u, psi = slv.admm(data, psi.clone(), z3(), psi, z3(), torch.zeros_like(psi), z3(),
-                      torch.zeros((zs, N, N), **c), 1e-3, 4, 4, niter, "poisson", verbose=False, history=hist)
+                      torch.zeros((zs, N, N), **c), 1e-3, 4, 4, niter, "poisson", verbose=False, history=hist,
+                      probe_iter=probe_iter)
     return u, psi, [(h["rho"], h["tau"]) for h in hist]
 
 
-def _reference(niter):
+def _reference(niter, probe_iter=0):
     from ptychotomo_b200 import Solver
     theta, prb, scan, obj = _problem()
     slv = Solver(prb, scan, theta, [NPRB, NPRB], 1e-6, 5.0, NTHETA, NZ, N, NTHETA, NZ)
     data = _data(slv, obj)
-    return (data,) + _admm(slv, data, niter, NTHETA, NZ)
+    out = (data,) + _admm(slv, data, niter, NTHETA, NZ, probe_iter)
+    return out + (slv.prb.cpu().numpy(),)
 
 
 def _free_port():
@@ -65,7 +67,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, niter, outdir, data_path):
+def _worker(rank, world, port, niter, outdir, data_path, probe_iter):
     import datetime
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -77,12 +79,13 @@ def _worker(rank, world, port, niter, outdir, data_path):
     comm = ShardComm(NTHETA, NZ)
     slv = ShardedSolver(prb, scan, theta, [NPRB, NPRB], 1e-6, 5.0, NTHETA, NZ, N, comm)
     data = slv.theta_shard(torch.from_numpy(np.load(data_path)).cuda()).contiguous()
-    u, psi, hist = _admm(slv, data, niter, slv.ntheta_held, slv.nz_held)
+    u, psi, hist = _admm(slv, data, niter, slv.ntheta_held, slv.nz_held, probe_iter)
     u_all, psi_all = slv.gather_z(u), slv.gather_theta(psi)
     if rank == 0:
         np.save(os.path.join(outdir, "u.npy"), u_all.cpu().numpy())
         np.save(os.path.join(outdir, "psi.npy"), psi_all.cpu().numpy())
         np.save(os.path.join(outdir, "hist.npy"), np.array(hist))
+        np.save(os.path.join(outdir, "prb.npy"), slv.prb.cpu().numpy())
     dist.barrier()
     dist.destroy_process_group()
 
@@ -96,7 +99,7 @@ def test_sharded_world1_is_the_solver_bitwise(backend):
     import datetime
     import torch.distributed as dist
     from ptychotomo_b200.sharded import ShardComm, ShardedSolver
-    data, u_ref, psi_ref, hist_ref = _reference(2)
+    data, u_ref, psi_ref, hist_ref, _ = _reference(2)
     store = dist.HashStore()
     kw = {"device_id": torch.device("cuda", 0)} if backend == "nccl" else {}
     dist.init_process_group(backend, store=store, rank=0, world_size=1, timeout=datetime.timedelta(seconds=60), **kw)
@@ -110,15 +113,18 @@ def test_sharded_world1_is_the_solver_bitwise(backend):
     assert torch.equal(u, u_ref) and torch.equal(psi, psi_ref)
 
 
-def test_sharded_two_ranks_on_one_gpu_match_the_solver(tmp_path):
+@pytest.mark.parametrize("probe_iter", [0, 2])
+def test_sharded_two_ranks_on_one_gpu_match_the_solver(tmp_path, probe_iter):
+    """probe_iter = 2 also retrieves the probe: its gradient is summed over the ranks."""
     import torch.multiprocessing as mp
     niter = 3
-    data, u_ref, psi_ref, hist_ref = _reference(niter)
+    data, u_ref, psi_ref, hist_ref, prb_ref = _reference(niter, probe_iter)
     data_path = str(tmp_path / "data.npy")
     np.save(data_path, data.cpu().numpy())
     ctx = mp.get_context("spawn")
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, niter, str(tmp_path), data_path)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, niter, str(tmp_path), data_path, probe_iter))
+             for r in range(2)]
     for p in procs:
         p.start()
     for p in procs:
@@ -132,3 +138,4 @@ def test_sharded_two_ranks_on_one_gpu_match_the_solver(tmp_path):
     assert hist == hist_ref
     assert _rel(np.load(tmp_path / "u.npy"), u_ref.cpu().numpy()) < 1e-4
     assert _rel(np.load(tmp_path / "psi.npy"), psi_ref.cpu().numpy()) < 1e-4
+    assert _rel(np.load(tmp_path / "prb.npy"), prb_ref) < 1e-4
