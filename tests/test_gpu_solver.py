@@ -122,7 +122,8 @@ def test_cg_ptycho_batch(problem, model):
     assert rel(pg, po) < 1e-3
 
 
-def test_admm_matches_oracle(problem):
+@pytest.mark.parametrize("model", ["poisson", "gaussian"])
+def test_admm_matches_oracle(problem, model):
     """Whole ADMM against the oracle.
 
     Every sub-step matches the oracle to 1e-5 .. 1e-3 (tests above), and the
@@ -142,10 +143,10 @@ def test_admm_matches_oracle(problem):
                     np.zeros((nz, n, n), np.complex64))
     h, e, psi, phi, lamd, mu, u = init()
     hist_g, hist_o = [], []
-    ug, psig = gs.admm(T(data), T(h), T(e), T(psi), T(phi), T(lamd), T(mu), T(u), 1e-9, 2, 2, 3, "poisson",
+    ug, psig = gs.admm(T(data), T(h), T(e), T(psi), T(phi), T(lamd), T(mu), T(u), 1e-9, 2, 2, 3, model,
                        verbose=False, history=hist_g)
     h, e, psi, phi, lamd, mu, u = init()
-    uo, psio = os_.admm(data, h, e, psi, phi, lamd, mu, u, 1e-9, 2, 2, 3, "poisson", history=hist_o)
+    uo, psio = os_.admm(data, h, e, psi, phi, lamd, mu, u, 1e-9, 2, 2, 3, model, history=hist_o)
     assert [x["rho"] for x in hist_g] == [x["rho"] for x in hist_o]
     assert [x["tau"] for x in hist_g] == [x["tau"] for x in hist_o]
     assert rel(psig, psio) < 1e-3
