@@ -19,6 +19,7 @@ Pass-model algorithmic bytes per call (complex64 = 8 B):
     python bench.py --admm        # ADMM wall time (128^3 run, 256^3 iterations)
     python bench.py --cg-kernels  # the ptycho CG's frame kernels at the operator workload
     python bench.py --precision   # operator errors vs direct sums, reconstruction errors
+    python bench.py --uneven      # uneven scans: one launch for all angles vs one per angle
 
 ``--impl reference`` times the reference's operators: by default the CPU
 restatement of the reference (oracle/, all host cores, a bounded sample of
@@ -774,6 +775,53 @@ def run_precision(args, local):
             "errors": out}
 
 
+def run_uneven(args, local):
+    """Uneven scans, batched against a per-angle loop: 256^3, 96 angles (a
+    sample of a 720-angle scan), per-angle scan counts drawn from [100, 400]
+    on a jittered spiral (padded with the -1 sentinel), 128^2 probe and
+    detector.  Times 4 ptycho CG iterations with all angles in one operator
+    launch (ptheta = ntheta) and with one launch per angle (ptheta = 1, the
+    reference's chunk loop at its finest)."""
+    import torch
+    from ptychotomo_b200 import Solver, synthetic
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n = nz = 256
+    nt, P = 96, 128
+    rng = np.random.default_rng(11)
+    counts = rng.integers(100, 401, nt)
+    scan = synthetic.jittered_spiral_scan(nt, n, nz, P, counts, jitter=3.0, seed=12)
+    theta = synthetic.angles(nt)
+    prb = synthetic.probe(P, seed=1)
+    obj = synthetic.phantom(n, nz, seed=2)
+    out = {}
+    data = None
+    for label, ptheta in (("batched", nt), ("per_angle", 1)):
+        slv = Solver(prb, scan, theta, [P, P], 1e-6, 5.0, nt, nz, n, ptheta, nz, device=dev)
+        if data is None:
+            inten = slv.fwd_ptycho_batch(slv.exptomo(slv.fwd_tomo_batch(torch.from_numpy(obj).to(dev))))
+            scale = 1e3 / float(inten.mean())
+            g = torch.Generator(device=dev).manual_seed(13)
+            data = torch.poisson(inten * scale, generator=g) / scale
+            del inten
+        psi = torch.ones((nt, nz, n), dtype=torch.complex64, device=dev)
+        slv.cg_ptycho_batch(data, psi, psi.clone(), torch.zeros_like(psi), 0.5, 1, "poisson")   # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        slv.cg_ptycho_batch(data, psi, psi.clone(), torch.zeros_like(psi), 0.5, 4, "poisson")
+        torch.cuda.synchronize()
+        out[label] = round(1e3 * (time.perf_counter() - t0) / 4, 2)
+        del slv
+        torch.cuda.empty_cache()
+    frames = int(counts.sum())
+    return {"metric": "ptycho CG ms per iteration, uneven scans: one launch for all angles vs one per angle",
+            "unit": "ms", "n_gpus": 1, "higher_is_better": False, "data": "synthetic",
+            "config": {"workload": "256^3, %d angles, scans per angle in [100, 400] (%d frames, padded to %d), "
+                                   "jittered spiral, 128^2 probe/detector, Poisson 1e3 photons" % (
+                                       nt, frames, nt * int(counts.max()))},
+            "ms_per_cg_iteration": out, "speedup": round(out["per_angle"] / out["batched"], 2)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -788,6 +836,7 @@ def main():
     ap.add_argument("--admm", action="store_true", help="ADMM wall time instead of operator throughput")
     ap.add_argument("--cg-kernels", action="store_true", help="device time of the ptycho CG's frame kernels")
     ap.add_argument("--precision", action="store_true", help="operator and reconstruction errors")
+    ap.add_argument("--uneven", action="store_true", help="uneven scans: batched vs per-angle launches")
     args = ap.parse_args()
     if args.ntheta:
         CFG["ntheta"] = args.ntheta
@@ -796,9 +845,10 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
-    if args.admm or args.cg_kernels or args.precision:
+    if args.admm or args.cg_kernels or args.precision or args.uneven:
         if rank == 0:
-            fn = run_admm if args.admm else run_cg_kernels if args.cg_kernels else run_precision
+            fn = (run_admm if args.admm else run_cg_kernels if args.cg_kernels else
+                  run_precision if args.precision else run_uneven)
             print(json.dumps(fn(args, local)), flush=True)
         return 0
     if args.impl == "reference":
