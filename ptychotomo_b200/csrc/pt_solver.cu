@@ -177,7 +177,8 @@ __device__ __forceinline__ void ls_pixel(double (&acc)[JB], const float (&gj)[JB
             const float b2 = a2 + delta;
             double dec;
             if (tiny || !(b2 >= 1e-30f)) {
-                dec = ls_decrease_f64(x, y, g, D, MODEL);
+                // d = 0 (a skipped scan's zero frame, say): no change for any step
+                dec = d2 == 0.f ? 0.0 : ls_decrease_f64(x, y, g, D, MODEL);
             } else if (MODEL == 0) {
                 dec = (double)(D * log1pf(delta * ia2) - delta);
             } else {
