@@ -402,6 +402,53 @@ __device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, 
     }
 }
 
+// Two independent lines through line_dft128 side by side: one twiddle load
+// and one pair of warp barriers serve both, and the two instruction streams
+// interleave.  sa and sb are two 1 KB exchange slots of the group.  Results
+// are bit-identical to two line_dft128 calls.
+template <int DIR>
+__device__ __forceinline__ void line_dft128x2(float2 (&a)[16], float2 (&b)[16], int t, float4 *sa, float4 *sb,
+                                              const float2 *tws)
+{
+    ptfft::Dft<16, DIR>::run(a);
+    ptfft::Dft<16, DIR>::run(b);
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) {
+        float2 w = tws[t * k1];
+        if (DIR > 0) w.y = -w.y;
+        a[k1] = cmul(a[k1], w);
+        b[k1] = cmul(b[k1], w);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        sa[t * 8 + ((q + t) & 7)] = make_float4(a[2 * q].x, a[2 * q].y, a[2 * q + 1].x, a[2 * q + 1].y);
+        sb[t * 8 + ((q + t) & 7)] = make_float4(b[2 * q].x, b[2 * q].y, b[2 * q + 1].x, b[2 * q + 1].y);
+    }
+    __syncwarp();
+    float2 a0[8], a1[8], b0[8], b1[8];
+#pragma unroll
+    for (int n2 = 0; n2 < 8; ++n2) {
+        const float4 wa = sa[n2 * 8 + ((t + n2) & 7)];
+        const float4 wb = sb[n2 * 8 + ((t + n2) & 7)];
+        a0[n2] = make_float2(wa.x, wa.y);
+        a1[n2] = make_float2(wa.z, wa.w);
+        b0[n2] = make_float2(wb.x, wb.y);
+        b1[n2] = make_float2(wb.z, wb.w);
+    }
+    ptfft::Dft<8, DIR>::run(a0);
+    ptfft::Dft<8, DIR>::run(a1);
+    ptfft::Dft<8, DIR>::run(b0);
+    ptfft::Dft<8, DIR>::run(b1);
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) {
+        a[k2] = a0[k2];
+        a[8 + k2] = a1[k2];
+        b[k2] = b0[k2];
+        b[8 + k2] = b1[k2];
+    }
+}
+
 template <bool FULL>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_fwd128(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
@@ -413,7 +460,8 @@ __global__ void __launch_bounds__(512, 1)
     float2 *tws = reinterpret_cast<float2 *>(sm4 + 64 * 128);
     for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
-    float4 *sc = fr + grp * 64;
+    // exchange slots: the whole frame buffer is idle during both passes
+    float4 *sa = fr + grp * 64, *sb = fr + 64 * 64 + grp * 64;
     const int off = FULL ? 0 : (128 - P) / 2;
     __syncthreads();
     for (int fid = blockIdx.x; fid < nframes; fid += gridDim.x) {
@@ -441,8 +489,8 @@ __global__ void __launch_bounds__(512, 1)
                     v[c][m] = val;
                 }
             }
-            line_dft128<-1>(v[c], t, sc, tws);
         }
+        line_dft128x2<-1>(v[0], v[1], t, sa, sb, tws);
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -462,9 +510,9 @@ __global__ void __launch_bounds__(512, 1)
         }
         __syncthreads();
         const float2 ph = scale * phase[fid];
+        line_dft128x2<-1>(v[0], v[1], t, sa, sb, tws);
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            line_dft128<-1>(v[c], t, sc, tws);
             float4 *row = reinterpret_cast<float4 *>(out + (2 * grp + c) * 128);
 #pragma unroll
             for (int k2 = 0; k2 < 8; ++k2) {
@@ -494,6 +542,20 @@ __device__ __forceinline__ void prefetch_half_frame(float4 *dst, const float2 *i
         const int id = threadIdx.x + 512 * i;
         const int row = id >> 6, c16 = id & 63;
         cp_async16(dst + row * 64 + (c16 ^ ((row & 1) << 2)), in + row * 128 + 2 * c16);
+    }
+    cp_async_commit();
+}
+
+// Row grp of frame `in` -> the group's own 1 KB row of the prefetch buffer,
+// in the layout of prefetch_half_frame.  Only the group's 8 threads touch
+// that row, so a warp barrier orders it against the group's exchange slot
+// there.
+__device__ __forceinline__ void prefetch_group_row(float4 *pre, const float2 *in, int grp, int t)
+{
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int c16 = t + 8 * j;
+        cp_async16(pre + grp * 64 + (c16 ^ ((grp & 1) << 2)), in + grp * 128 + 2 * c16);
     }
     cp_async_commit();
 }
@@ -536,12 +598,22 @@ __global__ void __launch_bounds__(512, 1)
     for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
     for (int e = threadIdx.x; e < nz * n; e += 512) slab[e] = czero();
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
-    float4 *sc = fr + grp * 64;
+    // X2: both lines of a group through line_dft128x2, the second exchange
+    // slot being the group's own prefetch row (measured faster with the
+    // Poisson residual, slower for the plain adjoint)
+    constexpr bool X2 = RESID == 1;
+    float4 *sa = fr + grp * 64, *sb = pre + grp * 64;
+    auto prefetch_frame = [&](const float2 *src) {
+        if constexpr (X2)
+            prefetch_group_row(pre, src, grp, t);
+        else
+            prefetch_half_frame(pre, src);
+    };
     const int off = FULL ? 0 : (128 - P) / 2;
     const float2 *gth = g + (size_t)th * nscan * 128 * 128;
     const float *dth = RESID ? data + (size_t)th * nscan * 128 * 128 : nullptr;
     if (part < nscan) {
-        prefetch_half_frame(pre, gth + (size_t)part * 128 * 128);
+        prefetch_frame(gth + (size_t)part * 128 * 128);
         if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)part * 128 * 128);
     }
     for (int s = part; s < nscan; s += parts) {
@@ -555,7 +627,7 @@ __global__ void __launch_bounds__(512, 1)
         if (stx < 0 || sty < 0) {  // skipped scan: keep the prefetch chain going
             __syncthreads();
             if (more) {
-                prefetch_half_frame(pre, in_next);
+                prefetch_frame(in_next);
                 if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
             }
             continue;
@@ -574,14 +646,17 @@ __global__ void __launch_bounds__(512, 1)
             if constexpr (RESID != 0) D = staged_count(cnt, grp, ky) * dscale;
             v[0][m] = scale * cmulc(ph, resid_of<RESID>(x, D));
         }
-        line_dft128<+1>(v[0], t, sc, tws);
+        if constexpr (!X2) line_dft128<+1>(v[0], t, sa, tws);
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             float D = 0.f;
             if constexpr (RESID != 0) D = staged_count(cnt, grp + 64, t + 8 * m) * dscale;
             v[1][m] = scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
         }
-        line_dft128<+1>(v[1], t, sc, tws);
+        if constexpr (X2)
+            line_dft128x2<+1>(v[0], v[1], t, sa, sb, tws);
+        else
+            line_dft128<+1>(v[1], t, sa, tws);
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -600,13 +675,17 @@ __global__ void __launch_bounds__(512, 1)
             v[1][m] = make_float2(q.z, q.w);
         }
         __syncthreads();
-        if (more) {
-            prefetch_half_frame(pre, in_next);
-            if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
+        if (more && !X2) prefetch_half_frame(pre, in_next);
+        if constexpr (RESID != 0)
+            if (more) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
+        if constexpr (X2) {
+            line_dft128x2<+1>(v[0], v[1], t, sa, sb, tws);
+            __syncwarp();  // the group's reads of its slot sb are done before the next frame lands there
+            if (more) prefetch_group_row(pre, in_next, grp, t);
         }
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            line_dft128<+1>(v[c], t, sc, tws);
+            if constexpr (!X2) line_dft128<+1>(v[c], t, sa, tws);
             const int py = 2 * grp + c - off;
             if (!FULL && (py < 0 || py >= P)) continue;
             float2 *row = slab + (size_t)(sty + py) * n + stx;
@@ -636,10 +715,12 @@ __global__ void __launch_bounds__(512, 1)
 // The same transform written for both adjoints.  PROBE: the adjoint with
 // respect to the probe (as k_ptycho_adj_probe): grid (blocks, 1), block b
 // walks frames b, b + gridDim.x, ... and accumulates conj(psi patch) x frame
-// into its P x P partial dst[b].  Otherwise as k_ptycho_adj128; the compiler
-// schedules this formulation better for the Gaussian residual (9.4 against
-// 11.0 ms at 256^3) and worse for the plain and Poisson adjoints, so each
-// launch takes the faster one.
+// into its P x P partial dst[b].  Otherwise as k_ptycho_adj128 with both
+// lines of a group through line_dft128x2.  At 256^3 this formulation takes
+// 7.7 ms for the Gaussian residual (11.0 for k_ptycho_adj128's) and 6.4 ms
+// for the Poisson probe adjoint (12.3 for k_ptycho_adj_probe), but 5.76 and
+// 8.16 ms for the plain and Poisson object adjoints (5.75 and 7.44 for
+// k_ptycho_adj128's), so each launch takes the faster one.
 template <bool FULL, int RESID, bool PROBE>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128v(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
@@ -658,13 +739,14 @@ __global__ void __launch_bounds__(512, 1)
     for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
     for (int e = threadIdx.x; e < (PROBE ? P * P : nz * n); e += 512) slab[e] = czero();
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
-    float4 *sc = fr + grp * 64;
+    // exchange slots: sa in the lower half, sb = the group's own prefetch row
+    float4 *sa = fr + grp * 64, *sb = pre + grp * 64;
     const int off = FULL ? 0 : (128 - P) / 2;
     // frames k = part, part + parts, ... < count: fid = k (probe) or angle th0's scan k
     const int count = PROBE ? nframes : nscan;
     const size_t fid0 = PROBE ? (size_t)part : (size_t)th0 * nscan + part;
     if (part < count) {
-        prefetch_half_frame(pre, g + fid0 * 128 * 128);
+        prefetch_group_row(pre, g + fid0 * 128 * 128, grp, t);
         if constexpr (RESID != 0) prefetch_counts(cnt, data + fid0 * 128 * 128);
     }
     for (int s = part; s < count; s += parts) {
@@ -679,7 +761,7 @@ __global__ void __launch_bounds__(512, 1)
         if (stx < 0 || sty < 0) {  // skipped scan: keep the prefetch chain going
             __syncthreads();
             if (more) {
-                prefetch_half_frame(pre, in_next);
+                prefetch_group_row(pre, in_next, grp, t);
                 if constexpr (RESID != 0) prefetch_counts(cnt, data + (size_t)(fid + parts) * 128 * 128);
             }
             continue;
@@ -698,14 +780,13 @@ __global__ void __launch_bounds__(512, 1)
             if constexpr (RESID != 0) D = staged_count(cnt, grp, ky) * dscale;
             v[0][m] = scale * cmulc(ph, resid_of<RESID>(x, D));
         }
-        line_dft128<+1>(v[0], t, sc, tws);
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             float D = 0.f;
             if constexpr (RESID != 0) D = staged_count(cnt, grp + 64, t + 8 * m) * dscale;
             v[1][m] = scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
         }
-        line_dft128<+1>(v[1], t, sc, tws);
+        line_dft128x2<+1>(v[0], v[1], t, sa, sb, tws);
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -724,13 +805,13 @@ __global__ void __launch_bounds__(512, 1)
             v[1][m] = make_float2(q.z, q.w);
         }
         __syncthreads();
-        if (more) {
-            prefetch_half_frame(pre, in_next);
-            if constexpr (RESID != 0) prefetch_counts(cnt, data + (size_t)(fid + parts) * 128 * 128);
-        }
+        if constexpr (RESID != 0)
+            if (more) prefetch_counts(cnt, data + (size_t)(fid + parts) * 128 * 128);
+        line_dft128x2<+1>(v[0], v[1], t, sa, sb, tws);
+        __syncwarp();  // the group's reads of its slot sb are done before the next frame lands there
+        if (more) prefetch_group_row(pre, in_next, grp, t);
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            line_dft128<+1>(v[c], t, sc, tws);
             const int py = 2 * grp + c - off;
             if (!FULL && (py < 0 || py >= P)) continue;
             // object: slab row += conj(c prbT) x; probe: partial row += conj(psi) x

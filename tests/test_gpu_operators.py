@@ -313,14 +313,15 @@ def test_operators_capture_in_a_cuda_graph():
             assert torch.equal(o, e)
 
 
-@pytest.mark.parametrize("det,nprb", [(32, 32), (128, 96)])
+@pytest.mark.parametrize("det,nprb", [(32, 32), (128, 96), (128, 128)])
 def test_ptycho_uneven_scan_counts(det, nprb):
     """Per-angle scan counts drawn from [lo, hi] on a jittered spiral, padded to the
     largest count with the -1 sentinel (kernels.cuh:256,280): every padded scan is
-    skipped by both transforms."""
+    skipped by both transforms.  The 128 x 128 probe case runs 24 angles, so the
+    adjoint's blocks walk runs of valid and skipped frames."""
     from ptychotomo_b200 import ptychofft, synthetic
-    rng = np.random.default_rng(det)
-    nt, n, nz = 4, 160, 150
+    rng = np.random.default_rng(det + nprb)
+    nt, n, nz = (24 if nprb == 128 else 4), 160, 150
     counts = rng.integers(5, 19, nt)
     scan = synthetic.jittered_spiral_scan(nt, n, nz, nprb, counts, jitter=3.0, seed=det)
     nscan = scan.shape[2]
