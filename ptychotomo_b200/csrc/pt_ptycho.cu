@@ -365,21 +365,30 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
 // column; slot (q, c) lives at q * 128 + (c ^ (q & 7)), so the 8 threads of a
 // group hit 8 distinct 4-bank groups both when writing (q varies) and when
 // reading (c varies).  The group exchange uses the same trick.
+// frame buffer 128 KB, then a 1 KB twiddle table
 constexpr int P128_SMEM = (64 * 128) * 16 + 128 * 8;
 // the fused-residual adjoint also stages the frame's 128 x 128 counts.  The
 // plain adjoint stays at P128_SMEM: the remaining ~125 KB of L1 keeps the
 // 128 KB probe table it rereads for every frame mostly resident (with 64 KB
 // more shared memory it ran at twice the time).
-constexpr int P128_SMEM_RESID = P128_SMEM + 128 * 128 * 4;
+// The fused-residual kernels keep a second 1 KB table, the row pass's
+// twiddles folded with the frame's scale x conj(phase) (see line_dft128).
+constexpr int P128_SMEM_RESID = P128_SMEM + 128 * 8 + 128 * 128 * 4;
 
-template <int DIR>
+
+// FOLD: the line still has to be multiplied by a per-frame factor f (the
+// scan's phase and the scale).  Since the transform is linear, f rides on the
+// twiddles: tws is then a per-frame table (fold_twiddles) already in the
+// transform's direction and multiplied by f, whose entry 0 is f itself, so
+// element 0 takes its product from the table as well.
+template <int DIR, bool FOLD = false>
 __device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, const float2 *tws)
 {
     ptfft::Dft<16, DIR>::run(v);
 #pragma unroll
-    for (int k1 = 1; k1 < 16; ++k1) {
+    for (int k1 = FOLD ? 0 : 1; k1 < 16; ++k1) {
         float2 w = tws[t * k1];
-        if (DIR > 0) w.y = -w.y;
+        if (DIR > 0 && !FOLD) w.y = -w.y;
         v[k1] = cmul(v[k1], w);
     }
     __syncwarp();
@@ -406,16 +415,16 @@ __device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, 
 // and one pair of warp barriers serve both, and the two instruction streams
 // interleave.  sa and sb are two 1 KB exchange slots of the group.  Results
 // are bit-identical to two line_dft128 calls.
-template <int DIR>
+template <int DIR, bool FOLD = false>
 __device__ __forceinline__ void line_dft128x2(float2 (&a)[16], float2 (&b)[16], int t, float4 *sa, float4 *sb,
                                               const float2 *tws)
 {
     ptfft::Dft<16, DIR>::run(a);
     ptfft::Dft<16, DIR>::run(b);
 #pragma unroll
-    for (int k1 = 1; k1 < 16; ++k1) {
+    for (int k1 = FOLD ? 0 : 1; k1 < 16; ++k1) {
         float2 w = tws[t * k1];
-        if (DIR > 0) w.y = -w.y;
+        if (DIR > 0 && !FOLD) w.y = -w.y;
         a[k1] = cmul(a[k1], w);
         b[k1] = cmul(b[k1], w);
     }
@@ -449,6 +458,20 @@ __device__ __forceinline__ void line_dft128x2(float2 (&a)[16], float2 (&b)[16], 
     }
 }
 
+// Per-frame folded twiddle table for line_dft128<DIR, true>: tw[i] in
+// direction DIR times f, entry 0 (a twiddle of 1) being f exactly.  Threads
+// 0..127 write one entry each.
+template <int DIR>
+__device__ __forceinline__ void fold_twiddles(float2 *twf, const float2 *__restrict__ tw, float2 f)
+{
+    const int i = threadIdx.x;
+    if (i < 128) {
+        float2 w = tw[i];
+        if (DIR > 0) w.y = -w.y;
+        twf[i] = i == 0 ? f : cmul(w, f);
+    }
+}
+
 template <bool FULL>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_fwd128(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
@@ -457,13 +480,13 @@ __global__ void __launch_bounds__(512, 1)
 {
     extern __shared__ float4 sm4[];
     float4 *fr = sm4;
-    float2 *tws = reinterpret_cast<float2 *>(sm4 + 64 * 128);
-    for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
+    // the shared table holds this frame's column twiddles x scale x phase
+    // (line_dft128's FOLD); the row pass reads the plain twiddles from global
+    float2 *twf = reinterpret_cast<float2 *>(sm4 + 64 * 128);
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
     // exchange slots: the whole frame buffer is idle during both passes
     float4 *sa = fr + grp * 64, *sb = fr + 64 * 64 + grp * 64;
     const int off = FULL ? 0 : (128 - P) / 2;
-    __syncthreads();
     for (int fid = blockIdx.x; fid < nframes; fid += gridDim.x) {
         const int th = fid / nscan;
         const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
@@ -490,7 +513,8 @@ __global__ void __launch_bounds__(512, 1)
                 }
             }
         }
-        line_dft128x2<-1>(v[0], v[1], t, sa, sb, tws);
+        line_dft128x2<-1>(v[0], v[1], t, sa, sb, tw);
+        fold_twiddles<-1>(twf, tw, scale * phase[fid]);  // read after the next block barrier
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -509,16 +533,13 @@ __global__ void __launch_bounds__(512, 1)
             v[1][m] = make_float2(q.z, q.w);
         }
         __syncthreads();
-        const float2 ph = scale * phase[fid];
-        line_dft128x2<-1>(v[0], v[1], t, sa, sb, tws);
+        line_dft128x2<-1, true>(v[0], v[1], t, sa, sb, twf);
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             float4 *row = reinterpret_cast<float4 *>(out + (2 * grp + c) * 128);
 #pragma unroll
-            for (int k2 = 0; k2 < 8; ++k2) {
-                const float2 a = cmul(v[c][k2], ph), b = cmul(v[c][8 + k2], ph);
-                row[t + 8 * k2] = make_float4(a.x, a.y, b.x, b.y);   // ky = 2t + 16 k2, +1
-            }
+            for (int k2 = 0; k2 < 8; ++k2)   // ky = 2t + 16 k2, +1
+                row[t + 8 * k2] = make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y);
         }
         __syncthreads();
     }
@@ -588,20 +609,25 @@ __global__ void __launch_bounds__(512, 1)
                     int P, float scale, const float2 *__restrict__ tw, const float *__restrict__ data,
                     float dscale)
 {
+    // X2: both lines of a group through line_dft128x2, the second exchange
+    // slot being the group's own prefetch row.  FOLD: the frame's scale x
+    // conj(phase) rides on the row-pass twiddles (line_dft128); the folded
+    // table is written for the next frame during the column pass, after the
+    // last read of the current one.  Both measured faster with the Poisson
+    // residual and slower for the plain adjoint (5.89 and 8.78 against
+    // 5.75 ms at 256^3).
+    constexpr bool X2 = RESID == 1, FOLD = RESID == 1;
     extern __shared__ float4 sm4[];
     float4 *fr = sm4;
     float4 *pre = sm4 + 64 * 64;  // upper 64 KB of the frame buffer
     float2 *tws = reinterpret_cast<float2 *>(sm4 + 64 * 128);
-    float *cnt = reinterpret_cast<float *>(sm4 + 64 * 128 + 64);  // RESID: this frame's counts
+    float2 *twf = tws + 128;  // RESID: the folded row-pass twiddles
+    float *cnt = reinterpret_cast<float *>(sm4 + 64 * 128 + 128);  // RESID: this frame's counts
     const int part = blockIdx.x, parts = gridDim.x, th = blockIdx.y;
     float2 *slab = dst + ((size_t)th * parts + part) * nz * n;
     for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
     for (int e = threadIdx.x; e < nz * n; e += 512) slab[e] = czero();
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
-    // X2: both lines of a group through line_dft128x2, the second exchange
-    // slot being the group's own prefetch row (measured faster with the
-    // Poisson residual, slower for the plain adjoint)
-    constexpr bool X2 = RESID == 1;
     float4 *sa = fr + grp * 64, *sb = pre + grp * 64;
     auto prefetch_frame = [&](const float2 *src) {
         if constexpr (X2)
@@ -609,10 +635,15 @@ __global__ void __launch_bounds__(512, 1)
         else
             prefetch_half_frame(pre, src);
     };
+    auto fold_for = [&](int f) {
+        const float2 p = phase[f];
+        fold_twiddles<+1>(twf, tw, make_float2(scale * p.x, -scale * p.y));
+    };
     const int off = FULL ? 0 : (128 - P) / 2;
     const float2 *gth = g + (size_t)th * nscan * 128 * 128;
     const float *dth = RESID ? data + (size_t)th * nscan * 128 * 128 : nullptr;
     if (part < nscan) {
+        if constexpr (FOLD) fold_for(th * nscan + part);
         prefetch_frame(gth + (size_t)part * 128 * 128);
         if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)part * 128 * 128);
     }
@@ -627,12 +658,13 @@ __global__ void __launch_bounds__(512, 1)
         if (stx < 0 || sty < 0) {  // skipped scan: keep the prefetch chain going
             __syncthreads();
             if (more) {
+                if constexpr (FOLD) fold_for(fid + parts);
                 prefetch_frame(in_next);
                 if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
             }
             continue;
         }
-        const float2 ph = phase[fid];
+        const float2 ph = FOLD ? make_float2(1.f, 0.f) : phase[fid];
         float2 v[2][16];
         // rows 64..127 from global first, so their latency hides behind row 0..63's work
 #pragma unroll
@@ -644,19 +676,19 @@ __global__ void __launch_bounds__(512, 1)
             const float2 x = (ky & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
             float D = 0.f;
             if constexpr (RESID != 0) D = staged_count(cnt, grp, ky) * dscale;
-            v[0][m] = scale * cmulc(ph, resid_of<RESID>(x, D));
+            v[0][m] = FOLD ? resid_of<RESID>(x, D) : scale * cmulc(ph, resid_of<RESID>(x, D));
         }
-        if constexpr (!X2) line_dft128<+1>(v[0], t, sa, tws);
+        if constexpr (!X2) line_dft128<+1, FOLD>(v[0], t, sa, FOLD ? twf : tws);
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             float D = 0.f;
             if constexpr (RESID != 0) D = staged_count(cnt, grp + 64, t + 8 * m) * dscale;
-            v[1][m] = scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
+            v[1][m] = FOLD ? resid_of<RESID>(v[1][m], D) : scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
         }
         if constexpr (X2)
-            line_dft128x2<+1>(v[0], v[1], t, sa, sb, tws);
+            line_dft128x2<+1, FOLD>(v[0], v[1], t, sa, sb, FOLD ? twf : tws);
         else
-            line_dft128<+1>(v[1], t, sa, tws);
+            line_dft128<+1, FOLD>(v[1], t, sa, FOLD ? twf : tws);
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -675,6 +707,8 @@ __global__ void __launch_bounds__(512, 1)
             v[1][m] = make_float2(q.z, q.w);
         }
         __syncthreads();
+        if constexpr (FOLD)
+            if (more) fold_for(fid + parts);
         if (more && !X2) prefetch_half_frame(pre, in_next);
         if constexpr (RESID != 0)
             if (more) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
@@ -717,7 +751,7 @@ __global__ void __launch_bounds__(512, 1)
 // walks frames b, b + gridDim.x, ... and accumulates conj(psi patch) x frame
 // into its P x P partial dst[b].  Otherwise as k_ptycho_adj128 with both
 // lines of a group through line_dft128x2.  At 256^3 this formulation takes
-// 7.7 ms for the Gaussian residual (11.0 for k_ptycho_adj128's) and 6.4 ms
+// 7.6 ms for the Gaussian residual (11.0 for k_ptycho_adj128's) and 6.4 ms
 // for the Poisson probe adjoint (12.3 for k_ptycho_adj_probe), but 5.76 and
 // 8.16 ms for the plain and Poisson object adjoints (5.75 and 7.44 for
 // k_ptycho_adj128's), so each launch takes the faster one.
@@ -732,7 +766,15 @@ __global__ void __launch_bounds__(512, 1)
     float4 *fr = sm4;
     float4 *pre = sm4 + 64 * 64;  // upper 64 KB of the frame buffer
     float2 *tws = reinterpret_cast<float2 *>(sm4 + 64 * 128);
-    float *cnt = reinterpret_cast<float *>(sm4 + 64 * 128 + 64);  // RESID: this frame's counts
+    // FOLD (object adjoint): the frame's scale x conj(phase) rides on the
+    // row-pass twiddles, as in k_ptycho_adj128
+    constexpr bool FOLD = !PROBE;
+    float2 *twf = tws + 128;
+    float *cnt = reinterpret_cast<float *>(sm4 + 64 * 128 + 128);  // RESID: this frame's counts
+    auto fold_for = [&](size_t f) {
+        const float2 p = phase[f];
+        fold_twiddles<+1>(twf, tw, make_float2(scale * p.x, -scale * p.y));
+    };
     const int part = blockIdx.x, parts = gridDim.x;
     const int th0 = blockIdx.y;   // the angle (object slabs)
     float2 *slab = PROBE ? dst + (size_t)part * P * P : dst + ((size_t)th0 * parts + part) * nz * n;
@@ -746,6 +788,7 @@ __global__ void __launch_bounds__(512, 1)
     const int count = PROBE ? nframes : nscan;
     const size_t fid0 = PROBE ? (size_t)part : (size_t)th0 * nscan + part;
     if (part < count) {
+        if constexpr (FOLD) fold_for(fid0);
         prefetch_group_row(pre, g + fid0 * 128 * 128, grp, t);
         if constexpr (RESID != 0) prefetch_counts(cnt, data + fid0 * 128 * 128);
     }
@@ -761,12 +804,13 @@ __global__ void __launch_bounds__(512, 1)
         if (stx < 0 || sty < 0) {  // skipped scan: keep the prefetch chain going
             __syncthreads();
             if (more) {
+                if constexpr (FOLD) fold_for((size_t)fid + parts);
                 prefetch_group_row(pre, in_next, grp, t);
                 if constexpr (RESID != 0) prefetch_counts(cnt, data + (size_t)(fid + parts) * 128 * 128);
             }
             continue;
         }
-        const float2 ph = phase[fid];
+        const float2 ph = FOLD ? make_float2(1.f, 0.f) : phase[fid];
         float2 v[2][16];
         // rows 64..127 from global first, so their latency hides behind row 0..63's work
 #pragma unroll
@@ -778,15 +822,15 @@ __global__ void __launch_bounds__(512, 1)
             const float2 x = (ky & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
             float D = 0.f;
             if constexpr (RESID != 0) D = staged_count(cnt, grp, ky) * dscale;
-            v[0][m] = scale * cmulc(ph, resid_of<RESID>(x, D));
+            v[0][m] = FOLD ? resid_of<RESID>(x, D) : scale * cmulc(ph, resid_of<RESID>(x, D));
         }
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             float D = 0.f;
             if constexpr (RESID != 0) D = staged_count(cnt, grp + 64, t + 8 * m) * dscale;
-            v[1][m] = scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
+            v[1][m] = FOLD ? resid_of<RESID>(v[1][m], D) : scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
         }
-        line_dft128x2<+1>(v[0], v[1], t, sa, sb, tws);
+        line_dft128x2<+1, FOLD>(v[0], v[1], t, sa, sb, FOLD ? twf : tws);
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -805,6 +849,8 @@ __global__ void __launch_bounds__(512, 1)
             v[1][m] = make_float2(q.z, q.w);
         }
         __syncthreads();
+        if constexpr (FOLD)
+            if (more) fold_for((size_t)fid + parts);
         if constexpr (RESID != 0)
             if (more) prefetch_counts(cnt, data + (size_t)(fid + parts) * 128 * 128);
         line_dft128x2<+1>(v[0], v[1], t, sa, sb, tws);
