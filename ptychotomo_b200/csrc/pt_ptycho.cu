@@ -599,6 +599,26 @@ __device__ __forceinline__ float staged_count(const float *cnt, int row, int col
     return cnt[row * 128 + ((col + 8 * (row & 3)) & 127)];
 }
 
+// row[px] += conj(mul[px]) x v for a thread's 16 pixels px = 2t + j + 16 k2
+// (v[8 j + k2]) with 16-byte accesses: row and mul 16-byte aligned at px = 0,
+// so pixels 2t + 16 k2 and the next share one.  All 8 row loads are issued
+// before any store.  Same arithmetic as the 8-byte form.
+__device__ __forceinline__ void rmw_row16(float2 *row, const float2 *__restrict__ mul, const float2 (&v)[16], int t)
+{
+    float4 *row4 = reinterpret_cast<float4 *>(row);
+    const float4 *mul4 = reinterpret_cast<const float4 *>(mul);
+    float4 cur[8];
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) cur[k2] = row4[t + 8 * k2];
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) {
+        const float4 w = __ldg(&mul4[t + 8 * k2]);
+        const float2 a = make_float2(cur[k2].x, cur[k2].y) + cmulc(make_float2(w.x, w.y), v[k2]);
+        const float2 b = make_float2(cur[k2].z, cur[k2].w) + cmulc(make_float2(w.z, w.w), v[8 + k2]);
+        row4[t + 8 * k2] = make_float4(a.x, a.y, b.x, b.y);
+    }
+}
+
 // grid (parts, ntheta): block (part, angle) owns slab dst[angle][part].
 // While the current frame finishes, the next frame's rows 0..63 are already
 // on their way into the idle half of the shared frame buffer.
@@ -640,6 +660,9 @@ __global__ void __launch_bounds__(512, 1)
         fold_twiddles<+1>(twf, tw, make_float2(scale * p.x, -scale * p.y));
     };
     const int off = FULL ? 0 : (128 - P) / 2;
+    // plain adjoint: slab rows of frames at an even column take 16-byte
+    // accesses (5.48 against 5.75 ms at 256^3; slower with the Poisson residual)
+    const bool vec = RESID == 0 && FULL && (n & 1) == 0 && ((uintptr_t)dst & 15) == 0;
     const float2 *gth = g + (size_t)th * nscan * 128 * 128;
     const float *dth = RESID ? data + (size_t)th * nscan * 128 * 128 : nullptr;
     if (part < nscan) {
@@ -723,6 +746,10 @@ __global__ void __launch_bounds__(512, 1)
             const int py = 2 * grp + c - off;
             if (!FULL && (py < 0 || py >= P)) continue;
             float2 *row = slab + (size_t)(sty + py) * n + stx;
+            if (vec && (stx & 1) == 0) {
+                rmw_row16(row, prbT + (size_t)py * 128, v[c], t);
+                continue;
+            }
             // all 16 slab values are loaded before any is stored back, so the
             // loads overlap instead of waiting on each other's stores
             float2 cur[16];
@@ -784,6 +811,10 @@ __global__ void __launch_bounds__(512, 1)
     // exchange slots: sa in the lower half, sb = the group's own prefetch row
     float4 *sa = fr + grp * 64, *sb = pre + grp * 64;
     const int off = FULL ? 0 : (128 - P) / 2;
+    // object adjoint: slab rows of frames at an even column take 16-byte
+    // accesses (7.36 against 7.58 ms for the Gaussian residual at 256^3; no
+    // steady gain for the probe adjoint)
+    const bool vec = !PROBE && FULL && (n & 1) == 0 && ((uintptr_t)dst & 15) == 0;
     // frames k = part, part + parts, ... < count: fid = k (probe) or angle th0's scan k
     const int count = PROBE ? nframes : nscan;
     const size_t fid0 = PROBE ? (size_t)part : (size_t)th0 * nscan + part;
@@ -863,6 +894,10 @@ __global__ void __launch_bounds__(512, 1)
             // object: slab row += conj(c prbT) x; probe: partial row += conj(psi) x
             float2 *row = PROBE ? slab + (size_t)py * P : slab + (size_t)(sty + py) * n + stx;
             const float2 *mul = PROBE ? psi + ((size_t)th * nz + sty + py) * n + stx : prbT + (size_t)py * P;
+            if (vec && (stx & 1) == 0) {
+                rmw_row16(row, mul, v[c], t);
+                continue;
+            }
             // all 16 slab values are loaded before any is stored back, so the
             // loads overlap instead of waiting on each other's stores
             float2 cur[16];

@@ -249,6 +249,27 @@ def test_ptycho_det128_misaligned_adjoint_input():
     assert rel(out.cpu().numpy(), orc.adj(g)) <= TOL
 
 
+@pytest.mark.parametrize("n,shift,parts", [(130, 0, "1"), (131, 0, None), (130, 1, "1")])
+def test_ptycho_det128_adjoint_row_alignment(n, shift, parts, monkeypatch):
+    """The det-128 adjoint adds a frame into its object rows with 16-byte
+    accesses when the frame starts at an even column of an even-width object
+    whose output is 16-byte aligned, and with 8-byte accesses otherwise.  Scans
+    at both column parities; an odd width; an output that is only 8-byte
+    aligned, written directly (one part per angle)."""
+    if parts:
+        monkeypatch.setenv("PT_PTYCHO_ADJ_PARTS", parts)
+    rng = np.random.default_rng(23 + n + shift)
+    op, orc, scan, _ = make_ptycho(2, 140, n, 6, 128, 128, rng)
+    cols = np.round(scan[0]).astype(int)[scan[0] >= 0]
+    assert (cols % 2 == 0).any() and (cols % 2 == 1).any()
+    g = crand(rng, (2, 6, 128, 128))
+    big = torch.zeros(2 * 140 * n + shift, dtype=torch.complex64, device="cuda")
+    out = big[shift:]
+    assert out.data_ptr() % 16 == 8 * shift
+    op.adj(out.data_ptr(), dev(g))
+    assert rel(out.view(2, 140, n).cpu().numpy(), orc.adj(g)) <= TOL
+
+
 @pytest.mark.parametrize("ntheta,nz,n,nscan,det,nprb", [(2, 130, 140, 6, 128, 128), (2, 100, 110, 4, 128, 96),
                                                        (2, 64, 64, 9, 64, 32), (3, 20, 20, 3, 8, 8)])
 @pytest.mark.parametrize("model", [0, 1])
