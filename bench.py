@@ -248,8 +248,18 @@ class Ops:
         return bi, bo
 
     def launches_per_step(self):
+        """Kernel launches of one step: radon fwd 4 per 8-slice chunk, radon adj 3,
+        ptycho fwd 1, ptycho adj 1 plus the slab reduction when the angles are
+        split into parts (the library's wave model, restated here)."""
         zc = -(-self.c["nz"] // 8)
-        return 3 * zc + 3 + 2   # radon fwd: 3 per 8-slice chunk; radon adj: 3; ptycho: 1 + 1
+        nt, S = self.c["ntheta"], self.c["nside"] ** 2
+        nsm = self.torch.cuda.get_device_properties(self.dev).multi_processor_count
+        best, parts = 1e300, 1
+        for p in range(1, min(S, 16) + 1):
+            cost = -(-nt * p // nsm) * -(-S // p) * (1.0 + 0.03 * (p - 1))
+            if cost < best - 1e-9:
+                best, parts = cost, p
+        return 4 * zc + 3 + 1 + 1 + (parts > 1)
 
 
 def run_ours(args, rank, world, local):
