@@ -376,21 +376,34 @@ constexpr int P128_SMEM = (64 * 128) * 16 + 128 * 8;
 constexpr int P128_SMEM_RESID = P128_SMEM + 128 * 8 + 128 * 128 * 4;
 
 
+// The det-128 twiddles a thread needs, w(t k1) for k1 = 0..15, in pairs:
+// entry q * 8 + t of the 64-entry float4 table holds w(2q t) and w((2q+1) t).
+// The 8 threads of a group read 8 consecutive entries (one conflict-free
+// 128-byte access, shared by the warp's 4 groups), 8 loads per line.
+//
 // FOLD: the line still has to be multiplied by a per-frame factor f (the
 // scan's phase and the scale).  Since the transform is linear, f rides on the
-// twiddles: tws is then a per-frame table (fold_twiddles) already in the
-// transform's direction and multiplied by f, whose entry 0 is f itself, so
-// element 0 takes its product from the table as well.
+// twiddles: tw4 is then a per-frame table (fold_twiddles) already in the
+// transform's direction and multiplied by f, whose k1 = 0 entries are f
+// itself, so element 0 takes its product from the table as well.
+template <int DIR, bool FOLD>
+__device__ __forceinline__ void twiddle16(float2 (&v)[16], float4 w, int q)
+{
+    float2 w0 = make_float2(w.x, w.y), w1 = make_float2(w.z, w.w);
+    if (DIR > 0 && !FOLD) {
+        w0.y = -w0.y;
+        w1.y = -w1.y;
+    }
+    if (FOLD || q > 0) v[2 * q] = cmul(v[2 * q], w0);
+    v[2 * q + 1] = cmul(v[2 * q + 1], w1);
+}
+
 template <int DIR, bool FOLD = false>
-__device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, const float2 *tws)
+__device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, const float4 *tw4)
 {
     ptfft::Dft<16, DIR>::run(v);
 #pragma unroll
-    for (int k1 = FOLD ? 0 : 1; k1 < 16; ++k1) {
-        float2 w = tws[t * k1];
-        if (DIR > 0 && !FOLD) w.y = -w.y;
-        v[k1] = cmul(v[k1], w);
-    }
+    for (int q = 0; q < 8; ++q) twiddle16<DIR, FOLD>(v, tw4[q * 8 + t], q);
     __syncwarp();
 #pragma unroll
     for (int q = 0; q < 8; ++q) sc[t * 8 + ((q + t) & 7)] = make_float4(v[2 * q].x, v[2 * q].y, v[2 * q + 1].x, v[2 * q + 1].y);
@@ -417,16 +430,15 @@ __device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, 
 // are bit-identical to two line_dft128 calls.
 template <int DIR, bool FOLD = false>
 __device__ __forceinline__ void line_dft128x2(float2 (&a)[16], float2 (&b)[16], int t, float4 *sa, float4 *sb,
-                                              const float2 *tws)
+                                              const float4 *tw4)
 {
     ptfft::Dft<16, DIR>::run(a);
     ptfft::Dft<16, DIR>::run(b);
 #pragma unroll
-    for (int k1 = FOLD ? 0 : 1; k1 < 16; ++k1) {
-        float2 w = tws[t * k1];
-        if (DIR > 0 && !FOLD) w.y = -w.y;
-        a[k1] = cmul(a[k1], w);
-        b[k1] = cmul(b[k1], w);
+    for (int q = 0; q < 8; ++q) {
+        const float4 w = tw4[q * 8 + t];
+        twiddle16<DIR, FOLD>(a, w, q);
+        twiddle16<DIR, FOLD>(b, w, q);
     }
     __syncwarp();
 #pragma unroll
@@ -458,17 +470,22 @@ __device__ __forceinline__ void line_dft128x2(float2 (&a)[16], float2 (&b)[16], 
     }
 }
 
-// Per-frame folded twiddle table for line_dft128<DIR, true>: tw[i] in
-// direction DIR times f, entry 0 (a twiddle of 1) being f exactly.  Threads
-// 0..127 write one entry each.
+// Per-frame folded twiddle table for line_dft128<DIR, true>: the pair table
+// tw4 in direction DIR times f, the k1 = 0 entries (a twiddle of 1) being f
+// exactly.  Threads 0..63 write one entry each.
 template <int DIR>
-__device__ __forceinline__ void fold_twiddles(float2 *twf, const float2 *__restrict__ tw, float2 f)
+__device__ __forceinline__ void fold_twiddles(float4 *twf, const float4 *__restrict__ tw4, float2 f)
 {
     const int i = threadIdx.x;
-    if (i < 128) {
-        float2 w = tw[i];
-        if (DIR > 0) w.y = -w.y;
-        twf[i] = i == 0 ? f : cmul(w, f);
+    if (i < 64) {
+        const float4 w = tw4[i];
+        float2 w0 = make_float2(w.x, w.y), w1 = make_float2(w.z, w.w);
+        if (DIR > 0) {
+            w0.y = -w0.y;
+            w1.y = -w1.y;
+        }
+        const float2 a = i < 8 ? f : cmul(w0, f), b = cmul(w1, f);
+        twf[i] = make_float4(a.x, a.y, b.x, b.y);
     }
 }
 
@@ -476,13 +493,13 @@ template <bool FULL>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_fwd128(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                    int nframes, int P, float scale, const float2 *__restrict__ tw)
+                    int nframes, int P, float scale, const float4 *__restrict__ tw)
 {
     extern __shared__ float4 sm4[];
     float4 *fr = sm4;
     // the shared table holds this frame's column twiddles x scale x phase
     // (line_dft128's FOLD); the row pass reads the plain twiddles from global
-    float2 *twf = reinterpret_cast<float2 *>(sm4 + 64 * 128);
+    float4 *twf = sm4 + 64 * 128;
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
     // exchange slots: the whole frame buffer is idle during both passes
     float4 *sa = fr + grp * 64, *sb = fr + 64 * 64 + grp * 64;
@@ -626,7 +643,7 @@ template <bool FULL, int RESID>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                    int P, float scale, const float2 *__restrict__ tw, const float *__restrict__ data,
+                    int P, float scale, const float4 *__restrict__ tw, const float *__restrict__ data,
                     float dscale)
 {
     // X2: both lines of a group through line_dft128x2, the second exchange
@@ -640,12 +657,12 @@ __global__ void __launch_bounds__(512, 1)
     extern __shared__ float4 sm4[];
     float4 *fr = sm4;
     float4 *pre = sm4 + 64 * 64;  // upper 64 KB of the frame buffer
-    float2 *tws = reinterpret_cast<float2 *>(sm4 + 64 * 128);
-    float2 *twf = tws + 128;  // RESID: the folded row-pass twiddles
+    float4 *tws = sm4 + 64 * 128;
+    float4 *twf = tws + 64;  // RESID: the folded row-pass twiddles
     float *cnt = reinterpret_cast<float *>(sm4 + 64 * 128 + 128);  // RESID: this frame's counts
     const int part = blockIdx.x, parts = gridDim.x, th = blockIdx.y;
     float2 *slab = dst + ((size_t)th * parts + part) * nz * n;
-    for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
+    for (int i = threadIdx.x; i < 64; i += 512) tws[i] = tw[i];
     for (int e = threadIdx.x; e < nz * n; e += 512) slab[e] = czero();
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
     float4 *sa = fr + grp * 64, *sb = pre + grp * 64;
@@ -786,17 +803,17 @@ template <bool FULL, int RESID, bool PROBE>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128v(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                    int P, float scale, const float2 *__restrict__ tw, const float *__restrict__ data,
+                    int P, float scale, const float4 *__restrict__ tw, const float *__restrict__ data,
                     float dscale, const float2 *__restrict__ psi = nullptr, int nframes = 0)
 {
     extern __shared__ float4 sm4[];
     float4 *fr = sm4;
     float4 *pre = sm4 + 64 * 64;  // upper 64 KB of the frame buffer
-    float2 *tws = reinterpret_cast<float2 *>(sm4 + 64 * 128);
+    float4 *tws = sm4 + 64 * 128;
     // FOLD (object adjoint): the frame's scale x conj(phase) rides on the
     // row-pass twiddles, as in k_ptycho_adj128
     constexpr bool FOLD = !PROBE;
-    float2 *twf = tws + 128;
+    float4 *twf = tws + 64;
     float *cnt = reinterpret_cast<float *>(sm4 + 64 * 128 + 128);  // RESID: this frame's counts
     auto fold_for = [&](size_t f) {
         const float2 p = phase[f];
@@ -805,7 +822,7 @@ __global__ void __launch_bounds__(512, 1)
     const int part = blockIdx.x, parts = gridDim.x;
     const int th0 = blockIdx.y;   // the angle (object slabs)
     float2 *slab = PROBE ? dst + (size_t)part * P * P : dst + ((size_t)th0 * parts + part) * nz * n;
-    for (int i = threadIdx.x; i < 128; i += 512) tws[i] = tw[i];
+    for (int i = threadIdx.x; i < 64; i += 512) tws[i] = tw[i];
     for (int e = threadIdx.x; e < (PROBE ? P * P : nz * n); e += 512) slab[e] = czero();
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
     // exchange slots: sa in the lower half, sb = the group's own prefetch row
@@ -1047,6 +1064,7 @@ struct pt_ptycho {
     bool ready = false;
     float c = 0.f;
     float2 *tw = nullptr, *prb = nullptr, *prbT = nullptr, *phase = nullptr, *partial = nullptr;
+    float4 *tw128 = nullptr;  // det = 128: the twiddles in line_dft128's pair layout
     int *corner = nullptr;
     // probe retrieval: a second transposed probe table (forward with a given
     // probe) and one P x P partial per block of the probe adjoint
@@ -1117,15 +1135,16 @@ int ptycho_adj_launch(pt_ptycho *h, float2 *out, const float2 *in, float scale, 
             if constexpr (RESID == 2)
                 k_ptycho_adj128v<true, RESID, false><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase, h->prbT,
                                                                              h->nz, h->n, h->nscan, h->P, scale,
-                                                                             h->tw, data, dscale);
+                                                                             h->tw128, data, dscale);
             else
                 k_ptycho_adj128<true, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz,
-                                                                     h->n, h->nscan, h->P, scale, h->tw, data,
+                                                                     h->n, h->nscan, h->P, scale, h->tw128, data,
                                                                      dscale);
         }
         else if (fast128)
             k_ptycho_adj128<false, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz,
-                                                                  h->n, h->nscan, h->P, scale, h->tw, data, dscale);
+                                                                  h->n, h->nscan, h->P, scale, h->tw128, data,
+                                                                  dscale);
         else
             k_ptycho_adj<DET, RESID><<<grid, F::NT, F::SMEM, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz, h->n,
                                                                   h->nscan, h->P, scale, h->tw, data, dscale);
@@ -1160,10 +1179,10 @@ int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scal
         const bool fast128 = DET == 128 && ((uintptr_t)out % 16) == 0;
         if (fast128 && h->P == DET)
             k_ptycho_fwd128<true><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
-                                                                  h->nscan, nframes, h->P, scale, h->tw);
+                                                                  h->nscan, nframes, h->P, scale, h->tw128);
         else if (fast128)
             k_ptycho_fwd128<false><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz,
-                                                                   h->n, h->nscan, nframes, h->P, scale, h->tw);
+                                                                   h->n, h->nscan, nframes, h->P, scale, h->tw128);
         else
             k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
                                                               h->nscan, nframes, h->P, scale, h->tw);
@@ -1218,7 +1237,7 @@ int probe_adj_launch(pt_ptycho *h, float2 *gprb, const float2 *in, const float2 
         const int smem = RESID ? P128_SMEM_RESID : P128_SMEM;
         if (fast128)
             k_ptycho_adj128v<true, RESID, true><<<h->prb_blocks, 512, smem, st>>>(
-                in, h->prb_part, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw, data,
+                in, h->prb_part, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw128, data,
                 dscale, psi, nframes);
         else
             k_ptycho_adj_probe<DET, RESID><<<h->prb_blocks, F::NT, F::SMEM, st>>>(
@@ -1248,7 +1267,7 @@ int probe_adj_dispatch(pt_ptycho *h, float2 *gprb, const float2 *in, const float
 
 void ptycho_free(pt_ptycho *h)
 {
-    void *bufs[] = {h->tw, h->prb, h->prbT, h->phase, h->partial, h->corner, h->prbT2, h->prb_part};
+    void *bufs[] = {h->tw, h->tw128, h->prb, h->prbT, h->phase, h->partial, h->corner, h->prbT2, h->prb_part};
     for (void *p : bufs)
         if (p) cudaFree(p);
 }
@@ -1306,6 +1325,7 @@ extern "C" int pt_ptycho_create(size_t ntheta, size_t nz, size_t n, size_t nthet
         }
     }
     bool ok = cudaMalloc((void **)&h->tw, detx * sizeof(float2)) == cudaSuccess &&
+              cudaMalloc((void **)&h->tw128, 64 * sizeof(float4)) == cudaSuccess &&
               cudaMalloc((void **)&h->prb, nprb * nprb * sizeof(float2)) == cudaSuccess &&
               cudaMalloc((void **)&h->prbT, nprb * nprb * sizeof(float2)) == cudaSuccess &&
               (h->parts == 1 || cudaMalloc((void **)&h->partial, (size_t)h->parts * ntheta * nz * n * sizeof(float2)) ==
@@ -1328,6 +1348,19 @@ extern "C" int pt_ptycho_create(size_t ntheta, size_t nz, size_t n, size_t nthet
     if (rc == PT_OK && cudaMemcpy(h->tw, tw.data(), detx * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
         pt::set_error("ptychofft: twiddle upload failed");
         rc = PT_ERR_CUDA;
+    }
+    if (rc == PT_OK && detx == 128) {
+        // entry q * 8 + t = (w(2q t), w((2q+1) t)), t k1 <= 105 < 128
+        std::vector<float4> tw4(64);
+        for (int q = 0; q < 8; ++q)
+            for (int t = 0; t < 8; ++t) {
+                const float2 a = tw[2 * q * t], b = tw[(2 * q + 1) * t];
+                tw4[q * 8 + t] = make_float4(a.x, a.y, b.x, b.y);
+            }
+        if (cudaMemcpy(h->tw128, tw4.data(), 64 * sizeof(float4), cudaMemcpyHostToDevice) != cudaSuccess) {
+            pt::set_error("ptychofft: twiddle upload failed");
+            rc = PT_ERR_CUDA;
+        }
     }
     if (rc != PT_OK) {
         ptycho_free(h);
