@@ -424,52 +424,6 @@ __device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, 
     }
 }
 
-// Two independent lines through line_dft128 side by side: one twiddle load
-// and one pair of warp barriers serve both, and the two instruction streams
-// interleave.  sa and sb are two 1 KB exchange slots of the group.  Results
-// are bit-identical to two line_dft128 calls.
-template <int DIR, bool FOLD = false>
-__device__ __forceinline__ void line_dft128x2(float2 (&a)[16], float2 (&b)[16], int t, float4 *sa, float4 *sb,
-                                              const float4 *tw4)
-{
-    ptfft::Dft<16, DIR>::run(a);
-    ptfft::Dft<16, DIR>::run(b);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const float4 w = tw4[q * 8 + t];
-        twiddle16<DIR, FOLD>(a, w, q);
-        twiddle16<DIR, FOLD>(b, w, q);
-    }
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        sa[t * 8 + ((q + t) & 7)] = make_float4(a[2 * q].x, a[2 * q].y, a[2 * q + 1].x, a[2 * q + 1].y);
-        sb[t * 8 + ((q + t) & 7)] = make_float4(b[2 * q].x, b[2 * q].y, b[2 * q + 1].x, b[2 * q + 1].y);
-    }
-    __syncwarp();
-    float2 a0[8], a1[8], b0[8], b1[8];
-#pragma unroll
-    for (int n2 = 0; n2 < 8; ++n2) {
-        const float4 wa = sa[n2 * 8 + ((t + n2) & 7)];
-        const float4 wb = sb[n2 * 8 + ((t + n2) & 7)];
-        a0[n2] = make_float2(wa.x, wa.y);
-        a1[n2] = make_float2(wa.z, wa.w);
-        b0[n2] = make_float2(wb.x, wb.y);
-        b1[n2] = make_float2(wb.z, wb.w);
-    }
-    ptfft::Dft<8, DIR>::run(a0);
-    ptfft::Dft<8, DIR>::run(a1);
-    ptfft::Dft<8, DIR>::run(b0);
-    ptfft::Dft<8, DIR>::run(b1);
-#pragma unroll
-    for (int k2 = 0; k2 < 8; ++k2) {
-        a[k2] = a0[k2];
-        a[8 + k2] = a1[k2];
-        b[k2] = b0[k2];
-        b[8 + k2] = b1[k2];
-    }
-}
-
 // Per-frame folded twiddle table for line_dft128<DIR, true>: the pair table
 // tw4 in direction DIR times f, the k1 = 0 entries (a twiddle of 1) being f
 // exactly.  Threads 0..63 write one entry each.
@@ -502,10 +456,7 @@ __global__ void __launch_bounds__(512, 1)
     float4 *twf = sm4 + 64 * 128;
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
     // exchange slots, one per line: the whole frame buffer is idle during both
-    // passes, so the two lines' exchanges need not wait on each other.  One
-    // line at a time (load, transform, store) measured faster here than
-    // line_dft128x2 (4.04 against 4.09 ms at 256^3), once the twiddles were
-    // in the pair layout and folded.
+    // passes, so the two lines' exchanges need not wait on each other
     float4 *sa = fr + grp * 64, *sb = fr + 64 * 64 + grp * 64;
     const int off = FULL ? 0 : (128 - P) / 2;
     for (int fid = blockIdx.x; fid < nframes; fid += gridDim.x) {
@@ -650,14 +601,14 @@ __global__ void __launch_bounds__(512, 1)
                     int P, float scale, const float4 *__restrict__ tw, const float *__restrict__ data,
                     float dscale)
 {
-    // X2: both lines of a group through line_dft128x2, the second exchange
-    // slot being the group's own prefetch row.  FOLD: the frame's scale x
-    // conj(phase) rides on the row-pass twiddles (line_dft128); the folded
-    // table is written for the next frame during the column pass, after the
-    // last read of the current one.  Both measured faster with the Poisson
-    // residual and slower for the plain adjoint (5.89 and 8.78 against
-    // 5.75 ms at 256^3).
-    constexpr bool X2 = RESID == 1, FOLD = RESID == 1;
+    // SLOT2: the second line of a group exchanges through the group's own
+    // prefetch row (already in registers), and the next frame's row is
+    // fetched by the group itself after a warp barrier.  FOLD: the frame's
+    // scale x conj(phase) rides on the row-pass twiddles (line_dft128); the
+    // folded table is written for the next frame during the column pass,
+    // after the last read of the current one.  Both measured faster with the
+    // Poisson residual and slower for the plain adjoint.
+    constexpr bool SLOT2 = RESID == 1, FOLD = RESID == 1;
     extern __shared__ float4 sm4[];
     float4 *fr = sm4;
     float4 *pre = sm4 + 64 * 64;  // upper 64 KB of the frame buffer
@@ -671,7 +622,7 @@ __global__ void __launch_bounds__(512, 1)
     const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
     float4 *sa = fr + grp * 64, *sb = pre + grp * 64;
     auto prefetch_frame = [&](const float2 *src) {
-        if constexpr (X2)
+        if constexpr (SLOT2)
             prefetch_group_row(pre, src, grp, t);
         else
             prefetch_half_frame(pre, src);
@@ -722,17 +673,14 @@ __global__ void __launch_bounds__(512, 1)
             if constexpr (RESID != 0) D = staged_count(cnt, grp, ky) * dscale;
             v[0][m] = FOLD ? resid_of<RESID>(x, D) : scale * cmulc(ph, resid_of<RESID>(x, D));
         }
-        if constexpr (!X2) line_dft128<+1, FOLD>(v[0], t, sa, FOLD ? twf : tws);
+        line_dft128<+1, FOLD>(v[0], t, sa, FOLD ? twf : tws);
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             float D = 0.f;
             if constexpr (RESID != 0) D = staged_count(cnt, grp + 64, t + 8 * m) * dscale;
             v[1][m] = FOLD ? resid_of<RESID>(v[1][m], D) : scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
         }
-        if constexpr (X2)
-            line_dft128x2<+1, FOLD>(v[0], v[1], t, sa, sb, FOLD ? twf : tws);
-        else
-            line_dft128<+1, FOLD>(v[1], t, sa, FOLD ? twf : tws);
+        line_dft128<+1, FOLD>(v[1], t, SLOT2 ? sb : sa, FOLD ? twf : tws);
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -753,17 +701,16 @@ __global__ void __launch_bounds__(512, 1)
         __syncthreads();
         if constexpr (FOLD)
             if (more) fold_for(fid + parts);
-        if (more && !X2) prefetch_half_frame(pre, in_next);
+        if (more && !SLOT2) prefetch_half_frame(pre, in_next);
         if constexpr (RESID != 0)
             if (more) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
-        if constexpr (X2) {
-            line_dft128x2<+1>(v[0], v[1], t, sa, sb, tws);
-            __syncwarp();  // the group's reads of its slot sb are done before the next frame lands there
-            if (more) prefetch_group_row(pre, in_next, grp, t);
-        }
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            if constexpr (!X2) line_dft128<+1>(v[c], t, sa, tws);
+            line_dft128<+1>(v[c], t, SLOT2 && c ? sb : sa, tws);
+            if (SLOT2 && c == 1) {
+                __syncwarp();  // the group's reads of its slot sb are done before the next frame lands there
+                if (more) prefetch_group_row(pre, in_next, grp, t);
+            }
             const int py = 2 * grp + c - off;
             if (!FULL && (py < 0 || py >= P)) continue;
             float2 *row = slab + (size_t)(sty + py) * n + stx;
@@ -797,12 +744,12 @@ __global__ void __launch_bounds__(512, 1)
 // The same transform written for both adjoints.  PROBE: the adjoint with
 // respect to the probe (as k_ptycho_adj_probe): grid (blocks, 1), block b
 // walks frames b, b + gridDim.x, ... and accumulates conj(psi patch) x frame
-// into its P x P partial dst[b].  Otherwise as k_ptycho_adj128 with both
-// lines of a group through line_dft128x2.  At 256^3 this formulation takes
-// 7.6 ms for the Gaussian residual (11.0 for k_ptycho_adj128's) and 6.4 ms
-// for the Poisson probe adjoint (12.3 for k_ptycho_adj_probe), but 5.76 and
-// 8.16 ms for the plain and Poisson object adjoints (5.75 and 7.44 for
-// k_ptycho_adj128's), so each launch takes the faster one.
+// into its P x P partial dst[b].  Otherwise as k_ptycho_adj128 with the
+// second line exchanging through the group's own prefetch row.  The compiler
+// schedules this formulation differently at the 128-register ceiling; it
+// measured faster for the Gaussian residual (11.0 ms for k_ptycho_adj128's)
+// and the probe adjoint (12.3 ms for k_ptycho_adj_probe) and slower for the
+// plain and Poisson object adjoints, so each launch takes the faster one.
 template <bool FULL, int RESID, bool PROBE>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128v(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
@@ -876,13 +823,14 @@ __global__ void __launch_bounds__(512, 1)
             if constexpr (RESID != 0) D = staged_count(cnt, grp, ky) * dscale;
             v[0][m] = FOLD ? resid_of<RESID>(x, D) : scale * cmulc(ph, resid_of<RESID>(x, D));
         }
+        line_dft128<+1, FOLD>(v[0], t, sa, FOLD ? twf : tws);
 #pragma unroll
         for (int m = 0; m < 16; ++m) {
             float D = 0.f;
             if constexpr (RESID != 0) D = staged_count(cnt, grp + 64, t + 8 * m) * dscale;
             v[1][m] = FOLD ? resid_of<RESID>(v[1][m], D) : scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
         }
-        line_dft128x2<+1, FOLD>(v[0], v[1], t, sa, sb, FOLD ? twf : tws);
+        line_dft128<+1, FOLD>(v[1], t, sb, FOLD ? twf : tws);
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -905,11 +853,13 @@ __global__ void __launch_bounds__(512, 1)
             if (more) fold_for((size_t)fid + parts);
         if constexpr (RESID != 0)
             if (more) prefetch_counts(cnt, data + (size_t)(fid + parts) * 128 * 128);
-        line_dft128x2<+1>(v[0], v[1], t, sa, sb, tws);
-        __syncwarp();  // the group's reads of its slot sb are done before the next frame lands there
-        if (more) prefetch_group_row(pre, in_next, grp, t);
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
+            line_dft128<+1>(v[c], t, c ? sb : sa, tws);
+            if (c == 1) {
+                __syncwarp();  // the group's reads of its slot sb are done before the next frame lands there
+                if (more) prefetch_group_row(pre, in_next, grp, t);
+            }
             const int py = 2 * grp + c - off;
             if (!FULL && (py < 0 || py >= P)) continue;
             // object: slab row += conj(c prbT) x; probe: partial row += conj(psi) x
