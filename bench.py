@@ -336,7 +336,7 @@ def run_ours(args, rank, world, local):
     # the roofline entry is for the step's largest single kernel: the ptycho
     # operators are one launch each (k_ptycho_fwd128, k_ptycho_adj128 plus a
     # short slab reduction); the radon operators are sequences of short
-    # launches (3 per 8-slice chunk forward), each far below either ptycho
+    # launches (4 per 8-slice chunk forward), each far below either ptycho
     # kernel, so their rates are in per_op_gbs only
     dom = max(("ptycho_fwd", "ptycho_adj"), key=per_op.get)
     achieved = bytes_op[dom] / (per_op[dom] * 1e-3) / 1e9
