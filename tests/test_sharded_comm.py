@@ -9,7 +9,6 @@ reductions and the gather used to assemble results.
 import os
 import socket
 
-import numpy as np
 import pytest
 
 torch = pytest.importorskip("torch")
