@@ -43,7 +43,6 @@ namespace {
 
 constexpr int ZC = 8;   // slices per chunk (slice-minor lanes)
 constexpr int CK = 2;   // grid columns per block in the column kernels
-constexpr int GB = 64;  // polar points staged per batch in the adjoint scatter
 constexpr double PI_REF = 3.1415926535;  // kernels.cuh:1
 
 template <int L>

@@ -21,8 +21,6 @@ constexpr int RB = 1184;    // reduction blocks (148 SMs x 8)
 constexpr int RT = 256;     // reduction threads per block
 constexpr int MAXK = 16;    // max outputs of one reduction
 
-__device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-
 template <int K>
 __device__ __forceinline__ void block_reduce_store(double (&acc)[K], double *work, int blk, int nblk)
 {
