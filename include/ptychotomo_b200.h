@@ -154,9 +154,12 @@ int pt_ls_frames_advance(void *f, const void *d, const float *data, float dscale
  * memory, or a latency-bound loop that must not call cudaMalloc (which can
  * synchronise the device) after start-up.  The scratch (148 KiB: 1184
  * blocks x 16 FP64 partials) is a static device array of the library, held
- * on every GPU that loads it until the process exits.  The first call on a
- * device looks up the array's address (cudaGetSymbolAddress) and should be
- * made before any stream capture.  J > 16 is rejected with PT_ERR_ARG.
+ * on every GPU that loads it until the process exits.  The array's device
+ * address belongs to a CUDA context: the first call in each context (the
+ * runtime's primary context of a device, a caller's own driver-API context,
+ * or the new primary context after cudaDeviceReset) looks it up with
+ * cudaGetSymbolAddress and caches it with that context's id; make that first
+ * call before any stream capture.  J > 16 is rejected with PT_ERR_ARG.
  * All calls share the scratch: calls that overlap on the GPU (different
  * streams, or concurrent host threads) race and give wrong sums. */
 int pt_ls_frames_noalloc(const void *f, const void *d, const float *data, float dscale, size_t n, int model,

@@ -15,6 +15,9 @@ Frame element (ix, iy) multiplies prb[ix, iy] with psi[sty+iy, stx+ix]
 from __future__ import annotations
 
 import numpy as np
+import scipy.fft as sfft
+
+from ._threads import WORKERS
 
 PI_REF = 3.1415926535  # kernels.cuh:1
 
@@ -73,7 +76,7 @@ class PtychoFFT:
                     continue
                 patch = f[t, y0:y0 + P, x0:x0 + P].astype(np.complex128).T   # [ix, iy]
                 g[t, s, rs:rs + P, cs:cs + P] = self.c * self.prb * patch
-        g = np.fft.fft2(g, axes=(-2, -1))
+        g = sfft.fft2(g, axes=(-2, -1), workers=WORKERS)
         g *= self.phase[:, :, None, None]
         return g
 
@@ -82,7 +85,7 @@ class PtychoFFT:
         g = np.asarray(g).reshape(self.ntheta, self.nscan, dx, dy).astype(np.complex128)
         rs, cs = (dx - P) // 2, (dy - P) // 2
         g = g * np.conj(self.phase)[:, :, None, None]
-        g = np.fft.ifft2(g, axes=(-2, -1)) * (dx * dy)
+        g = sfft.ifft2(g, axes=(-2, -1), workers=WORKERS) * (dx * dy)
         f = np.zeros((self.ntheta, self.nz, self.n), np.complex128)
         cp = self.c * np.conj(self.prb)
         for t in range(self.ntheta):
@@ -102,7 +105,7 @@ class PtychoFFT:
         g = np.asarray(g).reshape(self.ntheta, self.nscan, dx, dy).astype(np.complex128)
         f = np.asarray(f).reshape(self.ntheta, self.nz, self.n)
         rs, cs = (dx - P) // 2, (dy - P) // 2
-        G = np.fft.ifft2(g * np.conj(self.phase)[:, :, None, None], axes=(-2, -1)) * (dx * dy)
+        G = sfft.ifft2(g * np.conj(self.phase)[:, :, None, None], axes=(-2, -1), workers=WORKERS) * (dx * dy)
         gp = np.zeros((P, P), np.complex128)
         for t in range(self.ntheta):
             for s in range(self.nscan):

@@ -13,8 +13,11 @@ denominator gives beta = 0.
 """
 from __future__ import annotations
 
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 
+from ._threads import WORKERS
 from .ptycho import PtychoFFT
 from .usfft import RadonUSFFT
 
@@ -32,6 +35,18 @@ def _vdot(a, b):
     """sum(conj(a)*b) accumulated in complex128."""
     return complex(np.vdot(np.asarray(a).astype(np.complex128).ravel(),
                            np.asarray(b).astype(np.complex128).ravel()))
+
+
+def _par_sum(fn, *arrays):
+    """sum of fn(chunk...) over chunks of the arrays' first axis, in threads
+    (NumPy releases the GIL inside its elementwise loops)."""
+    k = min(WORKERS, arrays[0].shape[0])
+    if k < 2:
+        return fn(*arrays)
+    bounds = np.linspace(0, arrays[0].shape[0], k + 1).astype(int)
+    with ThreadPoolExecutor(k) as ex:
+        parts = ex.map(lambda i: fn(*(a[bounds[i]:bounds[i + 1]] for a in arrays)), range(k))
+        return sum(parts)
 
 
 class Solver:
@@ -183,12 +198,14 @@ class Solver:
 
     # ---- CG ptychography, solver.py:206-254 --------------------------------
     def cg_ptycho(self, data, init, h, lamd, rho, piter, model):
-        def minf(psi, fpsi):
+        def data_term(fpsi, data):
             if model == 'gaussian':
-                f = _norm2(np.abs(fpsi) - np.sqrt(data))
-            else:
-                a = np.abs(fpsi).astype(np.float64)
-                f = float(np.sum(a ** 2 - 2 * data.astype(np.float64) * self.mlog(a)))
+                return _norm2(np.abs(fpsi) - np.sqrt(data))
+            a = np.abs(fpsi).astype(np.float64)
+            return float(np.sum(a ** 2 - 2 * data.astype(np.float64) * self.mlog(a)))
+
+        def minf(psi, fpsi):
+            f = _par_sum(data_term, fpsi, data)
             f += rho * _norm2(h - psi + lamd / rho)
             return f
 
@@ -271,22 +288,33 @@ class Solver:
         return lagr
 
     # ---- ADMM, solver.py:308-336 -------------------------------------------
+    STATE = ("u", "psi", "h", "e", "phi", "lamd", "mu")
+
+    def admm_step(self, m, st, rho, tau, data, alpha, piter, titer, model):
+        """One iteration of the loop body solver.py:311-329 from the state st
+        (a dict of u, psi, h, e, phi, lamd, mu); returns (new state, rho, tau)."""
+        u, psi, h, e, phi, lamd, mu = (st[k] for k in self.STATE)
+        h0, e0 = h, e
+        psi = self.cg_ptycho_batch(data, psi, h, lamd, rho, piter + (m < 2) * 32, model)
+        xi0, xi1, K, pshift = self.takexi(psi, phi, lamd, mu, rho, tau)
+        u = self.cg_tomo(xi0, xi1, K, u, rho, tau, titer)
+        phi = self.solve_reg(u, mu, tau, alpha)
+        h = (self.exptomo(self.fwd_tomo_batch(u)) * np.exp(1j * pshift)).astype(np.complex64)
+        e = self.fwd_reg(u)
+        lamd = (lamd + rho * (h - psi)).astype(np.complex64)
+        mu = (mu + tau * (e - phi)).astype(np.complex64)
+        rho, tau = self.update_penalty(psi, h, h0, phi, e, e0, rho, tau)
+        return dict(u=u, psi=psi, h=h, e=e, phi=phi, lamd=lamd, mu=mu), rho, tau
+
     def admm(self, data, h, e, psi, phi, lamd, mu, u, alpha, piter, titer, niter, model,
              lagr_every=10, history=None):
         rho, tau = 0.5, 0.5
+        st = dict(u=u, psi=psi, h=h, e=e, phi=phi, lamd=lamd, mu=mu)
         for m in range(niter):
-            h0, e0 = h, e
-            psi = self.cg_ptycho_batch(data, psi, h, lamd, rho, piter + (m < 2) * 32, model)
-            xi0, xi1, K, pshift = self.takexi(psi, phi, lamd, mu, rho, tau)
-            u = self.cg_tomo(xi0, xi1, K, u, rho, tau, titer)
-            phi = self.solve_reg(u, mu, tau, alpha)
-            h = (self.exptomo(self.fwd_tomo_batch(u)) * np.exp(1j * pshift)).astype(np.complex64)
-            e = self.fwd_reg(u)
-            lamd = (lamd + rho * (h - psi)).astype(np.complex64)
-            mu = (mu + tau * (e - phi)).astype(np.complex64)
-            rho, tau = self.update_penalty(psi, h, h0, phi, e, e0, rho, tau)
+            st, rho, tau = self.admm_step(m, st, rho, tau, data, alpha, piter, titer, model)
             if history is not None:
                 history.append(dict(m=m, rho=rho, tau=tau))
             if lagr_every and m % lagr_every == 0 and history is not None:
-                history[-1]["lagr"] = self.take_lagr(psi, phi, data, h, e, lamd, mu, alpha, rho, tau, model)
-        return u, psi
+                history[-1]["lagr"] = self.take_lagr(st["psi"], st["phi"], data, st["h"], st["e"], st["lamd"],
+                                                     st["mu"], alpha, rho, tau, model)
+        return st["u"], st["psi"]

@@ -12,8 +12,10 @@ Arithmetic is complex128, except where the reference takes a discrete
 decision from a float32 value (polar coordinates, floor() of the grid
 position, the circular mask, the kernel parameter mu); those are evaluated
 in float32 exactly as the reference writes them.  cuFFT's C2C transforms
-are unnormalised with FORWARD = exp(-2*pi*i...), which numpy.fft matches
-(inverse = ifft * length).
+are unnormalised with FORWARD = exp(-2*pi*i...), which scipy.fft matches
+(inverse = ifft * length); the FFTs run on all host cores (``workers``).
+The gridding is one sparse matrix (taps x weights) applied to every slice
+at once, its columns split over threads.
 
 The reference computes the polar coordinates with the fast intrinsics
 ``__cosf``/``__sinf`` (kernels.cuh:91-92).  Their results cannot be
@@ -24,8 +26,13 @@ test can hand the oracle the exact tables a GPU computed.
 from __future__ import annotations
 
 import math
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
+import scipy.fft as sfft
+import scipy.sparse as sparse
+
+from ._threads import WORKERS
 
 PI_REF = 3.1415926535  # kernels.cuh:1 (#define PI 3.1415926535)
 
@@ -120,19 +127,33 @@ class GridTaps:
         self.idx = (cy[:, :, None] * G + cx[:, None, :])
         self.npts = x.size
         self.G = G
+        taps = (2 * M + 1) ** 2
+        self.S = sparse.csr_matrix((self.w.ravel(), self.idx.ravel(), np.arange(0, self.npts * taps + 1, taps)),
+                                   shape=(self.npts, G * G))
+        self.ST = self.S.T.tocsr()
+
+    @staticmethod
+    def _apply(A, X):
+        """A @ X for X [cols, k] complex, the k columns split over threads."""
+        k = X.shape[1]
+        if k < 2 or WORKERS < 2:
+            return A @ X
+        parts = np.array_split(np.arange(k), min(k, WORKERS))
+        with ThreadPoolExecutor(len(parts)) as ex:
+            cols = list(ex.map(lambda c: A @ X[:, c], parts))
+        return np.concatenate(cols, axis=1)
 
     def gather(self, F):
-        """F: [G, G] complex -> samples [npts]."""
-        vals = F.ravel()[self.idx]
-        return np.einsum("pij,pij->p", self.w, vals)
+        """F: [G, G] or [nz, G, G] complex -> samples [npts] or [npts, nz]."""
+        if F.ndim == 2:
+            return self.S @ F.ravel()
+        return self._apply(self.S, np.ascontiguousarray(F.reshape(F.shape[0], -1).T))
 
     def scatter(self, g):
-        """g: [npts] complex -> grid [G, G] (transpose of gather)."""
-        c = self.w * g[:, None, None]
-        flat = self.idx.ravel()
-        re = np.bincount(flat, weights=c.real.ravel(), minlength=self.G * self.G)
-        im = np.bincount(flat, weights=c.imag.ravel(), minlength=self.G * self.G)
-        return (re + 1j * im).reshape(self.G, self.G)
+        """g: [npts] or [npts, nz] complex -> grid [G, G] or [G*G, nz] (transpose of gather)."""
+        if g.ndim == 1:
+            return (self.ST @ g).reshape(self.G, self.G)
+        return self._apply(self.ST, np.ascontiguousarray(g))
 
 
 class RadonUSFFT:
@@ -175,13 +196,11 @@ class RadonUSFFT:
         fde[:, N // 2:N // 2 + N, N // 2:N // 2 + N] = fp / self._phi / (4 * N * N)  # divphi
         chk = checker(G)
         fde *= chk                                            # fftshiftc
-        F = np.fft.fft2(fde, axes=(-2, -1))                   # cufft fwd 2-D
+        F = sfft.fft2(fde, axes=(-2, -1), workers=WORKERS)    # cufft fwd 2-D
         F *= chk                                              # fftshiftc on the haloed grid
-        g = np.empty((self.ntheta, nz, N), np.complex128)
-        for z in range(nz):
-            g[:, z, :] = self._taps.gather(F[z]).reshape(self.ntheta, N) / N
+        g = (self._taps.gather(F) / N).reshape(self.ntheta, N, nz).transpose(0, 2, 1)
         s1 = checker1(N)
-        g = np.fft.ifft(g * s1, axis=-1) * N * s1             # fftshift1c, 1-D inverse, fftshift1c
+        g = sfft.ifft(g * s1, axis=-1, workers=WORKERS) * N * s1   # fftshift1c, 1-D inverse, fftshift1c
         return g[:, :, c0:c0 + n]
 
     # ---- adjoint: radonusfft.cu:94-139 ------------------------------------
@@ -192,15 +211,13 @@ class RadonUSFFT:
         idx = np.clip(np.arange(N), c0, 5 * N // 6 - 1) - c0   # pad (kernels.cuh:189)
         gl = g.astype(np.complex128)[:, :, idx]
         s1 = checker1(N)
-        gl = np.fft.fft(gl * s1, axis=-1) * s1                 # fftshift1c, 1-D fwd, fftshift1c
+        gl = sfft.fft(gl * s1, axis=-1, workers=WORKERS) * s1  # fftshift1c, 1-D fwd, fftshift1c
         chk = checker(G)
-        out = np.empty((nz, n, n), np.complex128)
-        for z in range(nz):
-            F = self._taps.scatter(gl[:, z, :].ravel() / N)     # scatter + wrapadj
-            F *= chk                                           # fftshiftc on haloed grid
-            fde = np.fft.ifft2(F) * (G * G)                    # cufft inverse 2-D
-            fde *= chk                                         # fftshiftc
-            fc = fde[N // 2:N // 2 + N, N // 2:N // 2 + N] / self._phi / (4 * N * N)
-            fc = fc * self._mask                               # circ
-            out[z] = fc[c0:c0 + n, c0:c0 + n]
-        return out
+        pts = np.ascontiguousarray(gl.transpose(0, 2, 1).reshape(self.ntheta * N, nz)) / N
+        F = self._taps.scatter(pts).T.reshape(nz, G, G)         # scatter + wrapadj
+        F *= chk                                               # fftshiftc on haloed grid
+        fde = sfft.ifft2(F, axes=(-2, -1), workers=WORKERS) * (G * G)   # cufft inverse 2-D
+        fde *= chk                                             # fftshiftc
+        fc = fde[:, N // 2:N // 2 + N, N // 2:N // 2 + N] / self._phi / (4 * N * N)
+        fc = fc * self._mask                                   # circ
+        return fc[:, c0:c0 + n, c0:c0 + n]

@@ -642,34 +642,79 @@ extern "C" int pt_abs2_c64(float *out, const void *x, size_t n, float scale, voi
 // Scratch of the reduction (one FP64 partial per block and step length) in a
 // file-scope device array: 1184 blocks x 16 step lengths x 8 B = 148 KiB, held
 // by every GPU that loads this library until the process exits.  Host code
-// cannot use the array's name as a device address, so its address is looked
-// up once per device with cudaGetSymbolAddress and cached.
+// cannot use the array's name as a device address; cudaGetSymbolAddress gives
+// the address in the calling thread's current context.  That address belongs
+// to the context, not to the device: after cudaDeviceReset the module is
+// loaded again (and may move), and a caller's own driver-API context on the
+// same device holds a separate copy.  So the address is cached together with
+// the unique id of the context it was looked up in (cuCtxGetId, reached
+// through cudaGetDriverEntryPointByVersion so that the library needs no link
+// to the driver), and looked up again whenever the current context differs.
+// Devices past the cache, or a driver without context ids, look it up on
+// every call.
 #include <mutex>
 
 namespace {
 static __device__ __align__(256) double g_ls_scratch[RB * MAXK];
 
-constexpr int MAX_DEVICES = 64;
-double *g_ls_scratch_ptr[MAX_DEVICES] = {};
+constexpr int MAX_CACHED_DEVICES = 64;
+struct ScratchSlot {
+    unsigned long long ctx_id;   // 0: nothing cached
+    double *ptr;
+};
+ScratchSlot g_ls_scratch_slot[MAX_CACHED_DEVICES] = {};
 std::mutex g_ls_scratch_mu;
 
-int ls_scratch_for_current_device(double **ptr)
+typedef int (*ctx_get_current_fn)(void **ctx);
+typedef int (*ctx_get_id_fn)(void *ctx, unsigned long long *id);
+
+// Unique id of the calling thread's current CUDA context; 0 when there is
+// none yet or the driver cannot report it.
+unsigned long long current_context_id()
+{
+    static ctx_get_current_fn get_current = nullptr;
+    static ctx_get_id_fn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &a, 12000, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &b, 12000, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess) {
+            get_current = (ctx_get_current_fn)a;
+            get_id = (ctx_get_id_fn)b;
+        }
+        cudaGetLastError();   // a failed query leaves no sticky error behind
+    });
+    if (!get_current || !get_id) return 0;
+    void *ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+int ls_scratch_for_current_context(double **ptr)
 {
     int dev = -1;
     PT_CUDA(cudaGetDevice(&dev));
-    PT_CHECK_ARG(dev >= 0 && dev < MAX_DEVICES, "ls_frames_noalloc: device ordinal %d out of range", dev);
+    const bool cached = dev >= 0 && dev < MAX_CACHED_DEVICES;
     std::lock_guard<std::mutex> lock(g_ls_scratch_mu);
-    if (!g_ls_scratch_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_ls_scratch);
-        if (e != cudaSuccess || !p) {
-            pt::set_error("ls_frames_noalloc: cudaGetSymbolAddress of the static scratch failed on device %d: %s",
-                          dev, cudaGetErrorString(e));
-            return PT_ERR_CUDA;
-        }
-        g_ls_scratch_ptr[dev] = (double *)p;
+    unsigned long long id = current_context_id();
+    if (cached && id != 0 && g_ls_scratch_slot[dev].ctx_id == id) {
+        *ptr = g_ls_scratch_slot[dev].ptr;
+        return PT_OK;
     }
-    *ptr = g_ls_scratch_ptr[dev];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_ls_scratch);
+    if (e != cudaSuccess || !p) {
+        pt::set_error("ls_frames_noalloc: cudaGetSymbolAddress of the static scratch failed on device %d: %s", dev,
+                      cudaGetErrorString(e));
+        return PT_ERR_CUDA;
+    }
+    id = current_context_id();   // the look-up may have created the context
+    if (cached) g_ls_scratch_slot[dev] = ScratchSlot{id, (double *)p};
+    *ptr = (double *)p;
     return PT_OK;
 }
 }  // namespace
@@ -683,7 +728,7 @@ extern "C" int pt_ls_frames_noalloc(const void *f, const void *d, const float *d
                  "ls_frames_noalloc: J = %d step lengths exceeds the static scratch (1 <= J <= %d)", J, MAXK);
     PT_CHECK_ARG(model == 0 || model == 1, "ls_frames_noalloc: model 0 (poisson) or 1 (gaussian)");
     double *work = nullptr;
-    const int rc = ls_scratch_for_current_device(&work);
+    const int rc = ls_scratch_for_current_context(&work);
     if (rc != PT_OK) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     // every partial that k_finish reads (J x nblk) is written by k_ls_frames in

@@ -1,11 +1,11 @@
 """Golden vectors for the scan and probe generators, from the reference itself.
 
 Loads the reference's src/ptychotomo/objects.py (it needs only NumPy) from
-/root/reference and stores probe(...) and scanner3(...) outputs for a few
+the reference source tree given on the command line and stores probe(...) and scanner3(...) outputs for a few
 argument sets; the random-scan cases seed NumPy's global generator first,
 as a caller of scanner3(randscan=True) would.
 
-    python tests/golden/make_golden_objects.py [REFERENCE_ROOT]
+    python tests/golden/make_golden_objects.py REFERENCE_ROOT
 """
 from __future__ import annotations
 
@@ -38,4 +38,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(__doc__)
+    main(sys.argv[1])

@@ -53,6 +53,28 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls():
         np.testing.assert_allclose(o, r, rtol=1e-12, atol=0)
 
 
+def test_noalloc_call_allocates_no_device_memory():
+    """After a first call (which loads the module and looks up the scratch),
+    a further call leaves the device's free memory unchanged."""
+    lib = _lib.lib()
+    n = 4096
+    f, d, data = _inputs(n, 7)
+    gam = torch.tensor([1.0, 0.5, 0.25], dtype=torch.float64, device="cuda")
+    out = torch.empty(3, dtype=torch.float64, device="cuda")
+
+    def call():
+        rc = lib.pt_ls_frames_noalloc(f.data_ptr(), d.data_ptr(), data.data_ptr(), 1.0, n, 0, gam.data_ptr(), 3,
+                                      out.data_ptr(), None)
+        assert rc == 0, _lib.last_error()
+        torch.cuda.synchronize()
+
+    call()
+    free0, _ = torch.cuda.mem_get_info()
+    call()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+
+
 def test_noalloc_rejects_more_step_lengths_than_its_scratch_holds():
     lib = _lib.lib()
     n = 1024
