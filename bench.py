@@ -20,6 +20,8 @@ Pass-model algorithmic bytes per call (complex64 = 8 B):
     python bench.py --cg-kernels  # the ptycho CG's frame kernels at the operator workload
     python bench.py --precision   # operator errors vs direct sums, reconstruction errors
     python bench.py --uneven      # uneven scans: one launch for all angles vs one per angle
+    python bench.py --precond     # learned preconditioner of the tomography CG (360 angles, missing wedge)
+    python bench.py --time-to-target   # time to the plain ADMM's reconstruction: plain vs graph-captured variants
 
 ``--impl reference`` times the reference's operators: by default the CPU
 restatement of the reference (oracle/, all host cores, a bounded sample of
@@ -73,20 +75,26 @@ def config_dict(c, extra=None):
     return d
 
 
-def dram_traffic(op):
-    """DRAM bytes (read + write) per call of `op` from the committed ncu summary
-    profiles/dram_traffic_bench_256cubed.md (rows `| op | bytes | ... |`)."""
-    path = ROOT / "profiles" / "dram_traffic_bench_256cubed.md"
-    if not path.exists():
+# DRAM bytes (read + write) of the ptycho adjoint kernel k_ptycho_adj128 per
+# 128^2 detector frame, from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum, one launch, --clock-control none) of
+#   python bench.py --ntheta 148 --steps 1 --warmup 1 --no-e2e --no-cpu-baseline
+# at 256^3: 3,691,507,712 + 500,559,104 bytes for 148 x 169 = 25,012 frames.
+# 148 angles are one wave of one-slab angle blocks, the per-wave layout of the
+# 384-angle workload, so the figure is scaled by the frame count of the run.
+PTYCHO_ADJ128_DRAM_PER_FRAME = (3691507712 + 500559104) / 25012
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_ptycho_adj128 launch at 148 angles "
+                  "(25,012 frames of 128^2, 256^3 object): %.0f B per frame, scaled by this run's frames"
+                  % PTYCHO_ADJ128_DRAM_PER_FRAME)
+
+
+def dram_traffic(c):
+    """DRAM bytes per ptycho-adjoint call, scaled from the per-frame capture;
+    None where the capture does not apply (other detector, probe or object
+    sizes, or fewer angles than SMs, where the angles are split into parts)."""
+    if (c["det"], c["nprb"], c["n"], c["nz"]) != (128, 128, 256, 256) or c["ntheta"] < 148:
         return None
-    for line in path.read_text().splitlines():
-        cells = [c.strip() for c in line.strip().strip("|").split("|")]
-        if len(cells) >= 2 and cells[0] == op:
-            try:
-                return int(float(cells[1]))
-            except ValueError:
-                return None
-    return None
+    return int(round(PTYCHO_ADJ128_DRAM_PER_FRAME * c["ntheta"] * c["nside"] ** 2))
 
 
 # ----------------------------------------------------------------------------
@@ -338,9 +346,10 @@ def run_ours(args, rank, world, local):
     # short slab reduction); the radon operators are sequences of short
     # launches (4 per 8-slice chunk forward), each far below either ptycho
     # kernel, so their rates are in per_op_gbs only
-    dom = max(("ptycho_fwd", "ptycho_adj"), key=per_op.get)
+    # the ptycho adjoint (k_ptycho_adj128): the largest single kernel of the step
+    dom = "ptycho_adj"
     achieved = bytes_op[dom] / (per_op[dom] * 1e-3) / 1e9
-    traffic = dram_traffic(dom)
+    traffic = dram_traffic(c)
 
     line = {"metric": "operator HBM GB/s (radonusfft fwd+adj + ptychofft fwd+adj, 256^3)",
             "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -355,6 +364,7 @@ def run_ours(args, rank, world, local):
             "gpu_launches": ops.launches_per_step() * args.steps,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "traffic_source": TRAFFIC_SOURCE if traffic is not None else None,
                          "peak_source": peak_src + " hbm_gbs (copy, burst)"},
             "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -837,6 +847,230 @@ def run_uneven(args, local):
             "ms_per_cg_iteration": out, "speedup": round(out["per_angle"] / out["batched"], 2)}
 
 
+# ---- learned preconditioner of the tomography CG ------------------------------
+# 256^3, 360 angles on [-60, 60) degrees (a 60-degree missing wedge), seeded
+# ellipsoid phantoms: 64 training and 16 held-out seeds (8-slice volumes for
+# the training targets; the symbol is per slice), the 3->64->64->1 network
+# trained on the GPU; then the tomography subproblem of cg_tomo on a held-out
+# 256^3 phantom (K = 1, xi0 = R u, xi1 = 0, rho = 0.5) solved to a 1e-4
+# gradient reduction by plain CG and by PCG with the analytic ramp symbol and
+# with the learned symbol.
+PRECOND = dict(n=256, nz=256, ntheta=360, lo=-np.pi / 3, hi=np.pi / 3, train=64, held=16, harvest_nz=8,
+               cg_iters=4, steps=1500, tol=1e-4, max_iter=400)
+
+
+def _precond_setup(c, torch, dev, nz):
+    from ptychotomo_b200 import Solver, synthetic
+    theta = synthetic.angles(c["ntheta"], c["lo"], c["hi"])
+    prb = synthetic.probe(16, seed=1)
+    scan = synthetic.raster_scan(c["ntheta"], 2, c["n"], nz, 16)
+    slv = Solver(prb, scan, theta, [16, 16], 1e-6, 5.0, c["ntheta"], nz, c["n"], c["ntheta"], nz, device=dev)
+    return slv, torch.from_numpy(theta).to(dev)
+
+
+def run_precond(args, local):
+    import torch
+    from ptychotomo_b200 import synthetic
+    from ptychotomo_b200.learned import FourierPreconditioner, harvest_targets, train_network
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    c = dict(PRECOND)
+    n = c["n"]
+    # training targets from plain CG runs on 8-slice volumes
+    hs, th = _precond_setup(c, torch, dev, c["harvest_nz"])
+    hpre = FourierPreconditioner(hs._tomo_all, th, hs.coeftomo, dev)
+    vols = (torch.from_numpy(synthetic.phantom(n, c["harvest_nz"], seed=1000 + s) * 1e5).to(dev)
+            for s in range(c["train"] + c["held"]))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tg = harvest_targets(hs._tomo_all, hpre, vols, cg_iters=c["cg_iters"], seed=11)
+    torch.cuda.synchronize()
+    t_harvest = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    net, hist, train_loss, held = train_network(hpre.x, tg[:c["train"]], tg[c["train"]:], steps=c["steps"],
+                                                lr=1e-2, lr_final=1e-3, seed=0)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    del hs, hpre, tg
+    torch.cuda.empty_cache()
+    # the subproblem at 256^3
+    slv, th = _precond_setup(c, torch, dev, c["nz"])
+    pre = FourierPreconditioner(slv._tomo_all, th, slv.coeftomo, dev)
+    u = torch.from_numpy(synthetic.phantom(n, c["nz"], seed=5000) * 1e5).to(dev)
+    xi0 = slv.fwd_tomo_batch(u)
+    Kt = torch.ones_like(xi0)
+    xi1 = torch.zeros((3, c["nz"], n, n), dtype=torch.complex64, device=dev)
+    u0 = torch.zeros_like(u)
+    _, dI = pre.diag()
+    k = np.fft.fftfreq(n)
+    r = np.hypot(k[None, :], k[:, None])
+    ramp = 1.0 / np.maximum(r, 1.0 / n)
+    ramp_log = torch.from_numpy(np.log(ramp * dI / ramp.mean()).astype(np.float32)).to(dev)
+    out = {}
+    for tau in (0.5, 0.05):
+        row = {}
+        for label in ("plain", "ramp", "learned"):
+            if label == "ramp":
+                pre.set_log_symbol(ramp_log)
+            elif label == "learned":
+                pre.set_network(net)
+            P = None if label == "plain" else pre
+            slv.pcg_tomo(xi0, xi1, Kt, u0, 0.5, tau, 2, P)      # warm-up
+            torch.cuda.synchronize()
+            hist_g = []
+            t0 = time.perf_counter()
+            slv.pcg_tomo(xi0, xi1, Kt, u0, 0.5, tau, c["max_iter"], P, tol=c["tol"], history=hist_g)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            reached = hist_g[-1] <= c["tol"]
+            row[label] = {"iterations": len(hist_g) - 1 if reached else None, "seconds": round(dt, 3),
+                          "final_reduction": float("%.3g" % hist_g[-1])}
+        out["tau_%g" % tau] = row
+    return {"metric": "tomography CG iterations and wall time to a 1e-4 gradient reduction, 256^3, 360 angles on "
+                      "[-60, 60) degrees", "unit": "iterations / s", "n_gpus": 1, "higher_is_better": False,
+            "data": "synthetic", "dtype": "c64 (fp32 complex); network bf16 weights, FP32 accumulation",
+            "config": {"workload": json.dumps({k: (round(v, 6) if isinstance(v, float) else v) for k, v in c.items()})},
+            "training": {"harvest_s": round(t_harvest, 2), "train_s": round(t_train, 2), "steps": c["steps"],
+                         "loss_first": hist[0][1], "train_loss": train_loss, "held_out_loss": held},
+            "subproblem": out}
+
+
+# ---- time to the plain method's reconstruction ---------------------------------
+# The operator workload's geometry (256^3, 384 angles on [0, pi), 13x13 scans,
+# 128^2 probe and detector), Poisson counts.  Plain: the drop-in Solver.admm
+# (the reference's algorithm, host-driven, FP32 with FP64 reductions) for
+# `iters` iterations; its last iterate is the target.  Variants: the same
+# algorithm with device-resident scalars and the steady iteration replayed as
+# a CUDA graph, without and with the learned preconditioner in the
+# tomography CG.  Each variant's time to rel-L2 <= 1e-3 of the target on
+# delta = -Re u and beta = Im u is the wall time of its iterations up to the
+# first that gets there (device-synchronised after every iteration).
+TTT = dict(n=256, nz=256, ntheta=384, nprb=128, det=128, nside=13, step=None, photons=1e3, alpha=1e-3, piter=4,
+           titer=4, voxel=1e-6, energy=5.0, iters=60, tol=1e-3)
+
+
+def _rel_parts(u, ref):
+    import torch
+    n = torch.linalg.vector_norm
+    return float(n(u.real - ref.real) / n(ref.real)), float(n(u.imag - ref.imag) / n(ref.imag))
+
+
+def run_time_to_target(args, local):
+    import torch
+    from ptychotomo_b200.graphed import GraphedADMM
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    c = dict(TTT)
+    if args.ttt_iters:
+        c["iters"] = args.ttt_iters
+    if args.ttt_size:
+        c.update(n=args.ttt_size, nz=args.ttt_size)
+    if args.ttt_alpha is not None:
+        c["alpha"] = args.ttt_alpha
+    if args.ttt_photons is not None:
+        c["photons"] = args.ttt_photons
+    slv, data, u_true = _admm_problem(c, torch, dev)
+    data = slv._as_data(data)
+    nt, nz, n = c["ntheta"], c["nz"], c["n"]
+    cx = dict(dtype=torch.complex64, device=dev)
+
+    def init():
+        one = torch.ones((nt, nz, n), **cx)
+        z3 = torch.zeros((3, nz, n, n), **cx)
+        return dict(u=torch.zeros((nz, n, n), **cx), psi=one.clone(), h=one.clone(), e=z3.clone(), phi=z3.clone(),
+                    lamd=torch.zeros_like(one), mu=z3.clone())
+
+    def plain_run():
+        st, rho, tau = init(), 0.5, 0.5
+        us, ts = [], []
+        t = 0.0
+        for m in range(c["iters"]):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st, rho, tau = slv.admm_step(m, st, rho, tau, data, c["alpha"], c["piter"], c["titer"], "poisson")
+            torch.cuda.synchronize()
+            t += time.perf_counter() - t0
+            us.append(st["u"].clone())
+            ts.append(t)
+        return us, ts
+
+    def graphed_run(pre):
+        g = GraphedADMM(slv, data, c["alpha"], c["piter"], c["titer"], "poisson", precond=pre)
+        st = init()
+        g.load(st, 0.5, 0.5)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g.capture()            # set-up, counted in the wall time
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        us, ts = [], []
+        for m in range(c["iters"]):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if m < 2:
+                g.step(m)
+            else:
+                g.replay()
+            torch.cuda.synchronize()
+            t += time.perf_counter() - t0
+            us.append(g.u.clone())
+            ts.append(t)
+        return us, ts
+
+    plain_run()   # warm-up (library state, allocator)
+    us_p, ts_p = plain_run()
+    ref = us_p[-1]
+    out = {}
+
+    def reach(us, ts):
+        for m, (u, t) in enumerate(zip(us, ts)):
+            ed, eb = _rel_parts(u, ref)
+            if max(ed, eb) <= c["tol"]:
+                return {"iteration": m, "seconds": round(t, 3)}
+        ed, eb = _rel_parts(us[-1], ref)
+        return {"iteration": None, "seconds": None, "final_rel_delta": float("%.3g" % ed),
+                "final_rel_beta": float("%.3g" % eb)}
+
+    out["plain"] = dict(reach(us_p, ts_p), ms_per_iteration_steady=round(1e3 * (ts_p[-1] - ts_p[2]) / max(len(ts_p) - 3, 1), 2))
+    del us_p
+    us_g, ts_g = graphed_run(None)
+    out["graphed"] = dict(reach(us_g, ts_g), ms_per_iteration_steady=round(1e3 * (ts_g[-1] - ts_g[2]) / max(len(ts_g) - 3, 1), 2))
+    del us_g
+    torch.cuda.empty_cache()
+    if not args.ttt_no_precond:
+        from ptychotomo_b200 import synthetic
+        from ptychotomo_b200.learned import FourierPreconditioner, harvest_targets, train_network
+        t0 = time.perf_counter()
+        pre = FourierPreconditioner(slv._tomo_all, slv.theta, slv.coeftomo, dev)
+        vols = (torch.from_numpy(synthetic.phantom(n, 8, seed=2000 + s) * 1e5).to(dev) for s in range(16))
+        hs = _precond_harvest_solver(slv, dev)
+        hpre = FourierPreconditioner(hs._tomo_all, slv.theta, hs.coeftomo, dev)
+        tg = harvest_targets(hs._tomo_all, hpre, vols, cg_iters=4, seed=5)
+        net, _, _, _ = train_network(hpre.x, tg, [], steps=1000, lr=1e-2, lr_final=1e-3)
+        pre.set_network(net)
+        torch.cuda.synchronize()
+        t_setup = time.perf_counter() - t0
+        del hs, hpre, tg
+        us_q, ts_q = graphed_run(pre)
+        out["graphed_learned_pcg"] = dict(reach(us_q, ts_q), preconditioner_setup_s=round(t_setup, 2),
+                                          ms_per_iteration_steady=round(1e3 * (ts_q[-1] - ts_q[2]) / max(len(ts_q) - 3, 1), 2))
+    ratios = {k: (round(out["plain"]["seconds"] / v["seconds"], 2) if v.get("seconds") and out["plain"].get("seconds")
+                  else None) for k, v in out.items() if k != "plain"}
+    cfg = {k: (v if not isinstance(v, float) else float("%.6g" % v)) for k, v in c.items()}
+    return {"metric": "time to rel-L2 <= 1e-3 of the plain FP32 ADMM reconstruction (delta and beta)", "unit": "s",
+            "n_gpus": 1, "higher_is_better": False, "data": "synthetic", "dtype": "c64 (fp32 complex), FP64 reductions",
+            "config": {"workload": "Poisson ADMM " + json.dumps(cfg)}, "variants": out, "speedup_vs_plain": ratios}
+
+
+def _precond_harvest_solver(slv, dev):
+    """A Solver with the same angles and width on 8 slices (training targets)."""
+    from ptychotomo_b200 import Solver, synthetic
+    theta = slv.theta.cpu().numpy()
+    nt, n = len(theta), slv.n
+    return Solver(synthetic.probe(16, seed=1), synthetic.raster_scan(nt, 2, n, 8, 16), theta, [16, 16], slv.voxelsize,
+                  slv.energy, nt, 8, n, nt, 8, device=dev)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -852,6 +1086,13 @@ def main():
     ap.add_argument("--cg-kernels", action="store_true", help="device time of the ptycho CG's frame kernels")
     ap.add_argument("--precision", action="store_true", help="operator and reconstruction errors")
     ap.add_argument("--uneven", action="store_true", help="uneven scans: batched vs per-angle launches")
+    ap.add_argument("--precond", action="store_true", help="learned preconditioner of the tomography CG")
+    ap.add_argument("--time-to-target", action="store_true", help="time to the plain ADMM's reconstruction")
+    ap.add_argument("--ttt-iters", type=int, default=None)
+    ap.add_argument("--ttt-size", type=int, default=None)
+    ap.add_argument("--ttt-alpha", type=float, default=None)
+    ap.add_argument("--ttt-photons", type=float, default=None)
+    ap.add_argument("--ttt-no-precond", action="store_true")
     args = ap.parse_args()
     if args.ntheta:
         CFG["ntheta"] = args.ntheta
@@ -860,10 +1101,11 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
-    if args.admm or args.cg_kernels or args.precision or args.uneven:
+    if args.admm or args.cg_kernels or args.precision or args.uneven or args.precond or args.time_to_target:
         if rank == 0:
             fn = (run_admm if args.admm else run_cg_kernels if args.cg_kernels else
-                  run_precision if args.precision else run_uneven)
+                  run_precision if args.precision else run_precond if args.precond else
+                  run_time_to_target if args.time_to_target else run_uneven)
             print(json.dumps(fn(args, local)), flush=True)
         return 0
     if args.impl == "reference":

@@ -68,6 +68,21 @@ int pt_radon_adj(pt_radon *h, void *f, const void *g, void *stream);
  * (Solver.fwd_tomo/adj_tomo apply coeftomo this way, solver.py:67-80). */
 int pt_radon_fwd_scaled(pt_radon *h, void *g, const void *f, float scale, void *stream);
 int pt_radon_adj_scaled(pt_radon *h, void *f, const void *g, float scale, void *stream);
+/* The exact adjoint of pt_radon_fwd, f = scale * R^T g (no counterpart in the
+ * reference).  The reference's adjoint replicates the edge samples of each
+ * detector line and crops the padded slice, so it equals R^T only where g
+ * and the result vanish on their borders (radonusfft.cu:94-139,
+ * kernels.cuh:189-216); here the lines are zero-padded (the adjoint of the
+ * forward's crop) and the padded slice is folded onto its edge pixels (the
+ * adjoint of the forward's edge replication).  Used by the preconditioned
+ * tomography CG, which needs the true gradient of its quadratic. */
+int pt_radon_adj_exact(pt_radon *h, void *f, const void *g, float scale, void *stream);
+/* Autotuner (no counterpart in the reference): times the forward with its
+ * 8-slice chunks on the caller's stream alone and pipelined on two streams
+ * (one chunk's FFTs under the previous chunk's gather), `trials` runs each
+ * after a warm-up, and keeps the faster for this handle.  g, f: caller
+ * buffers of the forward's shapes (overwritten).  Blocks the host. */
+int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials, int *streams_out, void *stream);
 /* Internal parameters: N, kernel half-width M, mu. */
 int pt_radon_get_params(const pt_radon *h, int *N, int *M, float *mu);
 /* Copies the polar coordinate tables x, y (device float[Ntheta][N] each). */
@@ -118,6 +133,15 @@ int pt_ptycho_adj_probe(pt_ptycho *h, void *gprb, const void *g, const void *psi
 int pt_ptycho_adj_probe_resid(pt_ptycho *h, void *gprb, const void *psi, const void *fpsi, const float *data,
                               float dscale, int model, float scale, void *stream);
 int pt_ptycho_fwd_probe(pt_ptycho *h, void *g, const void *psi, const void *prb, float scale, void *stream);
+/* Autotuner (no counterpart in the reference): the adjoint splits each
+ * angle's scans over `parts` blocks (own slabs, then a fixed-order sum);
+ * times the adjoint for parts in {1, 2, 3, 4, 6, 8, 12, 16} (<= Nscan),
+ * `trials` runs each after a warm-up, and keeps the fastest (default: a
+ * wave-count model).  f, g: caller buffers of the adjoint's shapes (f is
+ * overwritten).  Allocates the slabs; blocks the host. */
+int pt_ptycho_autotune(pt_ptycho *h, void *f, const void *g, int trials, int *parts_out, void *stream);
+/* The adjoint's current split. */
+int pt_ptycho_get_parts(const pt_ptycho *h, int *parts);
 
 
 /* ---- Solver arithmetic (src/ptychotomo/solver.py:48-336) -----------------
@@ -187,9 +211,137 @@ int pt_takexi_c64(void *K, void *xi0, const void *t, size_t n, float inv_tmax, f
  * u [nz][ny][nx], res/g [3][nz][ny][nx], scaled by s (2/sqrt(3), -2/sqrt(3)). */
 int pt_reg_fwd_c64(void *res, const void *u, int nz, int ny, int nx, float s, void *stream);
 int pt_reg_adj_c64(void *res, const void *g, int nz, int ny, int nx, float s, void *stream);
+/* Zeroes the components of g [3][nz][ny][nx] that no forward difference of J
+ * produces (x = nx-1 in component 0, y = ny-1 in 1, z = nz-1 in 2), so that
+ * pt_reg_adj_c64 of the result is the exact adjoint J^T (no counterpart in
+ * the reference: its adj_reg also reads those entries, solver.py:137-146). */
+int pt_reg_mask_c64(void *g, int nz, int ny, int nx, void *stream);
 /* solve_reg, solver.py:257-264: z = soft(J u + mu/tau, thr), isotropic over the 3 components. */
 int pt_solve_reg_c64(void *z, const void *u, const void *mu, int nz, int ny, int nx, float s, float inv_tau,
                      float thr, void *stream);
+
+/* ---- learned Fourier preconditioner of the tomography CG -----------------
+ * No counterpart in the reference: its tomography CG (solver.py:180-203) is
+ * unpreconditioned.  A 3 -> 64 -> 64 -> 1 MLP with SiLU activations maps the
+ * features of a Fourier frequency to the log of a positive filter value.
+ * Parameters: one FP32 vector of pt_mlp_param_count() values, W1 [64][3],
+ * b1 [64], W2 [64][64], b2 [64], W3 [64], b3.  bf16 != 0: the kernels round
+ * the weights (not the biases) to bfloat16, round-to-nearest-even, before
+ * their FP32 arithmetic. */
+int pt_mlp_param_count(void);
+/* Bytes of the workspace pt_mlp_grad needs. */
+size_t pt_mlp_workspace_bytes(void);
+/* z[p] = MLP(x[p][0..2]) for p < npts. */
+int pt_mlp_forward(const float *params, int bf16, const float *x, float *z, size_t npts, void *stream);
+/* Least-squares loss inv_wsum * sum_p w[p] (z[p] - y[p])^2 into *loss (device
+ * double) and its gradient with respect to the parameters into grad
+ * (device float[param_count]).  Deterministic: fixed per-block tiles, fixed
+ * block order. */
+int pt_mlp_grad(const float *params, int bf16, const float *x, const float *y, const float *w, size_t npts,
+                float inv_wsum, float *grad, double *loss, void *work, void *stream);
+/* One Adam step (bias-corrected, step >= 1) on the FP32 parameters. */
+int pt_mlp_adam(float *params, float *m, float *v, const float *grad, int step, float lr, float beta1, float beta2,
+                float eps, void *stream);
+
+/* The preconditioner P = D^-1/2 F2^-1 diag(p) F2 D^-1/2 of the tomography CG
+ * on volumes [nz][n][n] (F2: the 2-D DFT of each slice), with D the diagonal
+ * of rho kbar R^T R + tau J^T J and, in the interior,
+ * p(w) = (rho kbar dI + tau dJI) / (rho kbar a(w) + tau j(w)): a(w) the
+ * (learned) symbol of R^T R, j(w) the TV symbol.  n in {16 .. 512}, powers
+ * of two.  The handle owns its scratch (two volumes); apply allocates
+ * nothing. */
+typedef struct pt_precond pt_precond;
+int pt_precond_create(size_t nz, size_t n, pt_precond **out);
+int pt_precond_destroy(pt_precond *h);
+/* Features of every frequency of an n x n slice, x[(ky n + kx)][3] in DFT
+ * order: |w| / (n/2); the angular sampling density at the direction of w
+ * (measured Fourier lines within +-3 degrees over the count for ntheta
+ * uniform angles); the angle to the nearest measured line over pi/2 (the
+ * missing-wedge extent).  theta: device float[ntheta]. */
+int pt_precond_features(const float *theta, int ntheta, int n, float *x, void *stream);
+/* log_a: device float[n][n], the log of the symbol of R^T R in DFT order
+ * (the network's output); the handle keeps a = exp(log_a). */
+int pt_precond_set_log_symbol(pt_precond *h, const float *log_a, void *stream);
+/* Copies the symbol a (device float[n][n]). */
+int pt_precond_get_symbol(const pt_precond *h, float *a, void *stream);
+/* The diagonal of (scale R)^T (scale R) from the radon operator r (same n):
+ * exact for the edge pixels and one interior pixel (every other pixel takes
+ * its value).  Runs forwards of unit pixels; allocates; blocks the host. */
+int pt_precond_set_diag(pt_precond *h, pt_radon *r, float scale, void *stream);
+/* Copies the diagonal (device float[n][n]) and its interior value (host). */
+int pt_precond_get_diag(const pt_precond *h, float *dR, float *dI, void *stream);
+/* out = P in (out may alias in); rho_kbar = rho * mean |K|^2 > 0, tau >= 0. */
+int pt_precond_apply(pt_precond *h, void *out, const void *in, float rho_kbar, float tau, void *stream);
+/* num[k] += sum over slices of Re(conj(Z[k]) AZ[k]), den[k] += |Z[k]|^2 with
+ * Z = F2 z, AZ = F2 az (device double[n][n] each): the statistics of the
+ * per-frequency Rayleigh quotients that train the network. */
+int pt_precond_spectrum(pt_precond *h, double *num, double *den, const void *z, const void *az, void *stream);
+/* Training targets from the accumulated statistics: y = log(num / den) and
+ * w = 1 where num / den > 0 and den > den_max_rel * max(den), else 0 (device
+ * float[nn] each).  Reads den back to the host (blocks). */
+int pt_precond_targets(const double *num, const double *den, int nn, double den_max_rel, float *y, float *w,
+                       void *stream);
+/* dst = F2 src (unnormalised forward 2-D DFT of every slice). */
+int pt_precond_dft2(pt_precond *h, void *dst, const void *src, void *stream);
+/* dst = F2^-1(|F2 src| exp(2 pi i u)) with u uniform from a hash of (seed,
+ * index): a probe with src's modulus spectrum and random phases. */
+int pt_precond_phase_probe(pt_precond *h, void *dst, const void *src, unsigned seed, void *stream);
+
+/* ---- device-resident scalars: one ADMM iteration as a CUDA graph ---------
+ * No counterpart in the reference, whose Solver (solver.py:171-336) decides
+ * every step length, Dai-Yuan beta and penalty on the host.  Scalars live in
+ * device doubles; reductions (pt_reduce_c64, pt_ls_frames) write into them,
+ * the pt_scalar_* one-thread kernels apply the reference's rules there, and
+ * the *_dev kernels read them.  Coefficient arrays are (re, im) pairs. */
+/* out = sum_{j<k} coef_j x_j with coef (device double[2k]). */
+int pt_lincomb_dev_c64(void *out, size_t n, int k, const void *const *x, const double *coef, void *stream);
+/* Dai-Yuan beta = g2 / (dg - dg0) (solver.py:194-197; 0 for a zero
+ * denominator or first != 0); coef = (-1, 0, beta) for d <- -g + beta d. */
+int pt_scalar_dy_beta(const double *g2, const double *dg, const double *dg0, int first, double *coef, void *stream);
+/* The tomography line search (solver.py:171-177, minf of :181-184) on the
+ * closed form: c1 = rho q1[1] + tau q2[1], c2 = rho q1[2] + tau q2[2]
+ * (q = quad3 triples), rt = (rho, tau); gamma (in/out) halves while
+ * -(2 gamma c1 + gamma^2 c2) < 0 and gamma > 1e-12; coef = (1, 0, gamma). */
+int pt_scalar_tomo_gamma(const double *q1, const double *q2, const double *rt, double *gamma, double *coef,
+                         void *stream);
+/* gam[j] = gamma 2^-j, j < J <= 16. */
+int pt_scalar_ls_candidates(const double *gamma, int J, double *gam, void *stream);
+/* The ptycho line search over one pass (solver.py:171-177 with minf of
+ * :208-214): the first j with !(data[j] + rho (2 g_j q[1] - g_j^2 q[2]) < 0
+ * and g_j > 1e-12) is taken; none: step 0 and gamma <- g_{J-1} / 2;
+ * coef = (1, 0, step). */
+int pt_scalar_ptycho_gamma(const double *data, const double *gam, int J, const double *quad, const double *rt,
+                           double *gamma, double *coef, void *stream);
+/* takexi's scalars (solver.py:151-166): pshift = (band1 + band2) / (2 cnt),
+ * coef = (e, -e / rho) with e = exp(-i pshift). */
+int pt_scalar_takexi(const double *band1, const double *band2, double cnt, const double *rt, double *pshift,
+                     double *coef, void *stream);
+/* The multiplier updates' coefficients (solver.py:326-327): (1, rho, -rho) and (1, tau, -tau). */
+int pt_scalar_multipliers(const double *rt, double *coef_l, double *coef_m, void *stream);
+/* The penalty update (solver.py:267-282) of rt = (rho, tau) in place from
+ * r1 = ||psi - h||^2, s1 = ||h - h0||^2, r2 = ||phi - e||^2, s2 = ||e - e0||^2. */
+int pt_scalar_penalty(const double *r1, const double *s1, const double *r2, const double *s2, double *rt,
+                      void *stream);
+/* The preconditioned CG's scalars: beta = gz / gz0 (0 on the first
+ * iteration or after a restart), coef = (-1, 0, beta); the exact step
+ * gamma = -c1 / c2 when it descends (else 0 and a restart), coef = (1, 0,
+ * gamma); rk_tau = (rho |K|^2 / count, tau). */
+int pt_scalar_pcg_beta(const double *gz, double *gz0, double *restart, int first, double *coef, void *stream);
+int pt_scalar_pcg_step(const double *q1, const double *q2, const double *rt, double *restart, double *coef,
+                       void *stream);
+int pt_scalar_pcg_rk(const double *k2, double count, const double *rt, double *rk_tau, void *stream);
+/* coef = (a0 [* s0[0]], 0, a1 [* s1[0]], 0) (a null s multiplies by 1). */
+int pt_scalar_coef2(const double *s0, double a0, const double *s1, double a1, double *coef, void *stream);
+/* out = (a / x[0], 0). */
+int pt_scalar_inv(const double *x, double a, double *out, void *stream);
+/* pt_expmap_c64, pt_takexi_c64, pt_solve_reg_c64 and pt_precond_apply with
+ * their scalars read from device memory (phi; max|t|; rt = (rho, tau);
+ * rk_tau). */
+int pt_expmap_dev_c64(void *out, const void *x, size_t n, float s, const double *phi, void *stream);
+int pt_takexi_dev_c64(void *K, void *xi0, const void *t, size_t n, const double *tmax, float cxi, void *stream);
+int pt_solve_reg_dev_c64(void *z, const void *u, const void *mu, int nz, int ny, int nx, float s, const double *rt,
+                         float alpha, void *stream);
+int pt_precond_apply_dev(pt_precond *h, void *out, const void *in, const double *rk_tau, void *stream);
 
 #ifdef __cplusplus
 }

@@ -221,3 +221,31 @@ class RadonUSFFT:
         fc = fde[:, N // 2:N // 2 + N, N // 2:N // 2 + N] / self._phi / (4 * N * N)
         fc = fc * self._mask                                   # circ
         return fc[:, c0:c0 + n, c0:c0 + n]
+
+    # ---- exact adjoint of fwd (no counterpart in the reference) ---------------
+    def adj_exact(self, g):
+        """The exact adjoint of fwd: adj with the edge-replicating pad of the
+        detector lines replaced by the zero padding that is the adjoint of
+        fwd's crop, and the final crop replaced by the fold that is the adjoint
+        of pad2 (every margin pixel of the N x N slice added onto the edge
+        pixel it copies).  Equals adj where g and the result's border vanish."""
+        n, N, G, nz = self.n, self.N, self.G, self.nz
+        g = np.asarray(g).reshape(self.ntheta, nz, n)
+        c0 = N // 6
+        gl = np.zeros((self.ntheta, nz, N), np.complex128)
+        gl[:, :, c0:c0 + n] = g
+        s1 = checker1(N)
+        gl = sfft.fft(gl * s1, axis=-1, workers=WORKERS) * s1
+        chk = checker(G)
+        pts = np.ascontiguousarray(gl.transpose(0, 2, 1).reshape(self.ntheta * N, nz)) / N
+        F = self._taps.scatter(pts).T.reshape(nz, G, G)
+        F *= chk
+        fde = sfft.ifft2(F, axes=(-2, -1), workers=WORKERS) * (G * G)
+        fde *= chk
+        fc = fde[:, N // 2:N // 2 + N, N // 2:N // 2 + N] / self._phi / (4 * N * N)
+        fc = fc * self._mask
+        idx = np.clip(np.arange(N), c0, c0 + n - 1) - c0            # pad2's source index
+        fold = np.zeros((n, N))
+        fold[idx, np.arange(N)] = 1.0                                # fold[i, t] = 1 where t copies i
+        return np.einsum("it,ztu,ju->zij", fold, fc, fold)
+

@@ -50,6 +50,7 @@ SIGNATURES = {
     "pt_radon_adj": (_int, [_vp, _vp, _vp, _vp]),
     "pt_radon_fwd_scaled": (_int, [_vp, _vp, _vp, _f, _vp]),
     "pt_radon_adj_scaled": (_int, [_vp, _vp, _vp, _f, _vp]),
+    "pt_radon_adj_exact": (_int, [_vp, _vp, _vp, _f, _vp]),
     "pt_radon_get_params": (_int, [_vp, ctypes.POINTER(_int), ctypes.POINTER(_int), ctypes.POINTER(_f)]),
     "pt_radon_get_xy": (_int, [_vp, _vp, _vp, _vp]),
     "pt_ptycho_create": (_int, [_sz, _sz, _sz, _sz, _sz, _sz, _sz, _sz, ctypes.POINTER(_vp)]),
@@ -63,6 +64,9 @@ SIGNATURES = {
     "pt_ptycho_adj_probe": (_int, [_vp, _vp, _vp, _vp, _f, _vp]),
     "pt_ptycho_adj_probe_resid": (_int, [_vp, _vp, _vp, _vp, _vp, _f, _int, _f, _vp]),
     "pt_ptycho_fwd_probe": (_int, [_vp, _vp, _vp, _vp, _f, _vp]),
+    "pt_ptycho_autotune": (_int, [_vp, _vp, _vp, _int, ctypes.POINTER(_int), _vp]),
+    "pt_ptycho_get_parts": (_int, [_vp, ctypes.POINTER(_int)]),
+    "pt_radon_autotune": (_int, [_vp, _vp, _vp, _int, ctypes.POINTER(_int), _vp]),
     "pt_reduce_workspace_bytes": (_sz, []),
     "pt_reduce_c64": (_int, [_int, _vp, _vp, _sz, _int, _int, _int, _vp, _vp, _vp]),
     "pt_ls_frames": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp, _int, _vp, _vp, _vp]),
@@ -78,7 +82,42 @@ SIGNATURES = {
     "pt_takexi_c64": (_int, [_vp, _vp, _vp, _sz, _f, _f, _vp]),
     "pt_reg_fwd_c64": (_int, [_vp, _vp, _int, _int, _int, _f, _vp]),
     "pt_reg_adj_c64": (_int, [_vp, _vp, _int, _int, _int, _f, _vp]),
+    "pt_reg_mask_c64": (_int, [_vp, _int, _int, _int, _vp]),
     "pt_solve_reg_c64": (_int, [_vp, _vp, _vp, _int, _int, _int, _f, _f, _f, _vp]),
+    "pt_precond_create": (_int, [_sz, _sz, ctypes.POINTER(_vp)]),
+    "pt_precond_destroy": (_int, [_vp]),
+    "pt_precond_features": (_int, [_vp, _int, _int, _vp, _vp]),
+    "pt_precond_set_log_symbol": (_int, [_vp, _vp, _vp]),
+    "pt_precond_get_symbol": (_int, [_vp, _vp, _vp]),
+    "pt_precond_set_diag": (_int, [_vp, _vp, _f, _vp]),
+    "pt_precond_get_diag": (_int, [_vp, _vp, ctypes.POINTER(_f), _vp]),
+    "pt_precond_apply": (_int, [_vp, _vp, _vp, _f, _f, _vp]),
+    "pt_precond_spectrum": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "pt_precond_dft2": (_int, [_vp, _vp, _vp, _vp]),
+    "pt_precond_targets": (_int, [_vp, _vp, _int, ctypes.c_double, _vp, _vp, _vp]),
+    "pt_precond_phase_probe": (_int, [_vp, _vp, _vp, ctypes.c_uint, _vp]),
+    "pt_precond_apply_dev": (_int, [_vp, _vp, _vp, _vp, _vp]),
+    "pt_lincomb_dev_c64": (_int, [_vp, _sz, _int, ctypes.POINTER(_vp), _vp, _vp]),
+    "pt_scalar_dy_beta": (_int, [_vp, _vp, _vp, _int, _vp, _vp]),
+    "pt_scalar_tomo_gamma": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "pt_scalar_ls_candidates": (_int, [_vp, _int, _vp, _vp]),
+    "pt_scalar_ptycho_gamma": (_int, [_vp, _vp, _int, _vp, _vp, _vp, _vp, _vp]),
+    "pt_scalar_takexi": (_int, [_vp, _vp, ctypes.c_double, _vp, _vp, _vp, _vp]),
+    "pt_scalar_multipliers": (_int, [_vp, _vp, _vp, _vp]),
+    "pt_scalar_penalty": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "pt_scalar_pcg_beta": (_int, [_vp, _vp, _vp, _int, _vp, _vp]),
+    "pt_scalar_pcg_step": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "pt_scalar_pcg_rk": (_int, [_vp, ctypes.c_double, _vp, _vp, _vp]),
+    "pt_scalar_coef2": (_int, [_vp, ctypes.c_double, _vp, ctypes.c_double, _vp, _vp]),
+    "pt_scalar_inv": (_int, [_vp, ctypes.c_double, _vp, _vp]),
+    "pt_expmap_dev_c64": (_int, [_vp, _vp, _sz, _f, _vp, _vp]),
+    "pt_takexi_dev_c64": (_int, [_vp, _vp, _vp, _sz, _vp, _f, _vp]),
+    "pt_solve_reg_dev_c64": (_int, [_vp, _vp, _vp, _int, _int, _int, _f, _vp, _f, _vp]),
+    "pt_mlp_param_count": (_int, []),
+    "pt_mlp_workspace_bytes": (_sz, []),
+    "pt_mlp_forward": (_int, [_vp, _int, _vp, _vp, _sz, _vp]),
+    "pt_mlp_grad": (_int, [_vp, _int, _vp, _vp, _vp, _sz, _f, _vp, _vp, _vp, _vp]),
+    "pt_mlp_adam": (_int, [_vp, _vp, _vp, _vp, _int, _f, _f, _f, _f, _vp]),
 }
 
 _lib = None

@@ -59,6 +59,8 @@ namespace pt {
 // Thread-local last-error text (defined in pt_capi.cu).
 void set_error(const char *fmt, ...);
 void clear_error();
+// Slice count and angle count of a radon operator (pt_radon.cu).
+int radon_dims(const pt_radon *h, int *nz, int *ntheta);
 
 }  // namespace pt
 

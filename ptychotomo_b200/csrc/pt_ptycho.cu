@@ -1388,6 +1388,84 @@ extern "C" int pt_ptycho_fwd(pt_ptycho *h, void *g, const void *f, void *stream)
 {
     return ptycho_call(h, false, g, f, 1.0f, stream);
 }
+// ---- autotuner: the adjoint's angle split ---------------------------------
+// Times the object adjoint (the CG's dominant kernel) for each candidate
+// number of parts per angle and keeps the fastest.  Setup-time: allocates the
+// partial slabs of each candidate, blocks the host.
+extern "C" int pt_ptycho_autotune(pt_ptycho *h, void *f, const void *g, int trials, int *parts_out, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h && f && g && trials >= 1, "ptychofft.autotune: bad arguments");
+    if (h->det < 16) {   // the small-detector kernel has no angle split
+        if (parts_out) *parts_out = h->parts;
+        return PT_OK;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    PT_CUDA(cudaEventCreate(&e0));
+    PT_CUDA(cudaEventCreate(&e1));
+    const int cands[] = {1, 2, 3, 4, 6, 8, 12, 16};
+    int best_p = h->parts;
+    float best_t = 1e30f;
+    int rc = PT_OK;
+    for (int p : cands) {
+        if (p > h->nscan) break;
+        if (h->partial) {
+            cudaFree(h->partial);
+            h->partial = nullptr;
+        }
+        h->parts = p;
+        if (p > 1 && cudaMalloc((void **)&h->partial, (size_t)p * h->ntheta * h->nz * h->n * sizeof(float2)) !=
+                         cudaSuccess) {
+            cudaGetLastError();
+            h->parts = 1;
+            continue;   // this split does not fit: skip it
+        }
+        std::vector<float> ts;
+        for (int k = 0; k <= trials && rc == PT_OK; ++k) {   // the first run warms up
+            cudaEventRecord(e0, st);
+            rc = pt_ptycho_adj(h, f, g, stream);
+            cudaEventRecord(e1, st);
+            if (rc == PT_OK && cudaEventSynchronize(e1) == cudaSuccess && k > 0) {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ts.push_back(ms);
+            }
+        }
+        if (rc != PT_OK) break;
+        std::sort(ts.begin(), ts.end());
+        const float med = ts[ts.size() / 2];
+        if (med < best_t) {
+            best_t = med;
+            best_p = p;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (h->partial) {
+        cudaFree(h->partial);
+        h->partial = nullptr;
+    }
+    h->parts = best_p;
+    if (best_p > 1 &&
+        cudaMalloc((void **)&h->partial, (size_t)best_p * h->ntheta * h->nz * h->n * sizeof(float2)) != cudaSuccess) {
+        cudaGetLastError();
+        h->parts = 1;
+        pt::set_error("ptychofft.autotune: the chosen split's slabs could not be allocated");
+        return PT_ERR_ALLOC;
+    }
+    if (parts_out) *parts_out = h->parts;
+    return rc;
+}
+
+extern "C" int pt_ptycho_get_parts(const pt_ptycho *h, int *parts)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h && parts, "ptychofft: null pointer");
+    *parts = h->parts;
+    return PT_OK;
+}
+
 extern "C" int pt_ptycho_adj(pt_ptycho *h, void *f, const void *g, void *stream)
 {
     return ptycho_call(h, true, f, g, 1.0f, stream);

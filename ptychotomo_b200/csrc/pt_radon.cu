@@ -263,8 +263,10 @@ __global__ void __launch_bounds__(ZC * 32)
 }
 
 // ---- A1: pad (kernels.cuh:189-206) + fftshift1c/FFT/fftshift1c -------------
-// grid (ntheta, nzp / ZC); writes lines[(theta*N + k) * nzp + z]
-template <int N>
+// grid (ntheta, nzp / ZC); writes lines[(theta*N + k) * nzp + z].  ZP: the
+// exact adjoint's zero padding (the adjoint of the forward's crop) instead
+// of the reference's edge replication.
+template <int N, bool ZP = false>
 __global__ void __launch_bounds__(ZC * 32)
     k_adj_lines(const float2 *__restrict__ g, float2 *__restrict__ lines, int nz, int nzp, float pre,
                 const float2 *__restrict__ tw)
@@ -277,7 +279,10 @@ __global__ void __launch_bounds__(ZC * 32)
     float2 *b = sm + f * PITCH;
     for (int k = t; k < N; k += T) {
         float2 v = czero();
-        if (z < nz) v = g[((size_t)th * nz + z) * n + (min(max(k, c0), c1) - c0)];
+        if (z < nz) {
+            if (!ZP) v = g[((size_t)th * nz + z) * n + (min(max(k, c0), c1) - c0)];
+            else if (k >= c0 && k <= c1) v = g[((size_t)th * nz + z) * n + (k - c0)];
+        }
         b[k] = (k & 1) ? v : -1.f * v;
     }
     __syncthreads();
@@ -295,9 +300,11 @@ __global__ void __launch_bounds__(ZC * 32)
 // weights (0 where the window misses a cell), in increasing point order.
 // Lanes 0-15 / 16-31 = 16 slices x 2 entry streams, combined at the end in a
 // fixed order -> deterministic.  Each loaded g value feeds 4 accumulators.
+// ALL: write all N rows of the padded slice (rows N/2 .. N/2 + N - 1 of the
+// grid, for the exact adjoint's fold) instead of the n rows of the crop.
 constexpr int ZQ = 16;
 constexpr int CG = 4;  // cells per group
-template <int G>
+template <int G, bool ALL = false>
 __global__ void __launch_bounds__(ZQ *fft_threads<G>(), (G >= 1024 ? 1 : 2))
     k_adj_colgather(const float2 *__restrict__ lines, float2 *__restrict__ rbuf, const int *__restrict__ goff,
                     const int *__restrict__ gpt, const float4 *__restrict__ gw, const int *__restrict__ col_order,
@@ -381,9 +388,10 @@ __global__ void __launch_bounds__(ZQ *fft_threads<G>(), (G >= 1024 ? 1 : 2))
     __syncthreads();
     const int f = threadIdx.x / T, t = threadIdx.x % T;
     ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
-    for (int e = threadIdx.x; e < n * ZQ; e += blockDim.x) {
+    constexpr int ROWS = ALL ? N : n, YB = ALL ? N / 2 : Y0;
+    for (int e = threadIdx.x; e < ROWS * ZQ; e += blockDim.x) {
         const int r = e / ZQ, q = e % ZQ;
-        rbuf[((size_t)r * G + kx) * nzp + z0 + q] = sm[q * PITCH + Y0 + r];
+        rbuf[((size_t)r * G + kx) * nzp + z0 + q] = sm[q * PITCH + YB + r];
     }
 }
 
@@ -447,6 +455,70 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
     }
 }
 
+
+// ---- exact adjoint: rows of the whole padded slice, then the folds ---------
+// The forward's pad2 replicates the edge pixels of f into the margins of the
+// N x N slice (kernels.cuh:208-216) and its last step crops n of N detector
+// samples; their adjoints are a fold (every margin pixel added onto the edge
+// pixel it copies) and a zero padding.  grid (N, nzp / ZC): input row ty of
+// the padded slice (rbuf row ty, written by the ALL column gather): row
+// inverse FFT, sign, circ / phi / (4 N^2), and the fold along x; a row inside
+// the crop goes to out, a margin row (ty <= c0 or ty >= c0 + n - 1) to its
+// slot of mbuf [n/2 + 2][nz][n] for the fold along y.
+template <int G>
+__global__ void __launch_bounds__(ZC *fft_threads<G>())
+    k_adj_rows_exact(const float2 *__restrict__ rbuf, float2 *__restrict__ out, float2 *__restrict__ mbuf, int nz,
+                     int nzp, const float *__restrict__ fac, float scale, const float2 *__restrict__ tw)
+{
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, c0 = N / 6, PITCH = G + 1;
+    extern __shared__ float2 sm[];
+    const int ty = blockIdx.x, z0 = blockIdx.y * ZC;
+    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    for (int e = threadIdx.x; e < G * ZC; e += blockDim.x) {
+        const int kx = e / ZC, q = e % ZC;
+        sm[q * PITCH + kx] = rbuf[((size_t)ty * G + kx) * nzp + z0 + q];
+    }
+    __syncthreads();
+    ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
+    const int Y = N / 2 + ty;
+    const float *facr = fac + (size_t)ty * N;
+    for (int e = threadIdx.x; e < ZC * n; e += blockDim.x) {
+        const int q = e / n, c = e % n;
+        const int z = z0 + q;
+        if (z >= nz) continue;
+        // columns tx of the padded row that copy pixel c (fixed order)
+        const int lo = c == 0 ? 0 : c0 + c, hi = c == n - 1 ? N - 1 : c0 + c;
+        float2 acc = czero();
+        for (int tx = lo; tx <= hi; ++tx) {
+            const int X = N / 2 + tx;
+            float2 v = sm[q * PITCH + X];
+            if ((X + Y) & 1) v = -1.f * v;
+            acc = acc + __ldg(&facr[tx]) * v;
+        }
+        acc = scale * acc;
+        if (ty > c0 && ty < c0 + n - 1) {
+            out[((size_t)z * n + (ty - c0)) * n + c] = acc;
+        } else {
+            const int slot = ty <= c0 ? ty : (c0 + 1) + (ty - (c0 + n - 1));
+            mbuf[((size_t)slot * nz + z) * n + c] = acc;
+        }
+    }
+}
+
+// out row 0 = sum of margin slots 0..c0, row n-1 = the remaining slots (fixed order)
+__global__ void k_adj_fold_rows(const float2 *__restrict__ mbuf, float2 *__restrict__ out, int nz, int n, int c0,
+                                int nslots)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)nz * n) return;
+    const int z = (int)(i / n), c = (int)(i % n);
+    float2 a = czero(), b = czero();
+    for (int s = 0; s <= c0; ++s) a = a + mbuf[((size_t)s * nz + z) * n + c];
+    for (int s = c0 + 1; s < nslots; ++s) b = b + mbuf[((size_t)s * nz + z) * n + c];
+    out[((size_t)z * n) * n + c] = a;
+    out[((size_t)z * n + (n - 1)) * n + c] = b;
+}
+
 }  // namespace
 
 // ============================================================================
@@ -462,8 +534,15 @@ struct pt_radon {
     int *fxy = nullptr;
     // forward (per chunk of ZC slices)
     float2 *rbuf = nullptr, *fgrid = nullptr;
+    // a second chunk buffer set and a side stream: alternate chunks of the
+    // forward run on the caller's stream and on `side`, so one chunk's FFTs
+    // overlap the previous chunk's gather (fork/join by events)
+    float2 *rbuf2 = nullptr, *fgrid2 = nullptr;
+    int streams = 2;   // 1: every chunk on the caller's stream (pt_radon_autotune chooses)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // adjoint (all slices, slice-minor with nzp lanes)
-    float2 *lines = nullptr, *rbuf_adj = nullptr;
+    float2 *lines = nullptr, *rbuf_adj = nullptr, *mbuf = nullptr;
     int *goff = nullptr, *col_order = nullptr, *gpt = nullptr;
     float4 *gw = nullptr;
     float *deap = nullptr;  // N x N: circ / phi / (4 N^2)
@@ -474,10 +553,13 @@ namespace {
 
 void radon_free(pt_radon *h)
 {
-    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->rbuf, h->fgrid,
-                    h->lines, h->rbuf_adj, h->goff, h->col_order, h->gpt, h->gw, h->deap};
+    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->rbuf, h->fgrid, h->rbuf2, h->fgrid2,
+                    h->lines, h->rbuf_adj, h->mbuf, h->goff, h->col_order, h->gpt, h->gw, h->deap};
     for (void *p : bufs)
         if (p) cudaFree(p);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
 }
 
 // Kernel half-width for a forced M: choose -log(eps) so that the reference's
@@ -509,10 +591,13 @@ int set_attrs()
     PT_CUDA(cudaFuncSetAttribute(k_fwd_cols<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s2));
     const int s4 = ZQ * (G + 1) * sizeof(float2);
     PT_CUDA(cudaFuncSetAttribute(k_adj_colgather<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s4));
+    PT_CUDA(cudaFuncSetAttribute(k_adj_colgather<G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s4));
     PT_CUDA(cudaFuncSetAttribute(k_adj_rows<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
+    PT_CUDA(cudaFuncSetAttribute(k_adj_rows_exact<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
     const int s3 = ZC * (N + 1) * sizeof(float2);
     PT_CUDA(cudaFuncSetAttribute(k_fwd_lines<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     PT_CUDA(cudaFuncSetAttribute(k_adj_lines<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    PT_CUDA(cudaFuncSetAttribute(k_adj_lines<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     return PT_OK;
 }
 
@@ -525,22 +610,38 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
     const size_t s3 = ZC * (N + 1) * sizeof(float2);
     const float a = (float)(PI_REF * PI_REF / h->mu);
     const float pre = (float)(PI_REF / std::fabs(h->mu)) / (float)N;
-    for (int z0 = 0; z0 < h->nz; z0 += ZC) {
-        k_fwd_rows<G><<<N, ZC * T, s1, st>>>(f, h->rbuf, h->nz, z0, h->deap, h->tw_G);
+    const int nchunks = (h->nz + ZC - 1) / ZC;
+    const bool two = nchunks > 1 && h->streams == 2;
+    if (two) {   // fork: the side stream starts after everything queued on st so far
+        PT_CUDA(cudaEventRecord(h->ev_fork, st));
+        PT_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+    }
+    for (int c = 0; c < nchunks; ++c) {
+        const int z0 = c * ZC;
+        // chunk buffers: set c % 2 on stream c % 2 (a set is reused only by its
+        // own stream, in order); gathered lines at offset (c % 2) of the lines buffer
+        const bool odd = two && (c & 1);
+        cudaStream_t s = odd ? h->side : st;
+        float2 *rb = odd ? h->rbuf2 : h->rbuf, *fg = odd ? h->fgrid2 : h->fgrid;
+        float2 *ln = h->lines + (odd ? (size_t)h->ntheta * N * ZC : 0);
+        k_fwd_rows<G><<<N, ZC * T, s1, s>>>(f, rb, h->nz, z0, h->deap, h->tw_G);
         PT_LAUNCHED("k_fwd_rows");
-        k_fwd_cols<G><<<G / CK, CK * ZC * T, s2, st>>>(h->rbuf, h->fgrid, h->tw_G);
+        k_fwd_cols<G><<<G / CK, CK * ZC * T, s2, s>>>(rb, fg, h->tw_G);
         PT_LAUNCHED("k_fwd_cols");
-        k_fwd_gather_pts<N, M><<<dim3((N + GPB - 1) / GPB, h->ntheta), GPB * ZC, 0, st>>>(h->fgrid, h->lines, h->x,
-                                                                                          h->y, a, pre);
+        k_fwd_gather_pts<N, M><<<dim3((N + GPB - 1) / GPB, h->ntheta), GPB * ZC, 0, s>>>(fg, ln, h->x, h->y, a, pre);
         PT_LAUNCHED("k_fwd_gather_pts");
-        k_fwd_lines<N><<<h->ntheta, ZC * 32, s3, st>>>(h->lines, g, h->nz, z0, scale, h->tw_N);
+        k_fwd_lines<N><<<h->ntheta, ZC * 32, s3, s>>>(ln, g, h->nz, z0, scale, h->tw_N);
         PT_LAUNCHED("k_fwd_lines");
+    }
+    if (two) {   // join: st continues after the side stream's chunks
+        PT_CUDA(cudaEventRecord(h->ev_join, h->side));
+        PT_CUDA(cudaStreamWaitEvent(st, h->ev_join, 0));
     }
     return PT_OK;
 }
 
 template <int G, int M>
-int run_adj(pt_radon *h, float2 *f, const float2 *g, float scale, cudaStream_t st)
+int run_adj(pt_radon *h, float2 *f, const float2 *g, float scale, cudaStream_t st, bool exact)
 {
     constexpr int N = G / 2, n = G / 3, T = fft_threads<G>();
     const size_t s1 = ZC * (G + 1) * sizeof(float2);
@@ -548,6 +649,20 @@ int run_adj(pt_radon *h, float2 *f, const float2 *g, float scale, cudaStream_t s
     const size_t s4 = ZQ * (G + 1) * sizeof(float2);
     const float pre = (float)(PI_REF / std::fabs(h->mu)) / (float)N;
     const int nzp = h->nzp;
+    if (exact) {
+        k_adj_lines<N, true><<<dim3(h->ntheta, nzp / ZC), ZC * 32, s3, st>>>(g, h->lines, h->nz, nzp, pre, h->tw_N);
+        PT_LAUNCHED("k_adj_lines");
+        k_adj_colgather<G, true><<<dim3(nzp / ZQ, G), ZQ * T, s4, st>>>(h->lines, h->rbuf_adj, h->goff, h->gpt,
+                                                                       h->gw, h->col_order, nzp, h->tw_G);
+        PT_LAUNCHED("k_adj_colgather");
+        k_adj_rows_exact<G><<<dim3(N, nzp / ZC), ZC * T, s1, st>>>(h->rbuf_adj, f, h->mbuf, h->nz, nzp, h->deap,
+                                                                   scale, h->tw_G);
+        PT_LAUNCHED("k_adj_rows_exact");
+        const size_t cnt = (size_t)h->nz * n;
+        k_adj_fold_rows<<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(h->mbuf, f, h->nz, n, N / 6, n / 2 + 2);
+        PT_LAUNCHED("k_adj_fold_rows");
+        return PT_OK;
+    }
     k_adj_lines<N><<<dim3(h->ntheta, nzp / ZC), ZC * 32, s3, st>>>(g, h->lines, h->nz, nzp, pre, h->tw_N);
     PT_LAUNCHED("k_adj_lines");
     k_adj_colgather<G><<<dim3(nzp / ZQ, G), ZQ * T, s4, st>>>(h->lines, h->rbuf_adj, h->goff, h->gpt, h->gw,
@@ -580,13 +695,14 @@ int radon_set_attrs(int G)
     return PT_ERR_UNSUPPORTED;
 }
 
-int radon_dispatch(pt_radon *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st)
+int radon_dispatch(pt_radon *h, bool adj, float2 *out, const float2 *in, float scale, cudaStream_t st,
+                   bool exact = false)
 {
 #define PT_CASE(GG)                                                                 \
     if (h->G == GG) {                                                               \
-        if (h->M == 7) return adj ? run_adj<GG, 7>(h, out, in, scale, st)           \
+        if (h->M == 7) return adj ? run_adj<GG, 7>(h, out, in, scale, st, exact)    \
                                   : run_fwd<GG, 7>(h, out, in, scale, st);          \
-        if (h->M == 4) return adj ? run_adj<GG, 4>(h, out, in, scale, st)           \
+        if (h->M == 4) return adj ? run_adj<GG, 4>(h, out, in, scale, st, exact)    \
                                   : run_fwd<GG, 4>(h, out, in, scale, st);          \
     }
     PT_RADON_GRIDS(PT_CASE)
@@ -662,12 +778,23 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     if (rc == PT_OK) rc = dmalloc(&h->y, ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->fxy, 2 * ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->rbuf, N * G * ZC);
+    if (rc == PT_OK) rc = dmalloc(&h->rbuf2, N * G * ZC);
     if (rc == PT_OK) rc = dmalloc(&h->deap, (size_t)N * N);
     if (rc == PT_OK) rc = dmalloc(&h->fgrid, (size_t)(G + GH_ROWS) * (G + 2 * GH_PAIRS) * ZC);
+    if (rc == PT_OK) rc = dmalloc(&h->fgrid2, (size_t)(G + GH_ROWS) * (G + 2 * GH_PAIRS) * ZC);
+    if (rc == PT_OK && (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+                        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess)) {
+        pt::set_error("radonusfft: stream/event creation failed");
+        rc = PT_ERR_CUDA;
+    }
     h->nzp = (int)((nz + ZQ - 1) / ZQ * ZQ);
     const size_t nzp = h->nzp;
     if (rc == PT_OK) rc = dmalloc(&h->lines, ntheta * N * nzp);
-    if (rc == PT_OK) rc = dmalloc(&h->rbuf_adj, n * (size_t)G * nzp);
+    // all N rows of the padded slice (the exact adjoint's fold needs them; the
+    // reference adjoint uses the first n)
+    if (rc == PT_OK) rc = dmalloc(&h->rbuf_adj, N * (size_t)G * nzp);
+    if (rc == PT_OK) rc = dmalloc(&h->mbuf, (n / 2 + 2) * (size_t)nz * n);
     if (rc == PT_OK) rc = dmalloc(&h->goff, (size_t)G * (G / CG) + 1);
     if (rc == PT_OK) rc = dmalloc(&h->col_order, (size_t)G);
     if (rc == PT_OK) rc = radon_set_attrs(G);
@@ -819,7 +946,7 @@ extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
 }
 
 namespace {
-int radon_call(pt_radon *h, bool adj, void *out, const void *in, float scale, void *stream)
+int radon_call(pt_radon *h, bool adj, void *out, const void *in, float scale, void *stream, bool exact = false)
 {
     pt::clear_error();
     PT_CHECK_ARG(h != nullptr, "radonusfft: null handle");
@@ -830,7 +957,7 @@ int radon_call(pt_radon *h, bool adj, void *out, const void *in, float scale, vo
     }
     int rc = check_device(h);
     if (rc != PT_OK) return rc;
-    return radon_dispatch(h, adj, (float2 *)out, (const float2 *)in, scale, (cudaStream_t)stream);
+    return radon_dispatch(h, adj, (float2 *)out, (const float2 *)in, scale, (cudaStream_t)stream, exact);
 }
 }  // namespace
 
@@ -849,6 +976,62 @@ extern "C" int pt_radon_fwd_scaled(pt_radon *h, void *g, const void *f, float sc
 extern "C" int pt_radon_adj_scaled(pt_radon *h, void *f, const void *g, float scale, void *stream)
 {
     return radon_call(h, true, f, g, scale, stream);
+}
+
+// Autotuner: times the forward with its chunks on one stream and pipelined on
+// two, and keeps the faster (setup-time; blocks the host).
+extern "C" int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials, int *streams_out, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h && g && f && trials >= 1, "radonusfft.autotune: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    PT_CUDA(cudaEventCreate(&e0));
+    PT_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_s = h->streams, rc = PT_OK;
+    for (int sc = 1; sc <= 2 && rc == PT_OK; ++sc) {
+        h->streams = sc;
+        std::vector<float> ts;
+        for (int k = 0; k <= trials && rc == PT_OK; ++k) {
+            cudaEventRecord(e0, st);
+            rc = pt_radon_fwd(h, g, f, stream);
+            cudaEventRecord(e1, st);
+            if (rc == PT_OK && cudaEventSynchronize(e1) == cudaSuccess && k > 0) {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ts.push_back(ms);
+            }
+        }
+        if (rc != PT_OK) break;
+        std::sort(ts.begin(), ts.end());
+        if (ts[ts.size() / 2] < best) {
+            best = ts[ts.size() / 2];
+            best_s = sc;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->streams = best_s;
+    if (streams_out) *streams_out = best_s;
+    return rc;
+}
+
+int pt::radon_dims(const pt_radon *h, int *nz, int *ntheta)
+{
+    PT_CHECK_ARG(h != nullptr, "radonusfft: null handle");
+    if (!h->ready) {
+        pt::set_error("radonusfft: setobj(theta) has not been called");
+        return PT_ERR_STATE;
+    }
+    *nz = h->nz;
+    *ntheta = h->ntheta;
+    return PT_OK;
+}
+
+extern "C" int pt_radon_adj_exact(pt_radon *h, void *f, const void *g, float scale, void *stream)
+{
+    return radon_call(h, true, f, g, scale, stream, true);
 }
 
 extern "C" int pt_radon_get_params(const pt_radon *h, int *N, int *M, float *mu)

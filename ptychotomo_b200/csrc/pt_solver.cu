@@ -430,6 +430,19 @@ __global__ void k_reg_adj(float2 *__restrict__ res, const float2 *__restrict__ g
     }
 }
 
+// the entries of g [3][nz][ny][nx] outside the range of J: x = nx-1 of
+// component 0, y = ny-1 of 1, z = nz-1 of 2
+__global__ void k_reg_mask(float2 *__restrict__ g, int nz, int ny, int nx)
+{
+    const size_t vol = (size_t)nz * ny * nx;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < vol; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+        if (x == nx - 1) g[i] = czero();
+        if (y == ny - 1) g[vol + i] = czero();
+        if (z == nz - 1) g[2 * vol + i] = czero();
+    }
+}
+
 // solve_reg (solver.py:257-264): z = J u + mu/tau, isotropic soft threshold alpha/tau
 __global__ void k_solve_reg(float2 *__restrict__ z, const float2 *__restrict__ u, const float2 *__restrict__ mu,
                             int nz, int ny, int nx, float s, float inv_tau, float thr)
@@ -604,6 +617,15 @@ extern "C" int pt_reg_adj_c64(void *res, const void *g, int nz, int ny, int nx, 
     k_reg_adj<<<ew_blocks((size_t)nz * ny * nx), 256, 0, (cudaStream_t)stream>>>((float2 *)res, (const float2 *)g,
                                                                                   nz, ny, nx, s);
     PT_LAUNCHED("k_reg_adj");
+    return PT_OK;
+}
+
+extern "C" int pt_reg_mask_c64(void *g, int nz, int ny, int nx, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(g && nz > 0 && ny > 0 && nx > 0, "reg_mask: bad arguments");
+    k_reg_mask<<<ew_blocks((size_t)nz * ny * nx), 256, 0, (cudaStream_t)stream>>>((float2 *)g, nz, ny, nx);
+    PT_LAUNCHED("k_reg_mask");
     return PT_OK;
 }
 

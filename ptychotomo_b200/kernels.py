@@ -143,6 +143,13 @@ def reg_adj(res, g, s):
     return res
 
 
+def reg_mask(g):
+    """Zero the entries of g [3, nz, ny, nx] outside the range of J (in place)."""
+    _, nz, ny, nx = g.shape
+    check(lib().pt_reg_mask_c64(_c64(g), nz, ny, nx, current_stream()), "reg_mask")
+    return g
+
+
 def solve_reg(z, u, mu, s, inv_tau, thr):
     nz, ny, nx = u.shape
     check(lib().pt_solve_reg_c64(_c64(z), _c64(u), _c64(mu), nz, ny, nx, float(s), float(inv_tau), float(thr),

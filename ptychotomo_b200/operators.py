@@ -48,6 +48,22 @@ class radonusfft:  # noqa: N801 - reference class name
             check(lib().pt_radon_adj_scaled(self._h, as_ptr(f), as_ptr(g), float(scale), _s(stream)),
                   "radonusfft.adj")
 
+    def adj_exact(self, f, g, scale=1.0, stream=None):
+        """f = scale * R^T g, the exact adjoint of fwd (zero-padded detector
+        lines, margins of the padded slice folded onto the edge pixels); adj
+        is the reference's, exact only for border-vanishing g and f."""
+        check(lib().pt_radon_adj_exact(self._h, as_ptr(f), as_ptr(g), float(scale), _s(stream)),
+              "radonusfft.adj_exact")
+
+    def autotune(self, g, f, trials=3, stream=None):
+        """Time the forward on one stream and pipelined on two; keep the
+        faster for this operator.  g, f: buffers of fwd's shapes (g is
+        overwritten).  Returns the number of streams chosen."""
+        out = ctypes.c_int()
+        check(lib().pt_radon_autotune(self._h, as_ptr(g), as_ptr(f), int(trials), ctypes.byref(out), _s(stream)),
+              "radonusfft.autotune")
+        return out.value
+
     def get_xy(self, x, y, stream=None):
         """Copy the polar coordinate tables (each float32 [Ntheta, N])."""
         check(lib().pt_radon_get_xy(self._h, as_ptr(x), as_ptr(y), _s(stream)), "radonusfft.get_xy")
@@ -94,6 +110,21 @@ class ptychofft:  # noqa: N801 - reference class name
         else:
             check(lib().pt_ptycho_adj_scaled(self._h, as_ptr(f), as_ptr(g), float(scale), _s(stream)),
                   "ptychofft.adj")
+
+    def autotune(self, f, g, trials=3, stream=None):
+        """Time the adjoint for each split of an angle's scans over blocks and
+        keep the fastest.  f, g: buffers of adj's shapes (f is overwritten).
+        Returns the chosen number of parts."""
+        out = ctypes.c_int()
+        check(lib().pt_ptycho_autotune(self._h, as_ptr(f), as_ptr(g), int(trials), ctypes.byref(out), _s(stream)),
+              "ptychofft.autotune")
+        return out.value
+
+    @property
+    def parts(self):
+        out = ctypes.c_int()
+        check(lib().pt_ptycho_get_parts(self._h, ctypes.byref(out)), "ptychofft.parts")
+        return out.value
 
     def adj_resid(self, f, fpsi, data, dscale, model, scale=1.0, stream=None):
         """Gradient of the data term: f = scale * Q* F* residual(fpsi, dscale * data)."""

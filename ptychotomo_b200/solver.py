@@ -240,11 +240,92 @@ class Solver:
         return 0 if gamma <= 1e-12 else gamma
 
     # ---- CG tomography, solver.py:180-203 ---------------------------------
+    precond = None   # a learned.FourierPreconditioner: cg_tomo then runs the preconditioned CG
+
+    def set_preconditioner(self, pre):
+        """Use the preconditioned CG (``pcg_tomo``) with ``pre`` in cg_tomo and
+        admm from now on; None restores the reference's CG."""
+        self.precond = pre
+
     def cg_tomo(self, xi0, xi1, Kt, init, rho, tau, titer):
         return self._cg_tomo(xi0, xi1, Kt, init, rho, tau, titer)[0]
 
+    def pcg_tomo(self, xi0, xi1, Kt, init, rho, tau, titer, precond=None, tol=0.0, history=None):
+        """Preconditioned CG on the tomography subproblem of cg_tomo
+        (solver.py:180-203), rho ||K R u - xi0||^2 + tau ||J u - xi1||^2, a
+        quadratic in u: the exact gradient rho R^T conj(K) (K R u - xi0) +
+        tau J^T (J u - xi1) (R^T: radonusfft.adj_exact; J^T: adj_reg on the
+        range of J), z = P g, Fletcher-Reeves directions and the exact step
+        along each.  P is ``precond`` (SPD, so the minimiser is that of the
+        subproblem); None is the identity: plain CG with exact steps, the
+        fallback and the judge of the preconditioner's error.  Stops after
+        titer iterations or once ||g|| <= tol ||g_0||; ``history`` receives
+        ||g_k|| / ||g_0||.  Returns (u, R u)."""
+        return self._pcg_tomo(xi0, xi1, Kt, init, rho, tau, titer, precond, tol, history)
+
+    def _pcg_tomo(self, xi0, xi1, Kt, init, rho, tau, titer, precond, tol=0.0, history=None):
+        red = self.red
+        u = init.clone()
+        Ru = self.fwd_tomo_batch(u)
+        a = K.cmul(torch.empty_like(xi0), Kt, Ru)
+        K.lincomb(a, [(1.0, a), (-1.0, xi0)])
+        xi1m = K.reg_mask(xi1.clone())       # entries of xi1 outside the range of J are constant in u
+        b = self.fwd_reg(u)
+        K.lincomb(b, [(1.0, b), (-1.0, xi1m)])
+        rk = rho * red.norm2(Kt) / Kt.numel() if precond is not None else 0.0
+        ka = torch.empty_like(a)
+        g = torch.empty_like(u)
+        z = torch.empty_like(u) if precond is not None else g
+        d = None
+        gz0 = g0n = None
+        for _ in range(titer):
+            K.cmul(ka, Kt, a, mode=2)
+            self._tomo_all.adj_exact(g, ka, scale=self.coeftomo)
+            K.lincomb(g, [(rho, g), (tau, self.adj_reg(b))])
+            if precond is not None:
+                precond.apply(z, g, rk, tau)
+                gz = red.dot(g, z).real
+                gn = red.norm2(g) if (tol > 0 or history is not None) else None
+            else:
+                gz = red.norm2(g)
+                gn = gz
+            if gn is not None:
+                g0n = gn if g0n is None else g0n
+                if history is not None:
+                    history.append(math.sqrt(gn / g0n) if g0n > 0 else 0.0)
+                if tol > 0 and gn <= tol * tol * g0n:
+                    break
+            steepest = d is None or gz0 is None or gz0 <= 0
+            if steepest:
+                d = K.lincomb(torch.empty_like(z), [(-1.0, z)])
+            else:
+                K.lincomb(d, [(-1.0, z), (gz / gz0, d)])
+            gz0 = gz
+            Rd = self.fwd_tomo_batch(d)
+            fd = K.cmul(torch.empty_like(xi0), Kt, Rd)
+            gd = self.fwd_reg(d)
+            _, a_fd, fd2 = red.quad3(a, fd)
+            _, b_gd, gd2 = red.quad3(b, gd)
+            c1 = rho * a_fd + tau * b_gd
+            c2 = rho * fd2 + tau * gd2
+            if not (c1 < 0 and c2 > 0):
+                if not steepest:
+                    gz0 = None          # a conjugate direction that does not descend: retry along -z
+                    continue
+                break                   # -z does not descend either: converged to rounding
+            gamma = -c1 / c2
+            if self.trace is not None:
+                self.trace.append(("pcg", gamma))
+            K.lincomb(u, [(1.0, u), (gamma, d)])
+            K.lincomb(Ru, [(1.0, Ru), (gamma, Rd)])
+            K.lincomb(a, [(1.0, a), (gamma, fd)])
+            K.lincomb(b, [(1.0, b), (gamma, gd)])
+        return u, Ru
+
     def _cg_tomo(self, xi0, xi1, Kt, init, rho, tau, titer):
         """cg_tomo, also returning R u of the final iterate (for h in admm)."""
+        if self.precond is not None:
+            return self._pcg_tomo(xi0, xi1, Kt, init, rho, tau, titer, self.precond)
         red = self.red
         u = init.clone()
         gamma = 2
@@ -501,6 +582,28 @@ class Solver:
         return state
 
     # ---- ADMM, solver.py:308-336 ------------------------------------------
+    def admm_step(self, m, st, rho, tau, data, alpha, piter, titer, model, probe_iter=0):
+        """One ADMM iteration, the loop body of solver.py:311-329, from the state
+        st (a dict of u, psi, h, e, phi, lamd, mu; device tensors, data as
+        _as_data gives it); returns (new state, rho, tau).  With probe_iter > 0
+        the probe is refined after the ptycho subproblem (no counterpart in
+        the reference)."""
+        u, psi, h, e, phi, lamd, mu = (st[k] for k in self._STATE)
+        h0, e0 = h, e
+        psi = self.cg_ptycho_batch(data, psi, h, lamd, rho, piter + (m < 2) * 32, model)
+        if probe_iter > 0:
+            self.set_probe(self.cg_probe(data, psi, self.prb, probe_iter, model))
+        xi0, xi1, Kt, pshift = self.takexi(psi, phi, lamd, mu, rho, tau)
+        u, Ru = self._cg_tomo(self._theta_to_z(xi0), xi1, self._theta_to_z(Kt), u, rho, tau, titer)
+        phi = self.solve_reg(u, mu, tau, alpha)
+        h = K.expmap(torch.empty_like(psi), self._z_to_theta(Ru),
+                     self.voxelsize * self.wavenumber() / self.coeftomo, pshift)
+        e = self.fwd_reg(u)
+        lamd = K.lincomb(torch.empty_like(lamd), [(1.0, lamd), (rho, h), (-rho, psi)])
+        mu = K.lincomb(torch.empty_like(mu), [(1.0, mu), (tau, e), (-tau, phi)])
+        rho, tau = self.update_penalty(psi, h, h0, phi, e, e0, rho, tau)
+        return dict(u=u, psi=psi, h=h, e=e, phi=phi, lamd=lamd, mu=mu), rho, tau
+
     def admm(self, data, h, e, psi, phi, lamd, mu, u, alpha, piter, titer, niter, model, verbose=True,
              history=None, checkpoint=None, checkpoint_every=1, resume=False, probe_iter=0):
         """ADMM as solver.py:308-336.  With ``checkpoint`` (a file path) the state
@@ -518,20 +621,10 @@ class Solver:
             u, psi, h, e, phi, lamd, mu = (st[k] for k in self._STATE)
             if "prb" in st and not torch.equal(st["prb"], self.prb.cpu()):
                 self.set_probe(st["prb"])
+        st = dict(u=u, psi=psi, h=h, e=e, phi=phi, lamd=lamd, mu=mu)
         for m in range(m0, niter):
-            h0, e0 = h, e
-            psi = self.cg_ptycho_batch(data, psi, h, lamd, rho, piter + (m < 2) * 32, model)
-            if probe_iter > 0:
-                self.set_probe(self.cg_probe(data, psi, self.prb, probe_iter, model))
-            xi0, xi1, Kt, pshift = self.takexi(psi, phi, lamd, mu, rho, tau)
-            u, Ru = self._cg_tomo(self._theta_to_z(xi0), xi1, self._theta_to_z(Kt), u, rho, tau, titer)
-            phi = self.solve_reg(u, mu, tau, alpha)
-            h = K.expmap(torch.empty_like(psi), self._z_to_theta(Ru),
-                         self.voxelsize * self.wavenumber() / self.coeftomo, pshift)
-            e = self.fwd_reg(u)
-            lamd = K.lincomb(torch.empty_like(lamd), [(1.0, lamd), (rho, h), (-rho, psi)])
-            mu = K.lincomb(torch.empty_like(mu), [(1.0, mu), (tau, e), (-tau, phi)])
-            rho, tau = self.update_penalty(psi, h, h0, phi, e, e0, rho, tau)
+            st, rho, tau = self.admm_step(m, st, rho, tau, data, alpha, piter, titer, model, probe_iter)
+            u, psi, h, e, phi, lamd, mu = (st[k] for k in self._STATE)
             if history is not None:
                 history.append(dict(m=m, rho=rho, tau=tau))
             if np.mod(m, 10) == 0 and (verbose or history is not None):

@@ -130,3 +130,25 @@ def test_oracle_pinned_to_reference_ptycho(path):
 def test_golden_vectors_present():
     """The oracle must be pinned: fixtures generated from the reference exist."""
     assert GOLDEN_RADON and GOLDEN_PTYCHO, "run tests/golden/make_golden.py on a GPU"
+
+
+def test_usfft_exact_adjoint_identity_full_support():
+    """adj_exact is the adjoint of fwd for inputs that do not vanish on their
+    borders (where the reference's adj is not: it replicates edges)."""
+    from oracle.usfft import RadonUSFFT
+    n, nz, nt = 32, 2, 20
+    rng = np.random.default_rng(9)
+    op = RadonUSFFT(nt, nz, n)
+    op.setobj(np.linspace(0, np.pi, nt, endpoint=False).astype(np.float32))
+    f = rng.standard_normal((nz, n, n)) + 1j * rng.standard_normal((nz, n, n))
+    g = rng.standard_normal((nt, nz, n)) + 1j * rng.standard_normal((nt, nz, n))
+    a = np.vdot(op.fwd(f), g)
+    b = np.vdot(f, op.adj_exact(g))
+    assert abs(a - b) / abs(a) < 1e-12
+    assert abs(a - np.vdot(f, op.adj(g))) / abs(a) > 1e-2     # the reference's adjoint is not exact here
+    f0 = f.copy()
+    f0[:, 0, :] = f0[:, -1, :] = f0[:, :, 0] = f0[:, :, -1] = 0
+    g0 = g.copy()
+    g0[:, :, 0] = g0[:, :, -1] = 0
+    inner = (slice(None), slice(1, -1), slice(1, -1))
+    assert np.allclose(op.adj_exact(g0)[inner], op.adj(g0)[inner], rtol=0, atol=1e-12 * np.abs(op.adj(g0)).max())
