@@ -793,34 +793,74 @@ def run_precision(args, local):
         rec["photons_%g" % photons] = {"u_vs_oracle_solver": rel(ug, uo), "u_vs_phantom": rel(ug, obj),
                                        "oracle_u_vs_phantom": rel(uo, obj)}
     out["reconstruction_32cubed_4iter"] = rec
+    # reconstructions at 256^3: 512 angles on [0, pi), 13 x 13 scans, 128^2
+    # probe, Poisson counts at the three photon levels, 4 ADMM x 4 CG (the
+    # small configuration's schedule), against the phantom (the oracle Solver
+    # at this size would take hours on the host; it is compared at 32^3 above)
+    del gs, os_
+    torch.cuda.empty_cache()
+    c256 = dict(n=256, nz=256, ntheta=512, nprb=128, det=128, nside=13, step=None, voxel=1e-6, energy=5.0)
+    rec256 = {}
+    for photons in (1e2, 1e3, 1e4):
+        slv, data, u_true = _admm_problem(dict(c256, photons=photons), torch, dev, seed=4)
+        cx = dict(dtype=torch.complex64, device=dev)
+        one = torch.ones((512, 256, 256), **cx)
+        z3 = torch.zeros((3, 256, 256, 256), **cx)
+        t0 = time.perf_counter()
+        ug, _ = slv.admm(data, one.clone(), z3.clone(), one, z3.clone(), torch.zeros_like(one), z3.clone(),
+                         torch.zeros((256, 256, 256), **cx), 1e-3, 4, 4, 4, "poisson", verbose=False)
+        torch.cuda.synchronize()
+        rec256["photons_%g" % photons] = {
+            "u_vs_phantom": float(torch.linalg.vector_norm(ug - u_true) / torch.linalg.vector_norm(u_true)),
+            "delta_vs_phantom": float(torch.linalg.vector_norm(ug.real - u_true.real) /
+                                      torch.linalg.vector_norm(u_true.real)),
+            "beta_vs_phantom": float(torch.linalg.vector_norm(ug.imag - u_true.imag) /
+                                     torch.linalg.vector_norm(u_true.imag)),
+            "seconds": round(time.perf_counter() - t0, 2)}
+        del slv, data, u_true, ug, one, z3
+        torch.cuda.empty_cache()
+    out["reconstruction_256cubed_512angles_4iter"] = rec256
     return {"metric": "precision study (relative L2 errors)", "n_gpus": 1, "data": "synthetic",
             "config": {"workload": "operators 256^3 / 512 angles (sampled 2 slices x 16 angles for the USFFT "
                                    "direct sums, 2 angles x 169 frames for ptycho); reconstructions 32^3, 16 "
-                                   "angles, 4 ADMM iterations"},
+                                   "angles, 4 ADMM iterations (against the oracle Solver), and 256^3, 512 angles, "
+                                   "4 ADMM iterations (against the phantom)"},
             "errors": out}
 
 
 def run_uneven(args, local):
-    """Uneven scans, batched against a per-angle loop: 256^3, 96 angles (a
-    sample of a 720-angle scan), per-angle scan counts drawn from [100, 400]
-    on a jittered spiral (padded with the -1 sentinel), 128^2 probe and
-    detector.  Times 4 ptycho CG iterations with all angles in one operator
-    launch (ptheta = ntheta) and with one launch per angle (ptheta = 1, the
-    reference's chunk loop at its finest)."""
+    """Batched uneven scans with a graph-captured iteration, against a per-angle
+    loop: 256^3, 720 angles, per-angle scan counts drawn from [100, 400] on a
+    jittered spiral (+-3 px; padded with the -1 sentinel), 128^2 probe and
+    detector, Poisson counts at 1e3 photons.  Times (1) a ptycho CG iteration
+    with all angles in one operator launch (ptheta = ntheta) and with one
+    launch per angle (ptheta = 1, the reference's chunk loop at its finest),
+    and (2) a steady ADMM iteration (4 + 4 CG iterations): all angles batched
+    with device-resident scalars, replayed as one CUDA graph, against the
+    host-driven Solver with one launch per angle."""
     import torch
     from ptychotomo_b200 import Solver, synthetic
+    from ptychotomo_b200.graphed import GraphedADMM
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     n = nz = 256
-    nt, P = 96, 128
+    nt, P = args.ntheta or 720, 128
     rng = np.random.default_rng(11)
     counts = rng.integers(100, 401, nt)
     scan = synthetic.jittered_spiral_scan(nt, n, nz, P, counts, jitter=3.0, seed=12)
     theta = synthetic.angles(nt)
     prb = synthetic.probe(P, seed=1)
     obj = synthetic.phantom(n, nz, seed=2)
-    out = {}
+    out, adm = {}, {}
     data = None
+    cx = dict(dtype=torch.complex64, device=dev)
+
+    def init():
+        one = torch.ones((nt, nz, n), **cx)
+        z3 = torch.zeros((3, nz, n, n), **cx)
+        return dict(u=torch.zeros((nz, n, n), **cx), psi=one.clone(), h=one.clone(), e=z3.clone(), phi=z3.clone(),
+                    lamd=torch.zeros_like(one), mu=z3.clone())
+
     for label, ptheta in (("batched", nt), ("per_angle", 1)):
         slv = Solver(prb, scan, theta, [P, P], 1e-6, 5.0, nt, nz, n, ptheta, nz, device=dev)
         if data is None:
@@ -829,22 +869,48 @@ def run_uneven(args, local):
             g = torch.Generator(device=dev).manual_seed(13)
             data = torch.poisson(inten * scale, generator=g) / scale
             del inten
-        psi = torch.ones((nt, nz, n), dtype=torch.complex64, device=dev)
+            torch.cuda.empty_cache()
+        psi = torch.ones((nt, nz, n), **cx)
         slv.cg_ptycho_batch(data, psi, psi.clone(), torch.zeros_like(psi), 0.5, 1, "poisson")   # warm-up
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         slv.cg_ptycho_batch(data, psi, psi.clone(), torch.zeros_like(psi), 0.5, 4, "poisson")
         torch.cuda.synchronize()
         out[label] = round(1e3 * (time.perf_counter() - t0) / 4, 2)
+        del psi
+        torch.cuda.empty_cache()
+        # a steady ADMM iteration (m = 2) from the same start
+        if label == "batched":
+            gr = GraphedADMM(slv, data, 1e-3, 4, 4, "poisson")
+            gr.load(init(), 0.5, 0.5)
+            gr.capture()
+            gr.replay()                 # warm-up replay
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            gr.replay()
+            torch.cuda.synchronize()
+            adm["batched_graph"] = round(1e3 * (time.perf_counter() - t0), 1)
+            del gr
+        else:
+            st = init()
+            slv.admm_step(2, st, 0.5, 0.5, data, 1e-3, 4, 4, "poisson")     # warm-up
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            slv.admm_step(2, st, 0.5, 0.5, data, 1e-3, 4, 4, "poisson")
+            torch.cuda.synchronize()
+            adm["per_angle_host"] = round(1e3 * (time.perf_counter() - t0), 1)
+            del st
         del slv
         torch.cuda.empty_cache()
     frames = int(counts.sum())
-    return {"metric": "ptycho CG ms per iteration, uneven scans: one launch for all angles vs one per angle",
+    return {"metric": "ms per ADMM iteration and per ptycho CG iteration, uneven scans: batched (graph-replayed "
+                      "ADMM iteration) vs one launch per angle",
             "unit": "ms", "n_gpus": 1, "higher_is_better": False, "data": "synthetic",
             "config": {"workload": "256^3, %d angles, scans per angle in [100, 400] (%d frames, padded to %d), "
-                                   "jittered spiral, 128^2 probe/detector, Poisson 1e3 photons" % (
-                                       nt, frames, nt * int(counts.max()))},
-            "ms_per_cg_iteration": out, "speedup": round(out["per_angle"] / out["batched"], 2)}
+                                   "jittered spiral, 128^2 probe/detector, Poisson 1e3 photons, 4 + 4 CG iterations "
+                                   "per ADMM iteration" % (nt, frames, nt * int(counts.max()))},
+            "ms_per_admm_iteration": adm, "admm_speedup": round(adm["per_angle_host"] / adm["batched_graph"], 2),
+            "ms_per_cg_iteration": out, "cg_speedup": round(out["per_angle"] / out["batched"], 2)}
 
 
 # ---- learned preconditioner of the tomography CG ------------------------------

@@ -177,17 +177,23 @@ __global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
 // one 128-byte line).  The window's 15 columns are covered by 8 column pairs;
 // the one column outside the window gets weight 0.  Writes the gathered,
 // 1/N- and fftshift1c-scaled samples to lines[(theta N + k) ZC + z].
+// Points are visited in the order of `perm` (built at setobj): sorted by the
+// 16 x 16-cell grid tile their window starts in, so the 32 points of a block
+// read overlapping windows and most taps hit L1.  The order changes no
+// arithmetic: every point is gathered by one group of 8 lanes as before.
 constexpr int GPB = 32;
+constexpr int GTILE = 16;   // grid cells per tile edge of the visiting order
 template <int N, int M>
 __global__ void __launch_bounds__(GPB *ZC, 3)
     k_fwd_gather_pts(const float2 *__restrict__ fg, float2 *__restrict__ lines, const float *__restrict__ xt,
-                     const float *__restrict__ yt, float a, float pre)
+                     const float *__restrict__ yt, float a, float pre, const int *__restrict__ perm, int npts)
 {
     constexpr int G = 2 * N, W = 2 * M + 1, NP = (W + 2) / 2;  // column pairs covering the window
-    const int th = blockIdx.y;
     const int lane = threadIdx.x % ZC;
-    const int k = blockIdx.x * GPB + threadIdx.x / ZC;
-    if (k >= N) return;
+    const int pi = blockIdx.x * GPB + threadIdx.x / ZC;
+    if (pi >= npts) return;
+    const int p = __ldg(&perm[pi]);
+    const int th = p / N, k = p % N;
     const float x0 = xt[th * N + k], y0 = yt[th * N + k];
     // x0, y0 in [-1/2, 1/2) (validated at setobj); clamp keeps reads in bounds
     const int fx = min(max((int)floorf((float)G * x0), -N), N - 1);
@@ -532,6 +538,7 @@ struct pt_radon {
     float2 *tw_G = nullptr, *tw_N = nullptr;
     float *theta = nullptr, *x = nullptr, *y = nullptr;
     int *fxy = nullptr;
+    int *perm = nullptr;   // the forward gather's point order (grid tiles)
     // forward (per chunk of ZC slices)
     float2 *rbuf = nullptr, *fgrid = nullptr;
     // a second chunk buffer set and a side stream: alternate chunks of the
@@ -553,7 +560,7 @@ namespace {
 
 void radon_free(pt_radon *h)
 {
-    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->rbuf, h->fgrid, h->rbuf2, h->fgrid2,
+    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->perm, h->rbuf, h->fgrid, h->rbuf2, h->fgrid2,
                     h->lines, h->rbuf_adj, h->mbuf, h->goff, h->col_order, h->gpt, h->gw, h->deap};
     for (void *p : bufs)
         if (p) cudaFree(p);
@@ -628,7 +635,8 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
         PT_LAUNCHED("k_fwd_rows");
         k_fwd_cols<G><<<G / CK, CK * ZC * T, s2, s>>>(rb, fg, h->tw_G);
         PT_LAUNCHED("k_fwd_cols");
-        k_fwd_gather_pts<N, M><<<dim3((N + GPB - 1) / GPB, h->ntheta), GPB * ZC, 0, s>>>(fg, ln, h->x, h->y, a, pre);
+        const int npts = h->ntheta * N;
+        k_fwd_gather_pts<N, M><<<(npts + GPB - 1) / GPB, GPB * ZC, 0, s>>>(fg, ln, h->x, h->y, a, pre, h->perm, npts);
         PT_LAUNCHED("k_fwd_gather_pts");
         k_fwd_lines<N><<<h->ntheta, ZC * 32, s3, s>>>(ln, g, h->nz, z0, scale, h->tw_N);
         PT_LAUNCHED("k_fwd_lines");
@@ -777,6 +785,7 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     if (rc == PT_OK) rc = dmalloc(&h->x, ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->y, ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->fxy, 2 * ntheta * N);
+    if (rc == PT_OK) rc = dmalloc(&h->perm, ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->rbuf, N * G * ZC);
     if (rc == PT_OK) rc = dmalloc(&h->rbuf2, N * G * ZC);
     if (rc == PT_OK) rc = dmalloc(&h->deap, (size_t)N * N);
@@ -864,6 +873,18 @@ extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
         fxy[2 * p + 1] = (int)floorf((float)G * ys[p]);
     }
     PT_CUDA(cudaMemcpy(h->fxy, fxy.data(), 2 * npts * sizeof(int), cudaMemcpyHostToDevice));
+    {   // the forward gather's visiting order: by the grid tile of the window origin, then point index
+        std::vector<int> perm(npts);
+        std::vector<unsigned> tile(npts);
+        const int TPR = (G + GTILE - 1) / GTILE;
+        for (size_t p = 0; p < npts; ++p) {
+            perm[p] = (int)p;
+            const int ox = ((N + fxy[2 * p] - M) % G + G) % G, oy = ((N + fxy[2 * p + 1] - M) % G + G) % G;
+            tile[p] = (unsigned)((oy / GTILE) * TPR + ox / GTILE);
+        }
+        std::stable_sort(perm.begin(), perm.end(), [&](int i, int j) { return tile[i] < tile[j]; });
+        PT_CUDA(cudaMemcpy(h->perm, perm.data(), npts * sizeof(int), cudaMemcpyHostToDevice));
+    }
     // cell-group lists for the adjoint: a group is CG consecutive rows of one
     // grid column; every point is listed, in increasing point order, in each
     // group that its (2M+1)^2 window (mod G: the reference's halo fold,

@@ -13,10 +13,11 @@ ptycho CG iterations, solver.py:315) run the same sequence eagerly.
 
 Differences from Solver.admm, all by construction of a fixed sequence:
 * the ptycho line search evaluates J step lengths gamma 2^-j (j < J) per CG
-  iteration in one pass and takes the first that passes the reference's
-  test; if none does, that iteration steps by 0 and the next one starts from
-  gamma 2^-J (the host Solver would search further along the same
-  direction);
+  iteration in one pass (J_first = 16 on a call's first iteration, where
+  gamma restarts from 2; J = 4 after, where gamma persists) and takes the
+  first that passes the reference's test; if none does, that iteration steps
+  by 0 and the next one starts from gamma 2^-J (the host Solver would search
+  further along the same direction);
 * F Q psi advances by linearity (F Q (psi + g d) = F Q psi + g F Q d) for
   every step taken, recomputed once per CG call;
 * a CG whose step is 0 keeps iterating with zero steps (the host Solver
@@ -68,16 +69,19 @@ class GraphedADMM:
     with device-resident scalars.
 
     ``data``: the counts (device float32, as Solver.admm takes them);
-    alpha, piter, titer, model: as Solver.admm.  ``J``: step lengths per
-    ptycho line-search pass.  ``precond``: a FourierPreconditioner for the
-    tomography subproblem (None: the reference's CG)."""
+    alpha, piter, titer, model: as Solver.admm.  ``J``, ``J_first``: step
+    lengths per ptycho line-search pass (after and on a CG call's first
+    iteration).  ``precond``: a FourierPreconditioner for the tomography
+    subproblem (None: the reference's CG)."""
 
-    def __init__(self, slv, data, alpha, piter, titer, model, J=4, precond=None):
+    def __init__(self, slv, data, alpha, piter, titer, model, J=4, J_first=16, precond=None):
         if slv.ptheta != slv.ntheta_held or slv.nz_held != slv.nz:
             raise ValueError("GraphedADMM needs a Solver with ptheta = ntheta and pnz = nz")
         self.slv, self.alpha, self.piter, self.titer = slv, float(alpha), int(piter), int(titer)
         self.model = _MODELS[model]
-        self.J = int(J)
+        self.J, self.J_first = int(J), int(J_first)
+        if not (1 <= self.J <= 16 and 1 <= self.J_first <= 16):
+            raise ValueError("1 <= J, J_first <= 16")
         self.precond = precond
         self.data = slv._as_data(data)
         dev = slv.device
@@ -184,11 +188,12 @@ class GraphedADMM:
                 self._lin(self.pd, [g, self.pd], A("pbeta", 4))
             op.fwd(self.fd, self.pd, scale=slv.coefptycho)
             self._red(2, A("pq", 3), self.pw, self.pd)
-            check(lib().pt_scalar_ls_candidates(A("pgam", 4), self.J, A("gams", 16), self._st()), "ls_candidates")
+            J = self.J_first if i == 0 else self.J
+            check(lib().pt_scalar_ls_candidates(A("pgam", 4), J, A("gams", 16), self._st()), "ls_candidates")
             check(lib().pt_ls_frames(_p(self.fpsi), _p(self.fd), _p(self.data), float(dscale), self.fpsi.numel(),
-                                     self.model, A("gams", 16), self.J, _p(self.work), A("lsv", 16), self._st()),
+                                     self.model, A("gams", 16), J, _p(self.work), A("lsv", 16), self._st()),
                   "ls_frames")
-            check(lib().pt_scalar_ptycho_gamma(A("lsv", 16), A("gams", 16), self.J, A("pq", 3), rt, A("pgam", 4),
+            check(lib().pt_scalar_ptycho_gamma(A("lsv", 16), A("gams", 16), J, A("pq", 3), rt, A("pgam", 4),
                                                A("pstep", 4), self._st()), "ptycho_gamma")
             self._lin(self.psi, [self.psi, self.pd], A("pstep", 4))
             self._lin(self.fpsi, [self.fpsi, self.fd], A("pstep", 4))

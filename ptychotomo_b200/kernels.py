@@ -32,17 +32,45 @@ class Reducer:
     OPS = {"norm2": 0, "dot": 1, "quad3": 2, "maxabs": 3, "angle_band": 4, "norm2_diff": 5, "tv": 6,
            "maxangle": 7}
 
+    # values per op (many() packs them in this order)
+    _NVALS = {"norm2": 1, "dot": 2, "quad3": 3, "maxabs": 1, "norm2_diff": 1, "tv": 1, "maxangle": 1}
+
     def __init__(self, device):
         nbytes = lib().pt_reduce_workspace_bytes()
         self.work = torch.empty(nbytes // 8, dtype=torch.float64, device=device)
         self.out = torch.empty(16, dtype=torch.float64, device=device)
         self.gam = torch.empty(16, dtype=torch.float64, device=device)
+        self.outm = torch.empty(64, dtype=torch.float64, device=device)
 
     def _run(self, op, a, b=None, n=None, c0=0, c1=0, ncol=1, k=1):
         n = a.numel() if n is None else n
         check(lib().pt_reduce_c64(op, _c64(a), _c64(b) if b is not None else None, n, c0, c1, ncol,
                                   _p(self.work), _p(self.out), current_stream()), "reduce")
         return self.out[:k].tolist()
+
+    def many(self, ops):
+        """Several reductions with one read-back: ops = [(name, a[, b]), ...]
+        with name in norm2, dot, quad3, norm2_diff; returns their results in
+        order, as the single methods return them."""
+        off = 0
+        base = self.outm.data_ptr()
+        for name, *arrs in ops:
+            a = arrs[0]
+            b = arrs[1] if len(arrs) > 1 else None
+            check(lib().pt_reduce_c64(self.OPS[name], _c64(a), _c64(b) if b is not None else None, a.numel(), 0, 0, 1,
+                                      _p(self.work), base + 8 * off, current_stream()), "reduce")
+            off += self._NVALS[name]
+        return self.unpack(ops, self.outm[:off].tolist())
+
+    @classmethod
+    def unpack(cls, ops, flat):
+        out, off = [], 0
+        for name, *_ in ops:
+            k = cls._NVALS[name]
+            v = flat[off:off + k]
+            off += k
+            out.append(complex(v[0], v[1]) if name == "dot" else tuple(v) if name == "quad3" else v[0])
+        return out
 
     def norm2(self, a):
         """||a||^2 (cp.linalg.norm(a)**2 in the reference)."""

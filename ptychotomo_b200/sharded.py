@@ -181,6 +181,17 @@ class _GlobalReducer:
     def __init__(self, red, comm: ShardComm, device):
         self._red, self._comm, self._dev = red, comm, device
 
+    def many(self, ops):
+        """The local reductions of Reducer.many, then one all-reduce of all
+        their values (sums only)."""
+        if any(name in self._MAX for name, *_ in ops):
+            raise ValueError("many() batches sums only")
+        local = self._red.many(ops)
+        flat = []
+        for v in local:
+            flat += [v.real, v.imag] if isinstance(v, complex) else list(v) if isinstance(v, tuple) else [v]
+        return type(self._red).unpack(ops, self._comm.allreduce(flat, "sum", self._dev))
+
     def __getattr__(self, name):
         fn = getattr(self._red, name)
         if not callable(fn) or name.startswith("_"):

@@ -344,15 +344,15 @@ class Solver:
             if i == 0:
                 d = K.lincomb(torch.empty_like(grad), [(-1.0, grad)])
             else:
-                den = red.dot(d, grad) - red.dot(d, grad0)
-                beta = red.norm2(grad) / den if den != 0 else 0.0
+                dg, dg0, g2 = red.many([("dot", d, grad), ("dot", d, grad0), ("norm2", grad)])
+                den = dg - dg0
+                beta = g2 / den if den != 0 else 0.0
                 K.lincomb(d, [(-1.0, grad), (beta, d)])
             grad0 = grad
             Rd = self.fwd_tomo_batch(d)
             fd = K.cmul(torch.empty_like(xi0), Kt, Rd)
             gd = self.fwd_reg(d)
-            _, a_fd, fd2 = red.quad3(a, fd)
-            _, b_gd, gd2 = red.quad3(b, gd)
+            (_, a_fd, fd2), (_, b_gd, gd2) = red.many([("quad3", a, fd), ("quad3", b, gd)])
             c1 = rho * a_fd + tau * b_gd
             c2 = rho * fd2 + tau * gd2
             gamma = self._halve_until(gamma, lambda g: -(2 * g * c1 + g * g * c2))
@@ -387,8 +387,9 @@ class Solver:
             if i == 0:
                 d = K.lincomb(torch.empty_like(grad), [(-1.0, grad)])
             else:
-                den = red.dot(d, grad) - red.dot(d, grad0)
-                beta = red.norm2(grad) / den if den != 0 else 0.0
+                dg, dg0, g2 = red.many([("dot", d, grad), ("dot", d, grad0), ("norm2", grad)])
+                den = dg - dg0
+                beta = g2 / den if den != 0 else 0.0
                 K.lincomb(d, [(-1.0, grad), (beta, d)])
             grad0 = grad
             fd = self.fwd_ptycho(d)

@@ -1,0 +1,65 @@
+"""The autotuners: ptychofft.autotune picks the adjoint's angle split and
+radonusfft.autotune the forward's stream count by timing; either choice
+keeps the operators' results (against the oracle, rel-L2 <= 1e-5), and the
+two radon stream counts give bit-identical projections."""
+import numpy as np
+import pytest
+
+from oracle.ptycho import PtychoFFT
+from oracle.usfft import RadonUSFFT
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def crand(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+def T(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_ptycho_autotune_keeps_the_adjoint():
+    from ptychotomo_b200 import ptychofft
+    rng = np.random.default_rng(0)
+    nt, nz, n, ns, det = 4, 160, 160, 9, 128
+    scan = np.stack([rng.uniform(0, n - det - 0.5, (nt, ns)), rng.uniform(0, nz - det - 0.5, (nt, ns))]).astype(np.float32)
+    prb = crand(rng, (det, det))
+    op = ptychofft(nt, nz, n, nt, ns, det, det, det)
+    op.setobj(T(scan), T(prb))
+    g = T(crand(rng, (nt, ns, det, det)))
+    f = torch.empty((nt, nz, n), dtype=torch.complex64, device="cuda")
+    parts = op.autotune(f, g, trials=2)
+    assert parts == op.parts and 1 <= parts <= ns
+    op.adj(f, g)
+    orc = PtychoFFT(nt, nz, n, nt, ns, det, det, det)
+    orc.setobj(scan, prb)
+    assert rel(f.cpu().numpy(), orc.adj(g.cpu().numpy())) <= 1e-5
+
+
+def test_radon_autotune_keeps_the_forward():
+    from ptychotomo_b200 import radonusfft
+    rng = np.random.default_rng(1)
+    n, nz, nt = 64, 40, 48
+    theta = np.linspace(0, np.pi, nt, endpoint=False).astype(np.float32)
+    op = radonusfft(nt, nz, n)
+    op.setobj(T(theta))
+    f = T(crand(rng, (nz, n, n)))
+    g = torch.empty((nt, nz, n), dtype=torch.complex64, device="cuda")
+    before = torch.empty_like(g)
+    op.fwd(before, f)
+    s = op.autotune(g, f, trials=2)
+    assert s in (1, 2)
+    op.fwd(g, f)
+    assert torch.equal(g, before)       # one stream or two: the same kernels on the same chunks
+    x = torch.empty((nt, op.N), dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    op.get_xy(x, y)
+    orc = RadonUSFFT(nt, nz, n)
+    orc.setobj(theta, xy=(x.cpu().numpy(), y.cpu().numpy()))
+    assert rel(g.cpu().numpy(), orc.fwd(f.cpu().numpy())) <= 1e-5

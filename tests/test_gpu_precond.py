@@ -157,10 +157,10 @@ def test_phase_probe_keeps_the_modulus_spectrum_and_statistics():
 
 @pytest.fixture(scope="module")
 def wedge_problem():
-    """A tomography subproblem with a 60-degree missing wedge: 64 wide, 8
+    """A tomography subproblem with a 60-degree missing wedge: 64 wide, 16
     slices, 90 angles on [-60, 60) degrees, K = 1, xi0 = R u of a phantom."""
     from ptychotomo_b200 import Solver, synthetic
-    n, nz, nt = 64, 8, 90
+    n, nz, nt = 64, 16, 90
     theta = synthetic.angles(nt, -np.pi / 3, np.pi / 3)
     prb = synthetic.probe(16, seed=1)
     scan = synthetic.raster_scan(nt, 2, n, nz, 16)
