@@ -16,7 +16,8 @@ Pass-model algorithmic bytes per call (complex64 = 8 B):
                   (read the probe-sized patch, write the detector frame)
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-    python bench.py --admm        # ADMM wall time (128^3 run, 256^3 iterations)
+    python bench.py --admm        # ADMM wall time (128^3 run, 256^3 iterations); under torchrun with
+                                  # --gpus N: the sharded ADMM's iteration time and its all-to-alls
     python bench.py --cg-kernels  # the ptycho CG's frame kernels at the operator workload
     python bench.py --precision   # operator errors vs direct sums, reconstruction errors
     python bench.py --uneven      # uneven scans: one launch for all angles vs one per angle
@@ -650,6 +651,86 @@ def run_admm(args, local):
     return line
 
 
+def run_admm_sharded(args, rank, world, local):
+    """ADMM iterations of the sharded Solver on `world` GPUs (one process
+    each, NCCL): 256^3, 384 angles, 13x13 scans, 128^2 probe, Poisson 1e3
+    photons; every rank holds a block of angles and a block of slices.
+    Times 4 steady iterations (4 + 4 CG) as the maximum over ranks of CUDA
+    events, and the angle <-> slice all-to-alls inside them separately."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from ptychotomo_b200 import synthetic
+    from ptychotomo_b200.sharded import ShardComm, ShardedSolver
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if not dist.is_initialized():
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    c = dict(ADMM_SMALL, n=256, nz=256, ntheta=384, nprb=128, det=128, nside=13, step=None)
+    n, nz, nt = c["n"], c["nz"], c["ntheta"]
+    comm = ShardComm(nt, nz)
+    theta = synthetic.angles(nt)
+    prb = synthetic.probe(c["nprb"], seed=1)
+    scan = synthetic.raster_scan(nt, c["nside"], n, nz, c["nprb"])
+    obj = synthetic.phantom(n, nz, seed=2)
+    slv = ShardedSolver(prb, scan, theta, [c["det"], c["det"]], c["voxel"], c["energy"], nt, nz, n, comm, device=dev)
+    u_r = torch.from_numpy(slv.z_shard(obj)).to(dev)
+    inten = slv.fwd_ptycho_batch(slv.exptomo(slv._z_to_theta(slv.fwd_tomo_batch(u_r))))
+    scale = c["photons"] / float(inten.mean())
+    g = torch.Generator(device=dev).manual_seed(3 + rank)
+    data = torch.poisson(inten * scale, generator=g) / scale
+    del inten
+    th0, th1 = comm.theta_ranges[rank]
+    z0, z1 = comm.z_ranges[rank]
+    cx = dict(dtype=torch.complex64, device=dev)
+    one = torch.ones((th1 - th0, nz, n), **cx)
+    z3 = torch.zeros((3, z1 - z0, n, n), **cx)
+    st = dict(u=torch.zeros((z1 - z0, n, n), **cx), psi=one.clone(), h=one.clone(), e=z3.clone(), phi=z3.clone(),
+              lamd=torch.zeros_like(one), mu=z3.clone())
+    # time the all-to-alls inside the iterations with events around each call
+    xfer = []
+    orig_t2z, orig_z2t = comm.theta_to_z, comm.z_to_theta
+
+    def timed(fn):
+        def run(x):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            y = fn(x)
+            e1.record()
+            xfer.append((e0, e1))
+            return y
+        return run
+    comm.theta_to_z, comm.z_to_theta = timed(orig_t2z), timed(orig_z2t)
+    rho = tau = 0.5
+    st, rho, tau = slv.admm_step(2, st, rho, tau, data, c["alpha"], 4, 4, "poisson")    # warm-up
+    xfer.clear()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    K = max(1, args.steps if args.steps < 10 else 4)
+    for m in range(K):
+        st, rho, tau = slv.admm_step(2 + m, st, rho, tau, data, c["alpha"], 4, 4, "poisson")
+    e1.record()
+    dist.barrier()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    xms = sum(a.elapsed_time(b) for a, b in xfer) / K
+    t = torch.tensor([ms, xms], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, xms = t.tolist()
+    line = {"metric": "sharded ADMM ms per iteration (256^3, 384 angles)", "value": round(ms, 2), "unit": "ms",
+            "n_gpus": world, "steps": K, "higher_is_better": False, "scaling": "strong", "data": "synthetic",
+            "dtype": "c64 (fp32 complex), FP64 reductions",
+            "config": {"workload": "ShardedSolver, angle and slice blocks per rank, NCCL all-to-alls, 4 + 4 CG "
+                                   "iterations per ADMM iteration", "parallelism": "angles/slices over %d ranks" % world},
+            "all_to_all_ms_per_iteration": round(xms, 3)}
+    dist.barrier()
+    dist.destroy_process_group()
+    return line
+
+
 def run_cg_kernels(args, local):
     """Device time of the ptycho CG's frame-sized kernels at the operator workload:
     the gradient adjoint with the residual formed on load (Poisson, Gaussian) and
@@ -1061,9 +1142,9 @@ def run_time_to_target(args, local):
         return us, ts
 
     def graphed_run(pre):
+        slv.set_preconditioner(pre)
         g = GraphedADMM(slv, data, c["alpha"], c["piter"], c["titer"], "poisson", precond=pre)
-        st = init()
-        g.load(st, 0.5, 0.5)
+        g.load(init(), 0.5, 0.5)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.capture()            # set-up, counted in the wall time
@@ -1073,14 +1154,12 @@ def run_time_to_target(args, local):
         for m in range(c["iters"]):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            if m < 2:
-                g.step(m)
-            else:
-                g.replay()
+            g.run(m, m + 1)    # iterations 0-1 through the host Solver, then graph replays
             torch.cuda.synchronize()
             t += time.perf_counter() - t0
             us.append(g.u.clone())
             ts.append(t)
+        slv.set_preconditioner(None)
         return us, ts
 
     plain_run()   # warm-up (library state, allocator)
@@ -1167,6 +1246,11 @@ def main():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.admm and world > 1:
+        line = run_admm_sharded(args, rank, world, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return 0
     if args.admm or args.cg_kernels or args.precision or args.uneven or args.precond or args.time_to_target:
         if rank == 0:
             fn = (run_admm if args.admm else run_cg_kernels if args.cg_kernels else

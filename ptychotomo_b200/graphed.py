@@ -28,7 +28,6 @@ Solver.pcg_tomo instead.
 from __future__ import annotations
 
 import ctypes
-import math
 
 import numpy as np
 import torch
@@ -118,7 +117,6 @@ class GraphedADMM:
         self.td = torch.empty((nz, n, n), **c)
         self.work = torch.empty(lib().pt_reduce_workspace_bytes() // 8, dtype=torch.float64, device=dev)
         self.graph = None
-        self.graph_piter = None
 
     # ---- state in / out ---------------------------------------------------
     def load(self, st, rho, tau):
@@ -339,9 +337,19 @@ class GraphedADMM:
         self.graph.replay()
 
     def run(self, m0, niter, graph=True):
-        """Iterations m0 .. niter-1: eager while m < 2, replays after (graph=True)."""
+        """Iterations m0 .. niter-1.  Iterations 0 and 1 (36-step ptycho CGs
+        from psi = 1, whose last steps are decided within FP32 rounding) run
+        through the host Solver's admm_step, so they are those of Solver.admm;
+        later ones replay the graph (graph=True) or run its launch sequence
+        eagerly."""
         for m in range(m0, niter):
-            if m < 2 or not graph:
+            if m < 2:
+                st, rho, tau = self.state()
+                st, rho, tau = self.slv.admm_step(m, {k: v.clone() for k, v in st.items()}, rho, tau, self.data,
+                                                  self.alpha, self.piter, self.titer,
+                                                  ("poisson", "gaussian")[self.model])
+                self.load(st, rho, tau)
+            elif not graph:
                 self.step(m)
             else:
                 if self.graph is None:

@@ -190,7 +190,8 @@ class _GlobalReducer:
         flat = []
         for v in local:
             flat += [v.real, v.imag] if isinstance(v, complex) else list(v) if isinstance(v, tuple) else [v]
-        return type(self._red).unpack(ops, self._comm.allreduce(flat, "sum", self._dev))
+        from .kernels import Reducer
+        return Reducer.unpack(ops, self._comm.allreduce(flat, "sum", self._dev))
 
     def __getattr__(self, name):
         fn = getattr(self._red, name)

@@ -10,7 +10,6 @@
   differences ~100-fold, as in the lock-step test against the oracle).
 * With the learned preconditioner, the replay equals the eager run too.
 """
-import numpy as np
 import pytest
 
 from ptychotomo_b200 import synthetic

@@ -13,8 +13,6 @@ tomography CG.
   fewer iterations than plain CG, with a network trained on the method's
   own CG runs (training and held-out phantoms).
 """
-import math
-
 import numpy as np
 import pytest
 

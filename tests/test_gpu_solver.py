@@ -318,3 +318,14 @@ def test_cg_ptycho_advanced_frames_match_recomputed(problem, model):
     gs.advance_frames, gs.trace = True, None
     assert out[0][0] == out[1][0]
     assert rel(out[0][1], out[1][1]) < 1e-5
+
+
+def test_batched_reductions_equal_the_single_ones():
+    """Reducer.many (one read-back for the Dai-Yuan terms and the quad3
+    triples of a CG iteration) returns exactly what the single calls do."""
+    from ptychotomo_b200 import kernels as K
+    rng = np.random.default_rng(9)
+    a, b = T(crand(rng, (5, 37, 41))), T(crand(rng, (5, 37, 41)))
+    red = K.Reducer("cuda")
+    many = red.many([("dot", a, b), ("norm2", a), ("quad3", a, b), ("norm2_diff", a, b)])
+    assert many == [red.dot(a, b), red.norm2(a), red.quad3(a, b), red.norm2_diff(a, b)]

@@ -4,7 +4,8 @@ Two gloo ranks in spawned processes, ragged shards (5 angles and 7 slices over
 2 ranks).  Every rank builds the same seeded global arrays and checks its
 shards against them exactly: the angle -> slice and slice -> angle
 all-to-alls, the one-slice halos of the TV operator, the FP64 sum / max
-reductions and the gather used to assemble results.
+reductions (single and batched into one all-reduce) and the gather used to
+assemble results.
 """
 import os
 import socket
@@ -64,6 +65,18 @@ def _worker(rank, world, port, ntheta, nz, n, errq):
         tot_t = comm.allreduce_tensor(pr.clone())
         want = sum(_crand(torch.Generator().manual_seed(r), (5, 5)) for r in range(world))
         assert torch.allclose(tot_t, want, rtol=1e-6, atol=1e-6)
+        # batched reductions: one all-reduce for a CG iteration's Dai-Yuan terms
+        from ptychotomo_b200.kernels import Reducer
+        from ptychotomo_b200.sharded import _GlobalReducer
+
+        class LocalTerms:     # stands in for the device Reducer: rank-dependent partials
+            def many(self, ops):
+                r = float(rank + 1)
+                return Reducer.unpack(ops, [r, -r, 2 * r, 3 * r, 4 * r, 5 * r])
+        red = _GlobalReducer(LocalTerms(), comm, None)
+        ops = [("dot", None, None), ("norm2", None), ("quad3", None, None)]
+        tot = sum(range(1, world + 1))
+        assert red.many(ops) == [complex(tot, -tot), 2.0 * tot, (3.0 * tot, 4.0 * tot, 5.0 * tot)]
         # gather
         assert torch.equal(comm.gather(A[th0:th1].contiguous(), 0, comm.theta_ranges), A)
         assert torch.equal(comm.gather(U[:, z0:z1].contiguous(), 1, comm.z_ranges), U)
