@@ -79,10 +79,15 @@ int pt_radon_adj_scaled(pt_radon *h, void *f, const void *g, float scale, void *
 int pt_radon_adj_exact(pt_radon *h, void *f, const void *g, float scale, void *stream);
 /* Autotuner (no counterpart in the reference): times the forward with its
  * 8-slice chunks on the caller's stream alone and pipelined on two streams
- * (one chunk's FFTs under the previous chunk's gather), `trials` runs each
- * after a warm-up, and keeps the faster for this handle.  g, f: caller
- * buffers of the forward's shapes (overwritten).  Blocks the host. */
-int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials, int *streams_out, void *stream);
+ * (one chunk's FFTs under the previous chunk's gather), each with the
+ * Gaussian gather reading the grid through L1 and from shared-memory tiles
+ * (16 x 16 window origins per tile), `trials` runs each after a warm-up, and
+ * keeps the fastest for this handle (*out = streams + 2 * tiled).  g, f:
+ * caller buffers of the forward's shapes (overwritten).  Blocks the host.
+ * Every variant gives bit-identical results. */
+int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials, int *out, void *stream);
+/* Sets the forward's variant directly: streams 1 or 2, gather 0 (L1) or 1 (tiles). */
+int pt_radon_set_variant(pt_radon *h, int streams, int gather);
 /* Internal parameters: N, kernel half-width M, mu. */
 int pt_radon_get_params(const pt_radon *h, int *N, int *M, float *mu);
 /* Copies the polar coordinate tables x, y (device float[Ntheta][N] each). */

@@ -242,6 +242,90 @@ __global__ void __launch_bounds__(GPB *ZC, 3)
     lines[((size_t)th * N + k) * ZC + lane] = ((k & 1) ? pre : -pre) * acc;
 }
 
+// The same gather with the grid staged in shared memory.  Points were sorted
+// at setobj by the 16 x 16-cell tile of their window origin; a block takes a
+// chunk of at most TCH points of one tile, loads the part of the haloed grid
+// that their windows cover (rows ty0 .. ty0 + 16 + 2M - 1, column pairs
+// tx0/2 .. tx0/2 + 7 + NP - 1, clipped to the haloed grid) once, and gathers
+// from there.  Weights, loads and the order of the sums are those of
+// k_fwd_gather_pts, so the results are bit-identical.
+constexpr int TCH = 128;   // points per block of the tiled gather
+template <int M>
+constexpr int tile_rows() { return GTILE + 2 * M; }
+template <int M>
+constexpr int tile_pairs() { return (GTILE - 2) / 2 + (2 * M + 3) / 2; }
+template <int M>
+constexpr size_t tile_smem() { return (size_t)tile_rows<M>() * tile_pairs<M>() * ZC * sizeof(float4); }
+
+template <int N, int M>
+__global__ void __launch_bounds__(GPB *ZC, 3)
+    k_fwd_gather_tile(const float2 *__restrict__ fg, float2 *__restrict__ lines, const float *__restrict__ xt,
+                      const float *__restrict__ yt, float a, float pre, const int *__restrict__ perm,
+                      const int4 *__restrict__ chunks)
+{
+    constexpr int G = 2 * N, W = 2 * M + 1, NP = (W + 2) / 2;
+    constexpr int PS = G / 2 + GH_PAIRS, NROWS = G + GH_ROWS;   // the haloed grid's pair pitch and rows
+    constexpr int TR = tile_rows<M>(), TP = tile_pairs<M>();
+    extern __shared__ float4 tsm[];
+    const int4 ch = chunks[blockIdx.x];   // (tile row, tile column, first, count)
+    const int ty0 = ch.x * GTILE, px0 = ch.y * GTILE / 2;
+    const int rows = min(TR, NROWS - ty0), pairs = min(TP, PS - px0);
+    const float4 *g4 = reinterpret_cast<const float4 *>(fg);
+    for (int e = threadIdx.x; e < rows * pairs * ZC; e += blockDim.x) {
+        const int r = e / (pairs * ZC), rem = e % (pairs * ZC), pj = rem / ZC, q = rem % ZC;
+        tsm[(r * TP + pj) * ZC + q] = __ldg(&g4[((size_t)(ty0 + r) * PS + px0 + pj) * ZC + q]);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x % ZC;
+    for (int t = threadIdx.x / ZC; t < ch.w; t += GPB) {
+        const int p = __ldg(&perm[ch.z + t]);
+        const int th = p / N, k = p % N;
+        const float x0 = xt[th * N + k], y0 = yt[th * N + k];
+        const int fx = min(max((int)floorf((float)G * x0), -N), N - 1);
+        const int fy = min(max((int)floorf((float)G * y0), -N), N - 1);
+        const int c0 = wrapG(N + fx - M, G);
+        const int odd = c0 & 1;
+        float2 wxp[NP];
+        float wy[W];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            float w2[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i0 = 2 * j + h - odd;
+                const float w0 = (float)(fx - M + i0) / (float)G - x0;
+                w2[h] = (i0 >= 0 && i0 < W) ? __expf(-a * (w0 * w0)) : 0.f;
+            }
+            wxp[j] = make_float2(w2[0], w2[1]);
+        }
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+            const float w1 = (float)(fy - M + i) / (float)G - y0;
+            wy[i] = __expf(-a * (w1 * w1));
+        }
+        // window origin relative to the staged region (inside it by the tile sort)
+        const int rr = wrapG(N + fy - M, G) - ty0, pp = (c0 - odd) / 2 - px0;
+        const float4 *base = tsm + ((size_t)rr * TP + pp) * ZC + lane;
+        float2 acc = czero();
+#pragma unroll
+        for (int i1 = 0; i1 < W; ++i1) {
+            const float4 *rowp = base + (size_t)i1 * TP * ZC;
+            float2 rs = czero();
+#pragma unroll
+            for (int j = 0; j < NP; ++j) {
+                const float4 v = rowp[j * ZC];
+                rs.x = fmaf(wxp[j].x, v.x, rs.x);
+                rs.y = fmaf(wxp[j].x, v.y, rs.y);
+                rs.x = fmaf(wxp[j].y, v.z, rs.x);
+                rs.y = fmaf(wxp[j].y, v.w, rs.y);
+            }
+            acc.x = fmaf(wy[i1], rs.x, acc.x);
+            acc.y = fmaf(wy[i1], rs.y, acc.y);
+        }
+        lines[((size_t)th * N + k) * ZC + lane] = ((k & 1) ? pre : -pre) * acc;
+    }
+}
+
 // ---- K3b: fftshift1c / 1-D inverse FFT / fftshift1c + crop + scale --------
 template <int N>
 __global__ void __launch_bounds__(ZC * 32)
@@ -539,6 +623,9 @@ struct pt_radon {
     float *theta = nullptr, *x = nullptr, *y = nullptr;
     int *fxy = nullptr;
     int *perm = nullptr;   // the forward gather's point order (grid tiles)
+    int4 *chunks = nullptr;   // the tiled gather's blocks: (tile row, tile column, first, count)
+    int nchunks = 0, chunks_cap = 0;
+    int gather = 0;           // 0: gather through L1 (k_fwd_gather_pts), 1: shared-memory tiles
     // forward (per chunk of ZC slices)
     float2 *rbuf = nullptr, *fgrid = nullptr;
     // a second chunk buffer set and a side stream: alternate chunks of the
@@ -560,7 +647,8 @@ namespace {
 
 void radon_free(pt_radon *h)
 {
-    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->perm, h->rbuf, h->fgrid, h->rbuf2, h->fgrid2,
+    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->perm, h->chunks, h->rbuf, h->fgrid, h->rbuf2,
+                    h->fgrid2,
                     h->lines, h->rbuf_adj, h->mbuf, h->goff, h->col_order, h->gpt, h->gw, h->deap};
     for (void *p : bufs)
         if (p) cudaFree(p);
@@ -603,6 +691,10 @@ int set_attrs()
     PT_CUDA(cudaFuncSetAttribute(k_adj_rows_exact<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, s1));
     const int s3 = ZC * (N + 1) * sizeof(float2);
     PT_CUDA(cudaFuncSetAttribute(k_fwd_lines<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
+    PT_CUDA(cudaFuncSetAttribute(k_fwd_gather_tile<N, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_smem<7>()));
+    PT_CUDA(cudaFuncSetAttribute(k_fwd_gather_tile<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_smem<4>()));
     PT_CUDA(cudaFuncSetAttribute(k_adj_lines<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     PT_CUDA(cudaFuncSetAttribute(k_adj_lines<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     return PT_OK;
@@ -636,8 +728,15 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
         k_fwd_cols<G><<<G / CK, CK * ZC * T, s2, s>>>(rb, fg, h->tw_G);
         PT_LAUNCHED("k_fwd_cols");
         const int npts = h->ntheta * N;
-        k_fwd_gather_pts<N, M><<<(npts + GPB - 1) / GPB, GPB * ZC, 0, s>>>(fg, ln, h->x, h->y, a, pre, h->perm, npts);
-        PT_LAUNCHED("k_fwd_gather_pts");
+        if (h->gather == 1) {
+            k_fwd_gather_tile<N, M><<<h->nchunks, GPB * ZC, tile_smem<M>(), s>>>(fg, ln, h->x, h->y, a, pre, h->perm,
+                                                                              h->chunks);
+            PT_LAUNCHED("k_fwd_gather_tile");
+        } else {
+            k_fwd_gather_pts<N, M><<<(npts + GPB - 1) / GPB, GPB * ZC, 0, s>>>(fg, ln, h->x, h->y, a, pre, h->perm,
+                                                                             npts);
+            PT_LAUNCHED("k_fwd_gather_pts");
+        }
         k_fwd_lines<N><<<h->ntheta, ZC * 32, s3, s>>>(ln, g, h->nz, z0, scale, h->tw_N);
         PT_LAUNCHED("k_fwd_lines");
     }
@@ -884,6 +983,25 @@ extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
         }
         std::stable_sort(perm.begin(), perm.end(), [&](int i, int j) { return tile[i] < tile[j]; });
         PT_CUDA(cudaMemcpy(h->perm, perm.data(), npts * sizeof(int), cudaMemcpyHostToDevice));
+        // the tiled gather's blocks: runs of one tile in perm order, at most TCH points each
+        std::vector<int4> chunks;
+        for (size_t i = 0; i < npts;) {
+            size_t j = i;
+            while (j < npts && tile[perm[j]] == tile[perm[i]]) ++j;
+            const int t = (int)tile[perm[i]];
+            for (size_t f = i; f < j; f += TCH)
+                chunks.push_back(make_int4(t / TPR, t % TPR, (int)f, (int)std::min<size_t>(TCH, j - f)));
+            i = j;
+        }
+        if ((int)chunks.size() > h->chunks_cap) {
+            if (h->chunks) cudaFree(h->chunks);
+            h->chunks = nullptr;
+            h->chunks_cap = 0;
+            PT_CUDA(cudaMalloc(&h->chunks, chunks.size() * sizeof(int4)));
+            h->chunks_cap = (int)chunks.size();
+        }
+        h->nchunks = (int)chunks.size();
+        PT_CUDA(cudaMemcpy(h->chunks, chunks.data(), chunks.size() * sizeof(int4), cudaMemcpyHostToDevice));
     }
     // cell-group lists for the adjoint: a group is CG consecutive rows of one
     // grid column; every point is listed, in increasing point order, in each
@@ -1000,7 +1118,8 @@ extern "C" int pt_radon_adj_scaled(pt_radon *h, void *f, const void *g, float sc
 }
 
 // Autotuner: times the forward with its chunks on one stream and pipelined on
-// two, and keeps the faster (setup-time; blocks the host).
+// two, each with the gather through L1 and from shared-memory tiles, and
+// keeps the fastest (setup-time; blocks the host).
 extern "C" int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials, int *streams_out, void *stream)
 {
     pt::clear_error();
@@ -1010,9 +1129,11 @@ extern "C" int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials
     PT_CUDA(cudaEventCreate(&e0));
     PT_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
-    int best_s = h->streams, rc = PT_OK;
-    for (int sc = 1; sc <= 2 && rc == PT_OK; ++sc) {
+    int best_s = h->streams, best_g = h->gather, rc = PT_OK;
+    for (int combo = 0; combo < 4 && rc == PT_OK; ++combo) {
+        const int sc = 1 + (combo & 1);
         h->streams = sc;
+        h->gather = combo >> 1;
         std::vector<float> ts;
         for (int k = 0; k <= trials && rc == PT_OK; ++k) {
             cudaEventRecord(e0, st);
@@ -1029,12 +1150,14 @@ extern "C" int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials
         if (ts[ts.size() / 2] < best) {
             best = ts[ts.size() / 2];
             best_s = sc;
+            best_g = h->gather;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     h->streams = best_s;
-    if (streams_out) *streams_out = best_s;
+    h->gather = best_g;
+    if (streams_out) *streams_out = best_s + 2 * best_g;
     return rc;
 }
 
@@ -1047,6 +1170,16 @@ int pt::radon_dims(const pt_radon *h, int *nz, int *ntheta)
     }
     *nz = h->nz;
     *ntheta = h->ntheta;
+    return PT_OK;
+}
+
+extern "C" int pt_radon_set_variant(pt_radon *h, int streams, int gather)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h && (streams == 1 || streams == 2) && (gather == 0 || gather == 1),
+                 "radonusfft.set_variant: streams 1 or 2, gather 0 or 1");
+    h->streams = streams;
+    h->gather = gather;
     return PT_OK;
 }
 

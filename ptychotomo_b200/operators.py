@@ -56,13 +56,18 @@ class radonusfft:  # noqa: N801 - reference class name
               "radonusfft.adj_exact")
 
     def autotune(self, g, f, trials=3, stream=None):
-        """Time the forward on one stream and pipelined on two; keep the
-        faster for this operator.  g, f: buffers of fwd's shapes (g is
-        overwritten).  Returns the number of streams chosen."""
+        """Time the forward on one stream and pipelined on two, each with the
+        gather through L1 and from shared-memory tiles; keep the fastest for
+        this operator.  g, f: buffers of fwd's shapes (g is overwritten).
+        Returns (streams, tiled)."""
         out = ctypes.c_int()
         check(lib().pt_radon_autotune(self._h, as_ptr(g), as_ptr(f), int(trials), ctypes.byref(out), _s(stream)),
               "radonusfft.autotune")
-        return out.value
+        return out.value % 2 if out.value % 2 else 2, out.value // 2
+
+    def set_variant(self, streams=2, tiled=False):
+        """The forward's variant without timing (results are identical)."""
+        check(lib().pt_radon_set_variant(self._h, int(streams), int(bool(tiled))), "radonusfft.set_variant")
 
     def get_xy(self, x, y, stream=None):
         """Copy the polar coordinate tables (each float32 [Ntheta, N])."""

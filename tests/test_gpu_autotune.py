@@ -1,7 +1,8 @@
 """The autotuners: ptychofft.autotune picks the adjoint's angle split and
-radonusfft.autotune the forward's stream count by timing; either choice
-keeps the operators' results (against the oracle, rel-L2 <= 1e-5), and the
-two radon stream counts give bit-identical projections."""
+radonusfft.autotune the forward's stream count and gather variant by timing;
+every choice keeps the operators' results (against the oracle, rel-L2 <=
+1e-5), and the four radon forward variants (one or two streams, gather
+through L1 or from shared-memory tiles) give bit-identical projections."""
 import numpy as np
 import pytest
 
@@ -51,15 +52,41 @@ def test_radon_autotune_keeps_the_forward():
     op.setobj(T(theta))
     f = T(crand(rng, (nz, n, n)))
     g = torch.empty((nt, nz, n), dtype=torch.complex64, device="cuda")
+    op.set_variant(1, False)
     before = torch.empty_like(g)
     op.fwd(before, f)
-    s = op.autotune(g, f, trials=2)
-    assert s in (1, 2)
+    for streams in (1, 2):
+        for tiled in (False, True):
+            op.set_variant(streams, tiled)
+            op.fwd(g, f)
+            assert torch.equal(g, before), (streams, tiled)
+    streams, tiled = op.autotune(g, f, trials=2)
+    assert streams in (1, 2) and tiled in (0, 1)
     op.fwd(g, f)
-    assert torch.equal(g, before)       # one stream or two: the same kernels on the same chunks
+    assert torch.equal(g, before)
     x = torch.empty((nt, op.N), dtype=torch.float32, device="cuda")
     y = torch.empty_like(x)
     op.get_xy(x, y)
     orc = RadonUSFFT(nt, nz, n)
     orc.setobj(theta, xy=(x.cpu().numpy(), y.cpu().numpy()))
     assert rel(g.cpu().numpy(), orc.fwd(f.cpu().numpy())) <= 1e-5
+
+
+@pytest.mark.parametrize("n,nz,nt", [(16, 5, 12), (32, 9, 24), (256, 3, 384)])
+def test_tiled_gather_is_bit_identical(n, nz, nt):
+    """The shared-memory tiled gather against the L1 gather at small grids
+    (where the staged region is clipped to the haloed grid) and at the
+    bench's width and angle count."""
+    from ptychotomo_b200 import radonusfft
+    rng = np.random.default_rng(n)
+    theta = np.sort(rng.uniform(0, np.pi, nt)).astype(np.float32)
+    op = radonusfft(nt, nz, n)
+    op.setobj(T(theta))
+    f = T(crand(rng, (nz, n, n)))
+    a = torch.empty((nt, nz, n), dtype=torch.complex64, device="cuda")
+    b = torch.empty_like(a)
+    op.set_variant(1, False)
+    op.fwd(a, f)
+    op.set_variant(1, True)
+    op.fwd(b, f)
+    assert torch.equal(a, b)
