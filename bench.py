@@ -270,16 +270,9 @@ class Ops:
     def launches_per_step(self):
         """Kernel launches of one step: radon fwd 4 per 8-slice chunk, radon adj 3,
         ptycho fwd 1, ptycho adj 1 plus the slab reduction when the angles are
-        split into parts (the library's wave model, restated here)."""
+        split into parts (the operator's current split)."""
         zc = -(-self.c["nz"] // 8)
-        nt, S = self.c["ntheta"], self.c["nside"] ** 2
-        nsm = self.torch.cuda.get_device_properties(self.dev).multi_processor_count
-        best, parts = 1e300, 1
-        for p in range(1, min(S, 16) + 1):
-            cost = -(-nt * p // nsm) * -(-S // p) * (1.0 + 0.03 * (p - 1))
-            if cost < best - 1e-9:
-                best, parts = cost, p
-        return 4 * zc + 3 + 1 + 1 + (parts > 1)
+        return 4 * zc + 3 + 1 + 1 + (self.ptycho.parts > 1)
 
 
 def run_ours(args, rank, world, local):
@@ -1008,23 +1001,24 @@ def run_uneven(args, local):
 
 
 # ---- learned preconditioner of the tomography CG ------------------------------
-# 256^3, 360 angles on [-60, 60) degrees (a 60-degree missing wedge), seeded
-# ellipsoid phantoms: 64 training and 16 held-out seeds (8-slice volumes for
-# the training targets; the symbol is per slice), the 3->64->64->1 network
-# trained on the GPU; then the tomography subproblem of cg_tomo on a held-out
-# 256^3 phantom (K = 1, xi0 = R u, xi1 = 0, rho = 0.5) solved to a 1e-4
-# gradient reduction by plain CG and by PCG with the analytic ramp symbol and
-# with the learned symbol.
+# 256^3, 360 angles on [-60, 60) degrees (a 60-degree missing wedge): 64
+# training and 16 held-out seeds of white random-phase probes on 8-slice
+# volumes (the symbol is per slice) give the targets; the 3->64->64->1
+# network is trained on the GPU; then the tomography subproblem of cg_tomo
+# on a 256^3 phantom (K = 1, xi0 = R u, xi1 = 0, rho = 0.5) is solved to a
+# 1e-4 gradient reduction by plain CG and by PCG with: the diagonal alone
+# (Jacobi), the analytic ramp symbol, the symbol measured on the training
+# probes (no network), and the network's symbol.
 PRECOND = dict(n=256, nz=256, ntheta=360, lo=-np.pi / 3, hi=np.pi / 3, train=64, held=16, harvest_nz=8,
-               cg_iters=4, steps=1500, tol=1e-4, max_iter=400)
+               probes=4, steps=1500, tol=1e-4, max_iter=400)
 
 
 def _precond_setup(c, torch, dev, nz):
     from ptychotomo_b200 import Solver, synthetic
     theta = synthetic.angles(c["ntheta"], c["lo"], c["hi"])
-    prb = synthetic.probe(16, seed=1)
-    scan = synthetic.raster_scan(c["ntheta"], 2, c["n"], nz, 16)
-    slv = Solver(prb, scan, theta, [16, 16], 1e-6, 5.0, c["ntheta"], nz, c["n"], c["ntheta"], nz, device=dev)
+    prb = synthetic.probe(8, seed=1)          # the tomography operator is what is used here
+    scan = synthetic.raster_scan(c["ntheta"], 2, c["n"], nz, 8)
+    slv = Solver(prb, scan, theta, [8, 8], 1e-6, 5.0, c["ntheta"], nz, c["n"], c["ntheta"], nz, device=dev)
     return slv, torch.from_numpy(theta).to(dev)
 
 
@@ -1039,11 +1033,9 @@ def run_precond(args, local):
     # training targets from plain CG runs on 8-slice volumes
     hs, th = _precond_setup(c, torch, dev, c["harvest_nz"])
     hpre = FourierPreconditioner(hs._tomo_all, th, hs.coeftomo, dev)
-    vols = (torch.from_numpy(synthetic.phantom(n, c["harvest_nz"], seed=1000 + s) * 1e5).to(dev)
-            for s in range(c["train"] + c["held"]))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    tg = harvest_targets(hs._tomo_all, hpre, vols, cg_iters=c["cg_iters"], seed=11)
+    tg = harvest_targets(hs._tomo_all, hpre, range(1000, 1000 + c["train"] + c["held"]), probes=c["probes"])
     torch.cuda.synchronize()
     t_harvest = time.perf_counter() - t0
     t0 = time.perf_counter()
@@ -1051,6 +1043,10 @@ def run_precond(args, local):
                                                 lr=1e-2, lr_final=1e-3, seed=0)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
+    # the measured symbol itself (mean log over the training probe sets), for comparison
+    ys = torch.stack([y for y, _ in tg[:c["train"]]])
+    ws = torch.stack([w for _, w in tg[:c["train"]]])
+    est_log = ((ys * ws).sum(0) / ws.sum(0).clamp(min=1)).contiguous()
     del hs, hpre, tg
     torch.cuda.empty_cache()
     # the subproblem at 256^3
@@ -1066,12 +1062,17 @@ def run_precond(args, local):
     r = np.hypot(k[None, :], k[:, None])
     ramp = 1.0 / np.maximum(r, 1.0 / n)
     ramp_log = torch.from_numpy(np.log(ramp * dI / ramp.mean()).astype(np.float32)).to(dev)
+    jac_log = torch.full((n * n,), float(np.log(dI)), dtype=torch.float32, device=dev)
     out = {}
     for tau in (0.5, 0.05):
         row = {}
-        for label in ("plain", "ramp", "learned"):
-            if label == "ramp":
+        for label in ("plain", "jacobi", "ramp", "measured", "learned"):
+            if label == "jacobi":
+                pre.set_log_symbol(jac_log)
+            elif label == "ramp":
                 pre.set_log_symbol(ramp_log)
+            elif label == "measured":
+                pre.set_log_symbol(est_log)
             elif label == "learned":
                 pre.set_network(net)
             P = None if label == "plain" else pre
@@ -1196,14 +1197,12 @@ def run_time_to_target(args, local):
     del us_g
     torch.cuda.empty_cache()
     if not args.ttt_no_precond:
-        from ptychotomo_b200 import synthetic
         from ptychotomo_b200.learned import FourierPreconditioner, harvest_targets, train_network
         t0 = time.perf_counter()
         pre = FourierPreconditioner(slv._tomo_all, slv.theta, slv.coeftomo, dev)
-        vols = (torch.from_numpy(synthetic.phantom(n, 8, seed=2000 + s) * 1e5).to(dev) for s in range(16))
         hs = _precond_harvest_solver(slv, dev)
         hpre = FourierPreconditioner(hs._tomo_all, slv.theta, hs.coeftomo, dev)
-        tg = harvest_targets(hs._tomo_all, hpre, vols, cg_iters=4, seed=5)
+        tg = harvest_targets(hs._tomo_all, hpre, range(2000, 2016), probes=4)
         net, _, _, _ = train_network(hpre.x, tg, [], steps=1000, lr=1e-2, lr_final=1e-3)
         pre.set_network(net)
         torch.cuda.synchronize()
@@ -1225,7 +1224,7 @@ def _precond_harvest_solver(slv, dev):
     from ptychotomo_b200 import Solver, synthetic
     theta = slv.theta.cpu().numpy()
     nt, n = len(theta), slv.n
-    return Solver(synthetic.probe(16, seed=1), synthetic.raster_scan(nt, 2, n, 8, 16), theta, [16, 16], slv.voxelsize,
+    return Solver(synthetic.probe(8, seed=1), synthetic.raster_scan(nt, 2, n, 8, 8), theta, [8, 8], slv.voxelsize,
                   slv.energy, nt, 8, n, nt, 8, device=dev)
 
 

@@ -288,9 +288,10 @@ int pt_precond_targets(const double *num, const double *den, int nn, double den_
                        void *stream);
 /* dst = F2 src (unnormalised forward 2-D DFT of every slice). */
 int pt_precond_dft2(pt_precond *h, void *dst, const void *src, void *stream);
-/* dst = F2^-1(|F2 src| exp(2 pi i u)) with u uniform from a hash of (seed,
- * index): a probe with src's modulus spectrum and random phases. */
-int pt_precond_phase_probe(pt_precond *h, void *dst, const void *src, unsigned seed, void *stream);
+/* dst = F2^-1(sqrt(|F2 src|^2 + floor^2) exp(2 pi i u)) with u uniform from
+ * a hash of (seed, index): a probe with src's modulus spectrum (floored) and
+ * random phases; src = NULL: a white probe (unit modulus everywhere). */
+int pt_precond_phase_probe(pt_precond *h, void *dst, const void *src, unsigned seed, float floor, void *stream);
 
 /* ---- device-resident scalars: one ADMM iteration as a CUDA graph ---------
  * No counterpart in the reference, whose Solver (solver.py:171-336) decides
@@ -309,14 +310,22 @@ int pt_scalar_dy_beta(const double *g2, const double *dg, const double *dg0, int
  * -(2 gamma c1 + gamma^2 c2) < 0 and gamma > 1e-12; coef = (1, 0, gamma). */
 int pt_scalar_tomo_gamma(const double *q1, const double *q2, const double *rt, double *gamma, double *coef,
                          void *stream);
-/* gam[j] = gamma 2^-j, j < J <= 16. */
-int pt_scalar_ls_candidates(const double *gamma, int J, double *gam, void *stream);
-/* The ptycho line search over one pass (solver.py:171-177 with minf of
- * :208-214): the first j with !(data[j] + rho (2 g_j q[1] - g_j^2 q[2]) < 0
- * and g_j > 1e-12) is taken; none: step 0 and gamma <- g_{J-1} / 2;
- * coef = (1, 0, step). */
-int pt_scalar_ptycho_gamma(const double *data, const double *gam, int J, const double *quad, const double *rt,
-                           double *gamma, double *coef, void *stream);
+/* The ptycho line search (solver.py:171-177 with minf of :208-214) in passes,
+ * as Solver.cg_ptycho takes it: state = (accepted, step, gamma).
+ * ls_begin clears accepted; ls_candidates writes gam[j] = gamma 2^-j, j < J;
+ * ls_pass takes the first j with !(data[j] + rho (2 g_j q[1] - g_j^2 q[2])
+ * < 0 and g_j > 1e-12) (step 0 for g_j <= 1e-12) or sets gamma <- g_{J-1}/2,
+ * and does nothing once a step was accepted; ls_end writes coef = (1, 0,
+ * step) (0 if no pass accepted one). */
+int pt_scalar_ls_begin(double *state, void *stream);
+int pt_scalar_ls_candidates(const double *state, int J, double *gam, void *stream);
+int pt_scalar_ls_pass(const double *data, const double *gam, int J, const double *quad, const double *rt,
+                      double *state, void *stream);
+int pt_scalar_ls_end(const double *state, double *coef, void *stream);
+/* pt_ls_frames that does nothing when skip[0] != 0 (a device-side decision
+ * made the pass unnecessary); out is then left as it was. */
+int pt_ls_frames_dev(const void *f, const void *d, const float *data, float dscale, size_t n, int model,
+                     const double *gammas, int J, void *work, void *out, const double *skip, void *stream);
 /* takexi's scalars (solver.py:151-166): pshift = (band1 + band2) / (2 cnt),
  * coef = (e, -e / rho) with e = exp(-i pshift). */
 int pt_scalar_takexi(const double *band1, const double *band2, double cnt, const double *rt, double *pshift,

@@ -10,7 +10,7 @@
 //   * the tomography line search, solver.py:171-177 with minf of
 //     solver.py:181-184: halve gamma while the decrease
 //     -(2 g c1 + g^2 c2) < 0 and gamma > 1e-12 (c1, c2 of the closed form);
-//   * the ptycho line search over a pass of J candidates gamma 2^-j;
+//   * the ptycho line search over passes of 2, 8 and 16 step lengths;
 //   * takexi's background phase (solver.py:151-156) and max|t|;
 //   * the penalty update, solver.py:267-282.
 // Linear combinations then read their coefficients from the arena.
@@ -80,37 +80,51 @@ __global__ void k_tomo_gamma(const double *__restrict__ q1, const double *__rest
     coef[3] = 0;
 }
 
-// ptycho step candidates: gam[j] = gamma 2^-j, j < J
-__global__ void k_ls_candidates(const double *__restrict__ gamma, int J, double *__restrict__ gam)
+// ptycho line search over passes of J = 2, 8, 16 step lengths, as
+// Solver.cg_ptycho: state = (accepted, step, gamma).  A pass's candidates
+// are gamma 2^-j (j < J); once one passes, the later passes skip themselves
+// (their reduction kernels read `accepted`).
+__global__ void k_ls_begin(double *__restrict__ state)
 {
-    const int j = threadIdx.x;
-    if (j < J) gam[j] = gamma[0] * ldexp(1.0, -j);
+    state[0] = 0;
+    state[1] = 0;
 }
 
-// ptycho step: the first candidate j (of J) whose decision
-// dec_j = data_j + rho (2 g_j w_d - g_j^2 d2) satisfies !(dec < 0 && g > 1e-12)
-// is taken (0 when g <= 1e-12); if none, gamma <- g_{J-1}/2 and this
-// iteration steps by 0.  quad = (|w|^2, Re<w, d>, |d|^2).  Writes gamma and
-// coef = (1, 0, step, 0).
-__global__ void k_ptycho_gamma(const double *__restrict__ data, const double *__restrict__ gam, int J,
-                               const double *__restrict__ quad, const double *__restrict__ rt,
-                               double *__restrict__ gamma, double *__restrict__ coef)
+__global__ void k_ls_candidates(const double *__restrict__ state, int J, double *__restrict__ gam)
 {
+    const int j = threadIdx.x;
+    if (j < J) gam[j] = state[2] * ldexp(1.0, -j);
+}
+
+// one pass's decision: the first j with !(dec_j < 0 && g_j > 1e-12),
+// dec_j = data_j + rho (2 g_j w_d - g_j^2 d2), is taken (step 0 when
+// g_j <= 1e-12); none: gamma <- g_{J-1} / 2 for the next pass.  No-op once
+// a step was accepted.  quad = (|w|^2, Re<w, d>, |d|^2)
+__global__ void k_ls_pass(const double *__restrict__ data, const double *__restrict__ gam, int J,
+                          const double *__restrict__ quad, const double *__restrict__ rt, double *__restrict__ state)
+{
+    if (state[0] != 0) return;
     const double rho = rt[0], w_d = quad[1], d2 = quad[2];
-    double step = 0;
-    bool found = false;
-    for (int j = 0; j < J && !found; ++j) {
+    for (int j = 0; j < J; ++j) {
         const double g = gam[j];
         const double dec = data[j] + rho * (2 * g * w_d - g * g * d2);
         if (!(dec < 0 && g > 1e-12)) {
-            found = true;
-            step = g <= 1e-12 ? 0 : g;
+            const double step = g <= 1e-12 ? 0 : g;
+            state[0] = 1;
+            state[1] = step;
+            state[2] = step;
+            return;
         }
     }
-    gamma[0] = found ? step : gam[J - 1] * 0.5;
+    state[2] = gam[J - 1] * 0.5;
+}
+
+// coef = (1, 0, step, 0): the step taken (0 if no pass accepted one)
+__global__ void k_ls_end(const double *__restrict__ state, double *__restrict__ coef)
+{
     coef[0] = 1;
     coef[1] = 0;
-    coef[2] = step;
+    coef[2] = state[0] != 0 ? state[1] : 0.0;
     coef[3] = 0;
 }
 
@@ -321,22 +335,40 @@ extern "C" int pt_scalar_tomo_gamma(const double *q1, const double *q2, const do
     return PT_OK;
 }
 
-extern "C" int pt_scalar_ls_candidates(const double *gamma, int J, double *gam, void *stream)
+extern "C" int pt_scalar_ls_begin(double *state, void *stream)
 {
     pt::clear_error();
-    PT_CHECK_ARG(gamma && gam && J >= 1 && J <= 16, "scalar_ls_candidates: bad arguments");
-    k_ls_candidates<<<1, 32, 0, (cudaStream_t)stream>>>(gamma, J, gam);
+    PT_CHECK_ARG(state, "scalar_ls_begin: null pointer");
+    k_ls_begin<<<1, 1, 0, (cudaStream_t)stream>>>(state);
+    PT_LAUNCHED("k_ls_begin");
+    return PT_OK;
+}
+
+extern "C" int pt_scalar_ls_candidates(const double *state, int J, double *gam, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(state && gam && J >= 1 && J <= 16, "scalar_ls_candidates: bad arguments");
+    k_ls_candidates<<<1, 32, 0, (cudaStream_t)stream>>>(state, J, gam);
     PT_LAUNCHED("k_ls_candidates");
     return PT_OK;
 }
 
-extern "C" int pt_scalar_ptycho_gamma(const double *data, const double *gam, int J, const double *quad,
-                                      const double *rt, double *gamma, double *coef, void *stream)
+extern "C" int pt_scalar_ls_pass(const double *data, const double *gam, int J, const double *quad, const double *rt,
+                                 double *state, void *stream)
 {
     pt::clear_error();
-    PT_CHECK_ARG(data && gam && quad && rt && gamma && coef && J >= 1 && J <= 16, "scalar_ptycho_gamma: bad arguments");
-    k_ptycho_gamma<<<1, 1, 0, (cudaStream_t)stream>>>(data, gam, J, quad, rt, gamma, coef);
-    PT_LAUNCHED("k_ptycho_gamma");
+    PT_CHECK_ARG(data && gam && quad && rt && state && J >= 1 && J <= 16, "scalar_ls_pass: bad arguments");
+    k_ls_pass<<<1, 1, 0, (cudaStream_t)stream>>>(data, gam, J, quad, rt, state);
+    PT_LAUNCHED("k_ls_pass");
+    return PT_OK;
+}
+
+extern "C" int pt_scalar_ls_end(const double *state, double *coef, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(state && coef, "scalar_ls_end: null pointer");
+    k_ls_end<<<1, 1, 0, (cudaStream_t)stream>>>(state, coef);
+    PT_LAUNCHED("k_ls_end");
     return PT_OK;
 }
 

@@ -152,7 +152,8 @@ __global__ void __launch_bounds__(RPB *TF)
     }
 }
 
-// a random phase per element, keeping the modulus: x <- |x| exp(2 pi i u),
+// a random phase per element, keeping the modulus (floored): x <-
+// sqrt(|x|^2 + floor^2) exp(2 pi i u),
 // u from a counter-based hash of (seed, index) (C. Wellons' "lowbias32"
 // integer hash, applied twice), so probes are reproducible
 __device__ __forceinline__ unsigned mix32(unsigned x)
@@ -164,7 +165,7 @@ __device__ __forceinline__ unsigned mix32(unsigned x)
     x ^= x >> 16;
     return x;
 }
-__global__ void k_random_phase(float2 *__restrict__ x, size_t total, unsigned seed)
+__global__ void k_random_phase(float2 *__restrict__ x, size_t total, unsigned seed, float floor2)
 {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
@@ -173,7 +174,7 @@ __global__ void k_random_phase(float2 *__restrict__ x, size_t total, unsigned se
     float sn, cs;
     sincospif(2.f * u, &sn, &cs);
     const float2 v = x[i];
-    const float m = sqrtf(v.x * v.x + v.y * v.y);
+    const float m = sqrtf(v.x * v.x + v.y * v.y + floor2);
     x[i] = make_float2(m * cs, m * sn);
 }
 
@@ -334,12 +335,17 @@ int run_dft2(pt_precond *h, float2 *dst, const float2 *in, cudaStream_t st)
 // dst = the same modulus spectrum as src with random phases, back in space:
 // IDFT2(|DFT2(src)| exp(2 pi i u)) / L^2 (src and dst may alias)
 template <int L>
-int run_phase_probe(pt_precond *h, float2 *dst, const float2 *src, unsigned seed, cudaStream_t st)
+int run_phase_probe(pt_precond *h, float2 *dst, const float2 *src, unsigned seed, float floor, cudaStream_t st)
 {
-    int rc = run_dft2<L>(h, h->tmp, src, st);
-    if (rc != PT_OK) return rc;
     const size_t tot = (size_t)h->nz * L * L;
-    k_random_phase<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(h->tmp, tot, seed);
+    if (src) {
+        int rc = run_dft2<L>(h, h->tmp, src, st);
+        if (rc != PT_OK) return rc;
+    } else {   // white: unit modulus at every frequency
+        PT_CUDA(cudaMemsetAsync(h->tmp, 0, tot * sizeof(float2), st));
+        floor = 1.f;
+    }
+    k_random_phase<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(h->tmp, tot, seed, floor * floor);
     PT_LAUNCHED("k_random_phase");
     k_pre_cols<L, 2><<<dim3(L / RPB, h->nz), RPB * TF, 0, st>>>(h->tmp, nullptr, 0.f, 0.f, 0.f, 0.f, 0.f, h->tw,
                                                                 nullptr);
@@ -350,10 +356,10 @@ int run_phase_probe(pt_precond *h, float2 *dst, const float2 *src, unsigned seed
     return PT_OK;
 }
 
-int dispatch_phase_probe(pt_precond *h, float2 *dst, const float2 *src, unsigned seed, cudaStream_t st)
+int dispatch_phase_probe(pt_precond *h, float2 *dst, const float2 *src, unsigned seed, float floor, cudaStream_t st)
 {
 #define PT_CASE(L) \
-    if (h->n == L) return run_phase_probe<L>(h, dst, src, seed, st);
+    if (h->n == L) return run_phase_probe<L>(h, dst, src, seed, floor, st);
     PT_PRECOND_SIZES(PT_CASE)
 #undef PT_CASE
     return PT_ERR_UNSUPPORTED;
@@ -580,11 +586,12 @@ extern "C" int pt_precond_dft2(pt_precond *h, void *dst, const void *src, void *
     return dispatch_dft2(h, (float2 *)dst, (const float2 *)src, (cudaStream_t)stream);
 }
 
-extern "C" int pt_precond_phase_probe(pt_precond *h, void *dst, const void *src, unsigned seed, void *stream)
+extern "C" int pt_precond_phase_probe(pt_precond *h, void *dst, const void *src, unsigned seed, float floor,
+                                      void *stream)
 {
     pt::clear_error();
-    PT_CHECK_ARG(h && dst && src, "precond_phase_probe: null pointer");
-    return dispatch_phase_probe(h, (float2 *)dst, (const float2 *)src, seed, (cudaStream_t)stream);
+    PT_CHECK_ARG(h && dst && floor >= 0.f, "precond_phase_probe: bad arguments");
+    return dispatch_phase_probe(h, (float2 *)dst, (const float2 *)src, seed, floor, (cudaStream_t)stream);
 }
 
 extern "C" int pt_precond_targets(const double *num, const double *den, int nn, double den_max_rel, float *y, float *w,

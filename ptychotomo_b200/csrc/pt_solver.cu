@@ -41,8 +41,10 @@ __device__ __forceinline__ void block_reduce_store(double (&acc)[K], double *wor
 }
 
 // one block: out[k] = sum_b work[k * nblk + b] (fixed order per thread, then tree)
-__global__ void k_finish(const double *__restrict__ work, double *__restrict__ out, int K, int nblk, int op_max)
+__global__ void k_finish(const double *__restrict__ work, double *__restrict__ out, int K, int nblk, int op_max,
+                         const double *__restrict__ skip = nullptr)
 {
+    if (skip != nullptr && *skip != 0.0) return;   // a pass the caller's device-side decision made unnecessary
     __shared__ double red[RT];
     for (int k = 0; k < K; ++k) {
         double s = op_max ? -1.0 : 0.0;
@@ -195,8 +197,9 @@ template <int JB, int MODEL, bool ADV = false>
 __global__ void __launch_bounds__(RT) k_ls_frames(const float2 *__restrict__ f, const float2 *__restrict__ d,
                                                   const float *__restrict__ D, float dscale, size_t n,
                                                   const double *__restrict__ gam, int J, double *__restrict__ work,
-                                                  float2 *fo = nullptr)
+                                                  float2 *fo = nullptr, const double *__restrict__ skip = nullptr)
 {
+    if (skip != nullptr && *skip != 0.0) return;   // the whole grid skips together
     double acc[JB];
 #pragma unroll
     for (int j = 0; j < JB; ++j) acc[j] = 0;
@@ -249,14 +252,15 @@ int one_wave(Kern kern)
 
 template <int JB, int MODEL, bool ADV = false>
 int launch_ls_bucket(const float2 *f, const float2 *d, const float *data, float dscale, size_t n,
-                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk, float2 *fo = nullptr)
+                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk, float2 *fo = nullptr,
+                     const double *skip = nullptr)
 {
     const int grid = one_wave(k_ls_frames<JB, MODEL, ADV>);
     if (grid < 0) {
         pt::set_error("ls_frames: occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
         return PT_ERR_CUDA;
     }
-    k_ls_frames<JB, MODEL, ADV><<<grid, RT, 0, st>>>(f, d, data, dscale, n, gammas, J, work, fo);
+    k_ls_frames<JB, MODEL, ADV><<<grid, RT, 0, st>>>(f, d, data, dscale, n, gammas, J, work, fo, skip);
     PT_LAUNCHED("k_ls_frames");
     *nblk = grid;
     return PT_OK;
@@ -265,7 +269,8 @@ int launch_ls_bucket(const float2 *f, const float2 *d, const float *data, float 
 // Launches k_ls_frames; *nblk receives the number of partials per step length.
 // fo != nullptr: the advancing variant (fo = f + gammas[0] d, fo may be f).
 int launch_ls_frames(const float2 *f, const float2 *d, const float *data, float dscale, size_t n, int model,
-                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk, float2 *fo = nullptr)
+                     const double *gammas, int J, double *work, cudaStream_t st, int *nblk, float2 *fo = nullptr,
+                     const double *skip = nullptr)
 {
     if (fo != nullptr) {
         if (model == 0) {
@@ -278,13 +283,13 @@ int launch_ls_frames(const float2 *f, const float2 *d, const float *data, float 
         return launch_ls_bucket<16, 1, true>(f, d, data, dscale, n, gammas, J, work, st, nblk, fo);
     }
     if (model == 0) {
-        if (J <= 2) return launch_ls_bucket<2, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk);
-        if (J <= 8) return launch_ls_bucket<8, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk);
-        return launch_ls_bucket<16, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk);
+        if (J <= 2) return launch_ls_bucket<2, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk, nullptr, skip);
+        if (J <= 8) return launch_ls_bucket<8, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk, nullptr, skip);
+        return launch_ls_bucket<16, 0>(f, d, data, dscale, n, gammas, J, work, st, nblk, nullptr, skip);
     }
-    if (J <= 2) return launch_ls_bucket<2, 1>(f, d, data, dscale, n, gammas, J, work, st, nblk);
-    if (J <= 8) return launch_ls_bucket<8, 1>(f, d, data, dscale, n, gammas, J, work, st, nblk);
-    return launch_ls_bucket<16, 1>(f, d, data, dscale, n, gammas, J, work, st, nblk);
+    if (J <= 2) return launch_ls_bucket<2, 1>(f, d, data, dscale, n, gammas, J, work, st, nblk, nullptr, skip);
+    if (J <= 8) return launch_ls_bucket<8, 1>(f, d, data, dscale, n, gammas, J, work, st, nblk, nullptr, skip);
+    return launch_ls_bucket<16, 1>(f, d, data, dscale, n, gammas, J, work, st, nblk, nullptr, skip);
 }
 
 // Lagrangian data term, solver.py:294-298.  Poisson also subtracts the
@@ -529,6 +534,23 @@ extern "C" int pt_ls_frames_advance(void *f, const void *d, const float *data, f
                                     (double *)work, st, &nblk, (float2 *)f);
     if (rc != PT_OK) return rc;
     k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, J, nblk, 0);
+    PT_LAUNCHED("k_finish");
+    return PT_OK;
+}
+
+extern "C" int pt_ls_frames_dev(const void *f, const void *d, const float *data, float dscale, size_t n, int model,
+                                const double *gammas, int J, void *work, void *out, const double *skip, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(f && d && data && gammas && work && out, "ls_frames_dev: null pointer");
+    PT_CHECK_ARG(J >= 1 && J <= MAXK, "ls_frames_dev: 1 <= J <= %d", MAXK);
+    PT_CHECK_ARG(model == 0 || model == 1, "ls_frames_dev: model 0 (poisson) or 1 (gaussian)");
+    cudaStream_t st = (cudaStream_t)stream;
+    int nblk = 0;
+    const int rc = launch_ls_frames((const float2 *)f, (const float2 *)d, data, dscale, n, model, gammas, J,
+                                    (double *)work, st, &nblk, nullptr, skip);
+    if (rc != PT_OK) return rc;
+    k_finish<<<1, RT, 0, st>>>((const double *)work, (double *)out, J, nblk, 0, skip);
     PT_LAUNCHED("k_finish");
     return PT_OK;
 }

@@ -12,12 +12,11 @@ with torch.cuda.graph and replayed; the first two iterations (piter + 32
 ptycho CG iterations, solver.py:315) run the same sequence eagerly.
 
 Differences from Solver.admm, all by construction of a fixed sequence:
-* the ptycho line search evaluates J step lengths gamma 2^-j (j < J) per CG
-  iteration in one pass (J_first = 16 on a call's first iteration, where
-  gamma restarts from 2; J = 4 after, where gamma persists) and takes the
-  first that passes the reference's test; if none does, that iteration steps
-  by 0 and the next one starts from gamma 2^-J (the host Solver would search
-  further along the same direction);
+* the ptycho line search runs the host Solver's passes of 2, 8 and 16 step
+  lengths (a pass skips itself on the device once an earlier one accepted a
+  step); if none of the 26 candidates passes, that iteration steps by 0 and
+  the next starts from gamma 2^-26 of the first candidate (the host Solver
+  would keep halving along the same direction);
 * F Q psi advances by linearity (F Q (psi + g d) = F Q psi + g F Q d) for
   every step taken, recomputed once per CG call;
 * a CG whose step is 0 keeps iterating with zero steps (the host Solver
@@ -68,19 +67,15 @@ class GraphedADMM:
     with device-resident scalars.
 
     ``data``: the counts (device float32, as Solver.admm takes them);
-    alpha, piter, titer, model: as Solver.admm.  ``J``, ``J_first``: step
-    lengths per ptycho line-search pass (after and on a CG call's first
-    iteration).  ``precond``: a FourierPreconditioner for the tomography
-    subproblem (None: the reference's CG)."""
+    alpha, piter, titer, model: as Solver.admm.  ``precond``: a
+    FourierPreconditioner for the tomography subproblem (None: the
+    reference's CG)."""
 
-    def __init__(self, slv, data, alpha, piter, titer, model, J=4, J_first=16, precond=None):
+    def __init__(self, slv, data, alpha, piter, titer, model, precond=None):
         if slv.ptheta != slv.ntheta_held or slv.nz_held != slv.nz:
             raise ValueError("GraphedADMM needs a Solver with ptheta = ntheta and pnz = nz")
         self.slv, self.alpha, self.piter, self.titer = slv, float(alpha), int(piter), int(titer)
         self.model = _MODELS[model]
-        self.J, self.J_first = int(J), int(J_first)
-        if not (1 <= self.J <= 16 and 1 <= self.J_first <= 16):
-            raise ValueError("1 <= J, J_first <= 16")
         self.precond = precond
         self.data = slv._as_data(data)
         dev = slv.device
@@ -117,6 +112,7 @@ class GraphedADMM:
         self.td = torch.empty((nz, n, n), **c)
         self.work = torch.empty(lib().pt_reduce_workspace_bytes() // 8, dtype=torch.float64, device=dev)
         self.graph = None
+        self.trace = None   # a list: (kind, step) of every CG step of eager iterations (reads back each one)
 
     # ---- state in / out ---------------------------------------------------
     def load(self, st, rho, tau):
@@ -164,7 +160,7 @@ class GraphedADMM:
         rt = A("rt", 2)
         op = slv._ptycho_all
         dscale = slv.coefdata
-        check(lib().pt_scalar_coef2(None, 2.0, None, 0.0, A("pgam", 4), self._st()), "coef2")   # gamma = 2
+        check(lib().pt_scalar_coef2(None, 0.0, None, 2.0, A("pls", 4), self._st()), "coef2")   # gamma = 2
         op.fwd(self.fpsi, self.psi, scale=slv.coefptycho)
         # w = h - psi + lamd / rho: coefficients (1, -1, 1/rho)
         w = A("wcoef", 6)
@@ -186,13 +182,20 @@ class GraphedADMM:
                 self._lin(self.pd, [g, self.pd], A("pbeta", 4))
             op.fwd(self.fd, self.pd, scale=slv.coefptycho)
             self._red(2, A("pq", 3), self.pw, self.pd)
-            J = self.J_first if i == 0 else self.J
-            check(lib().pt_scalar_ls_candidates(A("pgam", 4), J, A("gams", 16), self._st()), "ls_candidates")
-            check(lib().pt_ls_frames(_p(self.fpsi), _p(self.fd), _p(self.data), float(dscale), self.fpsi.numel(),
-                                     self.model, A("gams", 16), J, _p(self.work), A("lsv", 16), self._st()),
-                  "ls_frames")
-            check(lib().pt_scalar_ptycho_gamma(A("lsv", 16), A("gams", 16), J, A("pq", 3), rt, A("pgam", 4),
-                                               A("pstep", 4), self._st()), "ptycho_gamma")
+            # the host's passes of 2, 8 and 16 step lengths; later passes skip
+            # themselves on the device once one accepted a step
+            state = A("pls", 3)
+            check(lib().pt_scalar_ls_begin(state, self._st()), "ls_begin")
+            for J in (2, 8, 16):
+                check(lib().pt_scalar_ls_candidates(state, J, A("gams", 16), self._st()), "ls_candidates")
+                check(lib().pt_ls_frames_dev(_p(self.fpsi), _p(self.fd), _p(self.data), float(dscale),
+                                             self.fpsi.numel(), self.model, A("gams", 16), J, _p(self.work),
+                                             A("lsv", 16), state, self._st()), "ls_frames_dev")
+                check(lib().pt_scalar_ls_pass(A("lsv", 16), A("gams", 16), J, A("pq", 3), rt, state, self._st()),
+                      "ls_pass")
+            check(lib().pt_scalar_ls_end(state, A("pstep", 4), self._st()), "ls_end")
+            if self.trace is not None:
+                self.trace.append(("ptycho", float(A.view("pstep")[2])))
             self._lin(self.psi, [self.psi, self.pd], A("pstep", 4))
             self._lin(self.fpsi, [self.fpsi, self.fd], A("pstep", 4))
 
@@ -277,6 +280,8 @@ class GraphedADMM:
                 check(lib().pt_scalar_tomo_gamma(A("q1", 3), A("q2", 3), rt, A("tgam", 4), A("tstep", 4),
                                                  self._st()), "tomo_gamma")
             st = A("tstep", 4)
+            if self.trace is not None:
+                self.trace.append(("pcg" if pcg else "tomo", float(A.view("tstep")[2])))
             self._lin(u, [u, self.td], st)
             self._lin(Ru, [Ru, self.tRd], st)
             self._lin(a, [a, self.tfd], st)
@@ -321,6 +326,7 @@ class GraphedADMM:
         self.graph = torch.cuda.CUDAGraph()
         saved = {k: getattr(self, k).clone() for k in ("u", "psi", "h", "e", "phi", "lamd", "mu")}
         rt = self.A.view("rt").clone()
+        trace, self.trace = self.trace, None
         s = torch.cuda.Stream(self.dev)
         s.wait_stream(torch.cuda.current_stream(self.dev))
         with torch.cuda.stream(s):
@@ -331,6 +337,7 @@ class GraphedADMM:
         for k, v in saved.items():
             getattr(self, k).copy_(v)
         self.A.view("rt").copy_(rt)
+        self.trace = trace
         torch.cuda.synchronize(self.dev)
 
     def replay(self):

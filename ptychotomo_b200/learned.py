@@ -145,9 +145,9 @@ class FourierPreconditioner:
         check(lib().pt_precond_spectrum(self._h, _p(num), _p(den), _p(z), _p(az), current_stream()),
               "precond spectrum")
 
-    def phase_probe(self, dst, src, seed):
-        check(lib().pt_precond_phase_probe(self._h, _p(dst), _p(src), int(seed) & 0xFFFFFFFF, current_stream()),
-              "precond phase_probe")
+    def phase_probe(self, dst, src, seed, floor=0.0):
+        check(lib().pt_precond_phase_probe(self._h, _p(dst), _p(src), int(seed) & 0xFFFFFFFF, float(floor),
+                                           current_stream()), "precond phase_probe")
         return dst
 
     def free(self):
@@ -162,56 +162,35 @@ class FourierPreconditioner:
             pass
 
 
-def harvest_targets(radon, pre, volumes, cg_iters=4, seed=0):
-    """Training targets from the method's own CG runs.
+def harvest_targets(radon, pre, seeds, probes=4):
+    """Training targets: per-frequency Rayleigh quotients of R^T R.
 
-    For each volume u (a phantom, [nz, n, n] on the device) plain CG runs on
-    min ||s R u' - s R u||^2 from u' = 0 (s = pre.scale; exact adjoint, exact
-    steps).  Every CG residual r_k = s^2 R^T (R u' - R u) becomes a probe z
-    with r_k's modulus spectrum and random phases (so that frequencies
-    decorrelate), and the per-frequency Rayleigh quotient of (z, s^2 R^T R z)
-    accumulates over the residuals and slices:
-        a*(w) = sum Re(conj(Z) AZ) / sum |Z|^2.
-    Returns [(log a*, weight)] per volume, float32 [n * n] each; the weight is
-    1 where the quotient is positive and the probes carry energy, else 0."""
-    from . import kernels as K
+    For each seed, ``probes`` white probes z (unit modulus at every 2-D
+    frequency of every slice, random phases from the seed) and their images
+    s^2 R^T R z (s = pre.scale; the exact adjoint) give
+        a*(w) = sum Re(conj(Z) AZ) / sum |Z|^2   (Z = F2 z, AZ = F2 R^T R z),
+    whose expectation over the phases is the diagonal of R^T R in the
+    Fourier basis, the symbol the preconditioner needs; the slices and probes
+    of a seed average its noise.  Returns [(log a*, weight)] per seed,
+    float32 [n * n] each; the weight is 1 where the quotient is positive.
+    (Probes with the modulus spectrum of CG residuals were tried first: where
+    a residual has little energy the quotient is dominated by leakage from
+    strong frequencies, and the network fit to them slowed the CG down.)"""
     s = pre.scale
-    red = K.Reducer(pre.device)
     n, nz = pre.n, pre.nz
     out = []
     cplx = dict(dtype=torch.complex64, device=pre.device)
-    for v, u_true in enumerate(volumes):
+    z, az = torch.empty((nz, n, n), **cplx), torch.empty((nz, n, n), **cplx)
+    rz = torch.empty((radon.Ntheta, nz, n), **cplx)
+    for seed in seeds:
         num = torch.zeros((n, n), dtype=torch.float64, device=pre.device)
         den = torch.zeros_like(num)
-        data = torch.empty((radon.Ntheta, nz, n), **cplx)
-        radon.fwd(data, u_true, scale=s)
-        u = torch.zeros((nz, n, n), **cplx)
-        res = torch.empty_like(data)          # s R u - data
-        K.lincomb(res, [(-1.0, data)])
-        g = torch.empty_like(u)
-        d = None
-        gg0 = None
-        z, az, rz = torch.empty_like(u), torch.empty_like(u), torch.empty_like(data)
-        for k in range(cg_iters):
-            radon.adj_exact(g, res, scale=s)
-            pre.phase_probe(z, g, seed * 1000003 + v * 1009 + k)
+        for k in range(probes):
+            check(lib().pt_precond_phase_probe(pre._h, _p(z), None, (int(seed) * 7919 + k) & 0xFFFFFFFF, 1.0,
+                                               current_stream()), "precond phase_probe")
             radon.fwd(rz, z, scale=s)
             radon.adj_exact(az, rz, scale=s)
             pre.spectrum(num, den, z, az)
-            gg = red.norm2(g)
-            if d is None:
-                d = K.lincomb(torch.empty_like(g), [(-1.0, g)])
-            else:
-                K.lincomb(d, [(-1.0, g), (gg / gg0, d)])
-            gg0 = gg
-            rd = torch.empty_like(data)
-            radon.fwd(rd, d, scale=s)
-            _, c1, c2 = red.quad3(res, rd)
-            if c2 <= 0:
-                break
-            gam = -c1 / c2
-            K.lincomb(u, [(1.0, u), (gam, d)])
-            K.lincomb(res, [(1.0, res), (gam, rd)])
         y = torch.empty(n * n, dtype=torch.float32, device=pre.device)
         w = torch.empty_like(y)
         check(lib().pt_precond_targets(_p(num), _p(den), n * n, 1e-12, _p(y), _p(w), current_stream()),

@@ -3,11 +3,12 @@
 * A replay equals the same iterations run eagerly, bit for bit (the graph
   holds exactly the eager launch sequence; every kernel is deterministic).
 * The device-scalar iteration tracks the host Solver.admm_step from the same
-  state (each iteration from the host's state before it): the same penalty decisions, psi within 1e-5 and u within 1e-3 (its
-  ptycho line search tries 16 then 4 step lengths per pass and advances F Q
-  psi by linearity, so the arithmetic differs from the host's at FP32
-  rounding; u is the tomography response to psi's phase and amplifies the
-  differences ~100-fold, as in the lock-step test against the oracle).
+  state (each iteration from the host's state before it): the same step
+  lengths, the same penalty decisions, psi within 1e-5 and u within 1e-3
+  (F Q psi advances by linearity instead of the host's occasional new
+  forward, so the arithmetic differs at FP32 rounding; u is the tomography
+  response to psi's phase and amplifies differences ~100-fold, as in the
+  lock-step test against the oracle).
 * With the learned preconditioner, the replay equals the eager run too.
 """
 import pytest
@@ -83,10 +84,18 @@ def test_device_scalar_iteration_tracks_host_solver(problem):
     st, r, t = {k: v.clone() for k, v in st0.items()}, rho, tau
     for m in (2, 3, 4):      # lock-step: both from the host Solver's state before iteration m
         g.load(st, r, t)
+        slv.trace, g.trace = [], []
         st, r, t = slv.admm_step(m, st, r, t, slv._as_data(data), 1e-3, 4, 4, "poisson")
         g.step(m)
         gs, gr, gt = g.state()
         print("m", m, "psi", rel(gs["psi"], st["psi"]), "u", rel(gs["u"], st["u"]))
+        print("  host steps ", slv.trace)
+        print("  graph steps", g.trace)
+        for kind in ("ptycho", "tomo"):   # the host stops a CG at a zero step; the graph steps by 0
+            hs = [v for k, v in slv.trace if k == kind]
+            gs_ = [v for k, v in g.trace if k == kind]
+            assert gs_[:len(hs)] == hs and all(v == 0 for v in gs_[len(hs):]), (kind, hs, gs_)
+        slv.trace = None
         assert (gr, gt) == (r, t)
         assert rel(gs["psi"], st["psi"]) <= 1e-5
         assert rel(gs["u"], st["u"]) <= 1e-3

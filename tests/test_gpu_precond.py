@@ -10,8 +10,9 @@ tomography CG.
   of D^-1/2 F2^-1 p F2 D^-1/2, the phase probes and spectrum statistics;
 * the preconditioned CG keeps the subproblem's minimiser (plain CG, run
   long, judges it: rel-L2 <= 1e-3) and reaches a 1e-4 gradient reduction in
-  fewer iterations than plain CG, with a network trained on the method's
-  own CG runs (training and held-out phantoms).
+  fewer iterations than plain CG, with a network trained by the library's
+  kernels on the symbol measured with random-phase probes (training and
+  held-out probe sets).
 """
 import numpy as np
 import pytest
@@ -182,11 +183,11 @@ def test_pcg_keeps_the_minimiser_and_trained_network_gains(wedge_problem):
     slv, theta = wedge_problem
     n, nz = slv.n, slv.nz
     pre = FourierPreconditioner(slv._tomo_all, T(theta), slv.coeftomo, "cuda")
-    vols = [T(synthetic.phantom(n, nz, seed=100 + s) * 1e5) for s in range(12)]
-    tg = harvest_targets(slv._tomo_all, pre, vols, cg_iters=4, seed=3)
+    tg = harvest_targets(slv._tomo_all, pre, range(100, 112), probes=4)
     net, hist, train_loss, held = train_network(pre.x, tg[:8], tg[8:], steps=800, lr=1e-2, lr_final=1e-3, seed=0)
-    assert hist[-1][1] < 0.2 * hist[0][1], hist
-    assert held < 2.0 * train_loss + 1e-2, (train_loss, held)
+    print("loss history", hist, "held-out", held)
+    assert hist[-1][1] < 0.5 * hist[0][1], hist
+    assert held < 1.5 * train_loss, (train_loss, held)
     pre.set_network(net)
     xi0, xi1, Kt = _subproblem(slv, seed=7)
     u0 = torch.zeros((nz, n, n), dtype=torch.complex64, device="cuda")
