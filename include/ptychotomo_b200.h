@@ -299,8 +299,10 @@ int pt_precond_phase_probe(pt_precond *h, void *dst, const void *src, unsigned s
  * device doubles; reductions (pt_reduce_c64, pt_ls_frames) write into them,
  * the pt_scalar_* one-thread kernels apply the reference's rules there, and
  * the *_dev kernels read them.  Coefficient arrays are (re, im) pairs. */
-/* out = sum_{j<k} coef_j x_j with coef (device double[2k]). */
-int pt_lincomb_dev_c64(void *out, size_t n, int k, const void *const *x, const double *coef, void *stream);
+/* out = sum_{j<k} coef_j x_j with coef (device double[2k]); does nothing when
+ * skip_zero is not NULL and *skip_zero == 0. */
+int pt_lincomb_dev_c64(void *out, size_t n, int k, const void *const *x, const double *coef, const double *skip_zero,
+                       void *stream);
 /* Dai-Yuan beta = g2 / (dg - dg0) (solver.py:194-197; 0 for a zero
  * denominator or first != 0); coef = (-1, 0, beta) for d <- -g + beta d. */
 int pt_scalar_dy_beta(const double *g2, const double *dg, const double *dg0, int first, double *coef, void *stream);
@@ -311,17 +313,24 @@ int pt_scalar_dy_beta(const double *g2, const double *dg, const double *dg0, int
 int pt_scalar_tomo_gamma(const double *q1, const double *q2, const double *rt, double *gamma, double *coef,
                          void *stream);
 /* The ptycho line search (solver.py:171-177 with minf of :208-214) in passes,
- * as Solver.cg_ptycho takes it: state = (accepted, step, gamma).
- * ls_begin clears accepted; ls_candidates writes gam[j] = gamma 2^-j, j < J;
- * ls_pass takes the first j with !(data[j] + rho (2 g_j q[1] - g_j^2 q[2])
- * < 0 and g_j > 1e-12) (step 0 for g_j <= 1e-12) or sets gamma <- g_{J-1}/2,
- * and does nothing once a step was accepted; ls_end writes coef = (1, 0,
- * step) (0 if no pass accepted one). */
+ * as Solver.cg_ptycho takes it: state = (accepted, step, gamma, the step by
+ * which the frames are currently advanced).
+ * ls_begin clears accepted and keeps gamma0 = gamma; ls_candidates writes
+ * gam[j] = gamma 2^-j, j < J; ls_pass takes the first j with !(data[j] + rho
+ * (2 g_j q[1] - g_j^2 q[2]) < 0 and g_j > 1e-12) (step 0 for g_j <= 1e-12) or
+ * sets gamma <- g_{J-1}/2, and does nothing once a step was accepted; ls_end
+ * writes coef = (1, 0, step) (0 if no pass accepted one) and corr = (1, 0,
+ * step - gamma0), the correction of frames that the first pass advanced by
+ * gamma0 (pt_ls_frames_advance). */
 int pt_scalar_ls_begin(double *state, void *stream);
 int pt_scalar_ls_candidates(const double *state, int J, double *gam, void *stream);
 int pt_scalar_ls_pass(const double *data, const double *gam, int J, const double *quad, const double *rt,
                       double *state, void *stream);
-int pt_scalar_ls_end(const double *state, double *coef, void *stream);
+int pt_scalar_ls_end(const double *state, double *coef, double *corr, void *stream);
+/* After the first pass: if it accepted no step, coef = (1, 0, -gamma0) undoes
+ * its advance of the frames (and the state records it); else coef = (1, 0, 0),
+ * for a pass that skips itself (pt_lincomb_dev_c64 with skip_zero = &coef[2]). */
+int pt_scalar_ls_unadvance(double *state, double *coef, void *stream);
 /* pt_ls_frames that does nothing when skip[0] != 0 (a device-side decision
  * made the pass unnecessary); out is then left as it was. */
 int pt_ls_frames_dev(const void *f, const void *d, const float *data, float dscale, size_t n, int model,

@@ -98,13 +98,14 @@ SIGNATURES = {
     "pt_precond_targets": (_int, [_vp, _vp, _int, ctypes.c_double, _vp, _vp, _vp]),
     "pt_precond_phase_probe": (_int, [_vp, _vp, _vp, ctypes.c_uint, _f, _vp]),
     "pt_precond_apply_dev": (_int, [_vp, _vp, _vp, _vp, _vp]),
-    "pt_lincomb_dev_c64": (_int, [_vp, _sz, _int, ctypes.POINTER(_vp), _vp, _vp]),
+    "pt_lincomb_dev_c64": (_int, [_vp, _sz, _int, ctypes.POINTER(_vp), _vp, _vp, _vp]),
     "pt_scalar_dy_beta": (_int, [_vp, _vp, _vp, _int, _vp, _vp]),
     "pt_scalar_tomo_gamma": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pt_scalar_ls_begin": (_int, [_vp, _vp]),
     "pt_scalar_ls_candidates": (_int, [_vp, _int, _vp, _vp]),
     "pt_scalar_ls_pass": (_int, [_vp, _vp, _int, _vp, _vp, _vp, _vp]),
-    "pt_scalar_ls_end": (_int, [_vp, _vp, _vp]),
+    "pt_scalar_ls_end": (_int, [_vp, _vp, _vp, _vp]),
+    "pt_scalar_ls_unadvance": (_int, [_vp, _vp, _vp]),
     "pt_ls_frames_dev": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp, _int, _vp, _vp, _vp, _vp]),
     "pt_scalar_takexi": (_int, [_vp, _vp, ctypes.c_double, _vp, _vp, _vp, _vp]),
     "pt_scalar_multipliers": (_int, [_vp, _vp, _vp, _vp]),

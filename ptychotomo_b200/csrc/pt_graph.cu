@@ -24,9 +24,13 @@ struct LinDev {
     const float2 *x[4];
 };
 
-// out = sum_{j<k} (coef[2j] + i coef[2j+1]) x_j with coefficients in device memory
-__global__ void k_lincomb_dev(float2 *__restrict__ out, size_t n, int k, LinDev p, const double *__restrict__ coef)
+// out = sum_{j<k} (coef[2j] + i coef[2j+1]) x_j with coefficients in device
+// memory; nothing when skip_zero != null and *skip_zero == 0 (a correction
+// the device found unnecessary)
+__global__ void k_lincomb_dev(float2 *__restrict__ out, size_t n, int k, LinDev p, const double *__restrict__ coef,
+                              const double *__restrict__ skip_zero)
 {
+    if (skip_zero != nullptr && *skip_zero == 0.0) return;
     float2 c[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) c[j] = j < k ? make_float2((float)coef[2 * j], (float)coef[2 * j + 1]) : czero();
@@ -88,6 +92,7 @@ __global__ void k_ls_begin(double *__restrict__ state)
 {
     state[0] = 0;
     state[1] = 0;
+    state[3] = state[2];   // the first pass's first step, by which it advances the frames
 }
 
 __global__ void k_ls_candidates(const double *__restrict__ state, int J, double *__restrict__ gam)
@@ -119,13 +124,37 @@ __global__ void k_ls_pass(const double *__restrict__ data, const double *__restr
     state[2] = gam[J - 1] * 0.5;
 }
 
-// coef = (1, 0, step, 0): the step taken (0 if no pass accepted one)
-__global__ void k_ls_end(const double *__restrict__ state, double *__restrict__ coef)
+// after the first pass (which advanced the frames by gamma0 = state[3]): if
+// it accepted no step, the later passes need the frames of psi itself:
+// coef = (1, 0, -gamma0, 0) and state[3] <- 0; else coef = (1, 0, 0, 0),
+// which the correction pass (skip_zero = &coef[2]) skips
+__global__ void k_ls_unadvance(double *__restrict__ state, double *__restrict__ coef)
 {
     coef[0] = 1;
     coef[1] = 0;
-    coef[2] = state[0] != 0 ? state[1] : 0.0;
     coef[3] = 0;
+    if (state[0] == 0) {
+        coef[2] = -state[3];
+        state[3] = 0;
+    } else {
+        coef[2] = 0;
+    }
+}
+
+// coef = (1, 0, step, 0): the step taken (0 if no pass accepted one);
+// corr = (1, 0, step - state[3], 0): what the frames, advanced by state[3],
+// still need
+__global__ void k_ls_end(const double *__restrict__ state, double *__restrict__ coef, double *__restrict__ corr)
+{
+    const double step = state[0] != 0 ? state[1] : 0.0;
+    coef[0] = 1;
+    coef[1] = 0;
+    coef[2] = step;
+    coef[3] = 0;
+    corr[0] = 1;
+    corr[1] = 0;
+    corr[2] = step - state[3];
+    corr[3] = 0;
 }
 
 // takexi scalars (solver.py:151-166): pshift = (m1 + m2) / 2 with
@@ -301,7 +330,8 @@ unsigned ew_blocks(size_t n)
 
 }  // namespace
 
-extern "C" int pt_lincomb_dev_c64(void *out, size_t n, int k, const void *const *x, const double *coef, void *stream)
+extern "C" int pt_lincomb_dev_c64(void *out, size_t n, int k, const void *const *x, const double *coef,
+                                  const double *skip_zero, void *stream)
 {
     pt::clear_error();
     PT_CHECK_ARG(out && x && coef && k >= 1 && k <= 4, "lincomb_dev: 1..4 terms");
@@ -310,7 +340,7 @@ extern "C" int pt_lincomb_dev_c64(void *out, size_t n, int k, const void *const 
         p.x[j] = j < k ? (const float2 *)x[j] : nullptr;
         PT_CHECK_ARG(j >= k || p.x[j], "lincomb_dev: null term %d", j);
     }
-    k_lincomb_dev<<<ew_blocks(n), 256, 0, (cudaStream_t)stream>>>((float2 *)out, n, k, p, coef);
+    k_lincomb_dev<<<ew_blocks(n), 256, 0, (cudaStream_t)stream>>>((float2 *)out, n, k, p, coef, skip_zero);
     PT_LAUNCHED("k_lincomb_dev");
     return PT_OK;
 }
@@ -363,11 +393,20 @@ extern "C" int pt_scalar_ls_pass(const double *data, const double *gam, int J, c
     return PT_OK;
 }
 
-extern "C" int pt_scalar_ls_end(const double *state, double *coef, void *stream)
+extern "C" int pt_scalar_ls_unadvance(double *state, double *coef, void *stream)
 {
     pt::clear_error();
-    PT_CHECK_ARG(state && coef, "scalar_ls_end: null pointer");
-    k_ls_end<<<1, 1, 0, (cudaStream_t)stream>>>(state, coef);
+    PT_CHECK_ARG(state && coef, "scalar_ls_unadvance: null pointer");
+    k_ls_unadvance<<<1, 1, 0, (cudaStream_t)stream>>>(state, coef);
+    PT_LAUNCHED("k_ls_unadvance");
+    return PT_OK;
+}
+
+extern "C" int pt_scalar_ls_end(const double *state, double *coef, double *corr, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(state && coef && corr, "scalar_ls_end: null pointer");
+    k_ls_end<<<1, 1, 0, (cudaStream_t)stream>>>(state, coef, corr);
     PT_LAUNCHED("k_ls_end");
     return PT_OK;
 }

@@ -17,8 +17,11 @@ Differences from Solver.admm, all by construction of a fixed sequence:
   step); if none of the 26 candidates passes, that iteration steps by 0 and
   the next starts from gamma 2^-26 of the first candidate (the host Solver
   would keep halving along the same direction);
-* F Q psi advances by linearity (F Q (psi + g d) = F Q psi + g F Q d) for
-  every step taken, recomputed once per CG call;
+* F Q psi advances by linearity (F Q (psi + g d) = F Q psi + g F Q d): by
+  the first candidate step inside the first line-search pass, as the host's,
+  and by a correction pass (which skips itself when the first candidate was
+  taken) otherwise, where the host computes a new forward; it is recomputed
+  once per CG call;
 * a CG whose step is 0 keeps iterating with zero steps (the host Solver
   breaks out of the loop; the iterate is the same).
 With ``precond`` the tomography subproblem runs the preconditioned CG of
@@ -136,9 +139,10 @@ class GraphedADMM:
         check(lib().pt_reduce_c64(op, _p(a), _p(b) if b is not None else None, n, c0, c1, ncol, _p(self.work),
                                   slot, self._st()), "reduce")
 
-    def _lin(self, out, xs, coef):
+    def _lin(self, out, xs, coef, skip_zero=None):
         arr = (ctypes.c_void_p * 4)(*[_p(x) for x in xs] + [None] * (4 - len(xs)))
-        check(lib().pt_lincomb_dev_c64(_p(out), out.numel(), len(xs), arr, coef, self._st()), "lincomb_dev")
+        check(lib().pt_lincomb_dev_c64(_p(out), out.numel(), len(xs), arr, coef, skip_zero, self._st()),
+              "lincomb_dev")
 
     def _coef(self, name, a0, s0=None, a1=0.0, s1=None):
         """coef slot = (a0 * [s0], 0, a1 * [s1], 0) (s0, s1: slot addresses or None)."""
@@ -188,16 +192,27 @@ class GraphedADMM:
             check(lib().pt_scalar_ls_begin(state, self._st()), "ls_begin")
             for J in (2, 8, 16):
                 check(lib().pt_scalar_ls_candidates(state, J, A("gams", 16), self._st()), "ls_candidates")
-                check(lib().pt_ls_frames_dev(_p(self.fpsi), _p(self.fd), _p(self.data), float(dscale),
-                                             self.fpsi.numel(), self.model, A("gams", 16), J, _p(self.work),
-                                             A("lsv", 16), state, self._st()), "ls_frames_dev")
+                if J == 2:   # the first pass also advances the frames by its first step (as the host's)
+                    check(lib().pt_ls_frames_advance(_p(self.fpsi), _p(self.fd), _p(self.data), float(dscale),
+                                                     self.fpsi.numel(), self.model, A("gams", 16), J,
+                                                     _p(self.work), A("lsv", 16), self._st()), "ls_frames_advance")
+                else:
+                    check(lib().pt_ls_frames_dev(_p(self.fpsi), _p(self.fd), _p(self.data), float(dscale),
+                                                 self.fpsi.numel(), self.model, A("gams", 16), J, _p(self.work),
+                                                 A("lsv", 16), state, self._st()), "ls_frames_dev")
                 check(lib().pt_scalar_ls_pass(A("lsv", 16), A("gams", 16), J, A("pq", 3), rt, state, self._st()),
                       "ls_pass")
-            check(lib().pt_scalar_ls_end(state, A("pstep", 4), self._st()), "ls_end")
+                if J == 2:   # rejected: the later passes need the frames of psi itself
+                    ua = A("punadv", 4)
+                    check(lib().pt_scalar_ls_unadvance(state, ua, self._st()), "ls_unadvance")
+                    self._lin(self.fpsi, [self.fpsi, self.fd], ua, skip_zero=ua + 16)
+            check(lib().pt_scalar_ls_end(state, A("pstep", 4), A("pcorr", 4), self._st()), "ls_end")
             if self.trace is not None:
                 self.trace.append(("ptycho", float(A.view("pstep")[2])))
             self._lin(self.psi, [self.psi, self.pd], A("pstep", 4))
-            self._lin(self.fpsi, [self.fpsi, self.fd], A("pstep", 4))
+            # frames of the new iterate: already there when the first candidate was taken
+            corr = A("pcorr", 4)
+            self._lin(self.fpsi, [self.fpsi, self.fd], corr, skip_zero=corr + 16)
 
     def _takexi(self):
         slv, A = self.slv, self.A
