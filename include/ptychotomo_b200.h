@@ -286,6 +286,9 @@ int pt_precond_spectrum(pt_precond *h, double *num, double *den, const void *z, 
  * float[nn] each).  Reads den back to the host (blocks). */
 int pt_precond_targets(const double *num, const double *den, int nn, double den_max_rel, float *y, float *w,
                        void *stream);
+/* x *= W: a radial window about each slice's centre, 1 within r0 pixels,
+ * falling linearly to 0 at r1 (in place). */
+int pt_precond_window(pt_precond *h, void *x, float r0, float r1, void *stream);
 /* dst = F2 src (unnormalised forward 2-D DFT of every slice). */
 int pt_precond_dft2(pt_precond *h, void *dst, const void *src, void *stream);
 /* dst = F2^-1(sqrt(|F2 src|^2 + floor^2) exp(2 pi i u)) with u uniform from

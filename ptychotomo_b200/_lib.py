@@ -96,6 +96,7 @@ SIGNATURES = {
     "pt_precond_spectrum": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "pt_precond_dft2": (_int, [_vp, _vp, _vp, _vp]),
     "pt_precond_targets": (_int, [_vp, _vp, _int, ctypes.c_double, _vp, _vp, _vp]),
+    "pt_precond_window": (_int, [_vp, _vp, _f, _f, _vp]),
     "pt_precond_phase_probe": (_int, [_vp, _vp, _vp, ctypes.c_uint, _f, _vp]),
     "pt_precond_apply_dev": (_int, [_vp, _vp, _vp, _vp, _vp]),
     "pt_lincomb_dev_c64": (_int, [_vp, _sz, _int, ctypes.POINTER(_vp), _vp, _vp, _vp]),

@@ -236,6 +236,20 @@ __global__ void k_targets(const double *__restrict__ num, const double *__restri
     w[i] = ok ? 1.f : 0.f;
 }
 
+// x[z][y][x] *= W(y, x): a radial window, 1 inside radius r0 (pixels, about
+// the slice centre), falling linearly to 0 at r1; probes that vanish near
+// the slice border see the interior operator (no edge replication)
+__global__ void k_window(float2 *__restrict__ x, int nz, int n, float r0, float r1)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)nz * n * n) return;
+    const int c = (int)(i % n), r = (int)((i / n) % n);
+    const float dx = c - 0.5f * (n - 1), dy = r - 0.5f * (n - 1);
+    const float d = sqrtf(dx * dx + dy * dy);
+    const float w = d <= r0 ? 1.f : (d >= r1 ? 0.f : (r1 - d) / (r1 - r0));
+    x[i] = w * x[i];
+}
+
 __global__ void k_exp(const float *__restrict__ z, float *__restrict__ a, int nn)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -607,6 +621,16 @@ extern "C" int pt_precond_targets(const double *num, const double *den, int nn, 
     for (double v : hd) mx = v > mx ? v : mx;
     k_targets<<<(nn + 255) / 256, 256, 0, (cudaStream_t)stream>>>(num, den, nn, den_max_rel * mx, y, w);
     PT_LAUNCHED("k_targets");
+    return PT_OK;
+}
+
+extern "C" int pt_precond_window(pt_precond *h, void *x, float r0, float r1, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h && x && r0 >= 0.f && r1 > r0, "precond_window: bad arguments");
+    const size_t tot = (size_t)h->nz * h->n * h->n;
+    k_window<<<(unsigned)((tot + 255) / 256), 256, 0, (cudaStream_t)stream>>>((float2 *)x, h->nz, h->n, r0, r1);
+    PT_LAUNCHED("k_window");
     return PT_OK;
 }
 

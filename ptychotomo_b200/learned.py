@@ -162,20 +162,26 @@ class FourierPreconditioner:
             pass
 
 
-def harvest_targets(radon, pre, seeds, probes=4):
-    """Training targets: per-frequency Rayleigh quotients of R^T R.
+def harvest_targets(radon, pre, seeds, probes=4, window=(0.30, 0.42)):
+    """Training targets: per-frequency Rayleigh quotients of the interior
+    part of R^T R.
 
-    For each seed, ``probes`` white probes z (unit modulus at every 2-D
-    frequency of every slice, random phases from the seed) and their images
-    s^2 R^T R z (s = pre.scale; the exact adjoint) give
-        a*(w) = sum Re(conj(Z) AZ) / sum |Z|^2   (Z = F2 z, AZ = F2 R^T R z),
-    whose expectation over the phases is the diagonal of R^T R in the
-    Fourier basis, the symbol the preconditioner needs; the slices and probes
-    of a seed average its noise.  Returns [(log a*, weight)] per seed,
-    float32 [n * n] each; the weight is 1 where the quotient is positive.
-    (Probes with the modulus spectrum of CG residuals were tried first: where
-    a residual has little energy the quotient is dominated by leakage from
-    strong frequencies, and the network fit to them slowed the CG down.)"""
+    For each seed, ``probes`` white probes (unit modulus at every 2-D
+    frequency of every slice, random phases from the seed), windowed to the
+    slice interior (radial window W, 1 within window[0] n, 0 beyond
+    window[1] n), give z = W z0 and A z = W s^2 R^T R z (s = pre.scale; the
+    exact adjoint), and
+        a*(w) = sum Re(conj(Z) AZ) / sum |Z|^2   (Z = F2 z, AZ = F2 A z),
+    the symbol of the operator away from the border, where the forward's
+    edge replication makes the diagonal 8-54 times larger (the diagonal D of
+    the preconditioner handles the border; unwindowed probes spread that
+    border weight over every frequency, a white bias that swamps the small
+    high-frequency symbol).  The slices and probes of a seed average its
+    noise.  Returns [(log a*, weight)] per seed, float32 [n * n] each; the
+    weight is 1 where the quotient is positive.  (Probes with the modulus
+    spectrum of CG residuals were tried first: where a residual has little
+    energy the quotient is dominated by leakage from strong frequencies, and
+    the network fit to them slowed the CG down.)"""
     s = pre.scale
     n, nz = pre.n, pre.nz
     out = []
@@ -188,8 +194,14 @@ def harvest_targets(radon, pre, seeds, probes=4):
         for k in range(probes):
             check(lib().pt_precond_phase_probe(pre._h, _p(z), None, (int(seed) * 7919 + k) & 0xFFFFFFFF, 1.0,
                                                current_stream()), "precond phase_probe")
+            if window is not None:
+                check(lib().pt_precond_window(pre._h, _p(z), window[0] * n, window[1] * n, current_stream()),
+                      "precond window")
             radon.fwd(rz, z, scale=s)
             radon.adj_exact(az, rz, scale=s)
+            if window is not None:
+                check(lib().pt_precond_window(pre._h, _p(az), window[0] * n, window[1] * n, current_stream()),
+                      "precond window")
             pre.spectrum(num, den, z, az)
         y = torch.empty(n * n, dtype=torch.float32, device=pre.device)
         w = torch.empty_like(y)
