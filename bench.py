@@ -77,25 +77,31 @@ def config_dict(c, extra=None):
 
 
 # DRAM bytes (read + write) of the ptycho adjoint kernel k_ptycho_adj128 per
-# 128^2 detector frame, from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum, one launch, --clock-control none) of
-#   python bench.py --ntheta 148 --steps 1 --warmup 1 --no-e2e --no-cpu-baseline
-# at 256^3: 3,691,507,712 + 500,559,104 bytes for 148 x 169 = 25,012 frames.
-# 148 angles are one wave of one-slab angle blocks, the per-wave layout of the
-# 384-angle workload, so the figure is scaled by the frame count of the run.
-PTYCHO_ADJ128_DRAM_PER_FRAME = (3691507712 + 500559104) / 25012
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_ptycho_adj128 launch at 148 angles "
-                  "(25,012 frames of 128^2, 256^3 object): %.0f B per frame, scaled by this run's frames"
-                  % PTYCHO_ADJ128_DRAM_PER_FRAME)
+# 128^2 detector frame at 256^3, by the adjoint's angle split (parts), each
+# from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one
+# launch, --clock-control none) of
+#   python bench.py --ntheta 148 [--no-autotune --ptycho-parts P] --steps 1 --warmup 1 --no-e2e --no-cpu-baseline
+# parts 1: 3,691,507,712 + 500,559,104 bytes for 148 x 169 = 25,012 frames.
+# 148 angles are one wave of one-slab angle blocks (parts x 148 blocks for a
+# split), the per-wave layout of the 384-angle workload, so the figure is
+# scaled by the frame count of the run.
+PTYCHO_ADJ128_DRAM_PER_FRAME = {1: (3691507712 + 500559104) / 25012}
 
 
-def dram_traffic(c):
-    """DRAM bytes per ptycho-adjoint call, scaled from the per-frame capture;
-    None where the capture does not apply (other detector, probe or object
-    sizes, or fewer angles than SMs, where the angles are split into parts)."""
-    if (c["det"], c["nprb"], c["n"], c["nz"]) != (128, 128, 256, 256) or c["ntheta"] < 148:
+def traffic_source(parts):
+    return ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_ptycho_adj128 launch (parts %d) at 148 "
+            "angles (25,012 frames of 128^2, 256^3 object): %.0f B per frame, scaled by this run's frames"
+            % (parts, PTYCHO_ADJ128_DRAM_PER_FRAME[parts]))
+
+
+def dram_traffic(c, parts):
+    """DRAM bytes per ptycho-adjoint kernel launch, scaled from the per-frame
+    capture of the same split; None where no capture applies (other detector,
+    probe or object sizes, fewer angles than SMs, or an uncaptured split)."""
+    if ((c["det"], c["nprb"], c["n"], c["nz"]) != (128, 128, 256, 256) or c["ntheta"] < 148
+            or parts not in PTYCHO_ADJ128_DRAM_PER_FRAME):
         return None
-    return int(round(PTYCHO_ADJ128_DRAM_PER_FRAME * c["ntheta"] * c["nside"] ** 2))
+    return int(round(PTYCHO_ADJ128_DRAM_PER_FRAME[parts] * c["ntheta"] * c["nside"] ** 2))
 
 
 # ----------------------------------------------------------------------------
@@ -288,6 +294,9 @@ def run_ours(args, rank, world, local):
     ops = Ops(c, torch, dev)
     if not args.no_autotune:
         ops.autotune()
+    if args.ptycho_parts:
+        ops.ptycho.parts = args.ptycho_parts
+        ops.tuned = dict(ops.tuned or {}, ptycho_adj_parts=args.ptycho_parts, parts_source="--ptycho-parts")
     bytes_op = workload_bytes(c)
     step_bytes = sum(bytes_op.values())
 
@@ -356,7 +365,7 @@ def run_ours(args, rank, world, local):
     # the ptycho adjoint (k_ptycho_adj128): the largest single kernel of the step
     dom = "ptycho_adj"
     achieved = bytes_op[dom] / (per_op[dom] * 1e-3) / 1e9
-    traffic = dram_traffic(c)
+    traffic = dram_traffic(c, ops.ptycho.parts)
 
     line = {"metric": "operator HBM GB/s (radonusfft fwd+adj + ptychofft fwd+adj, 256^3)",
             "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -371,7 +380,7 @@ def run_ours(args, rank, world, local):
             "gpu_launches": ops.launches_per_step() * args.steps,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "traffic_source": TRAFFIC_SOURCE if traffic is not None else None,
+                         "traffic_source": traffic_source(ops.ptycho.parts) if traffic is not None else None,
                          "peak_source": peak_src + " hbm_gbs (copy, burst)"},
             "clocks": clk.summary()}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1273,6 +1282,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the operators' default variants")
+    ap.add_argument("--ptycho-parts", type=int, default=None, help="fix the ptycho adjoint's angle split")
     ap.add_argument("--ntheta", type=int, default=None, help="override the angle count (small profiling cases)")
     ap.add_argument("--nz", type=int, default=None, help="override the slice count (small profiling cases)")
     ap.add_argument("--admm", action="store_true", help="ADMM wall time instead of operator throughput")

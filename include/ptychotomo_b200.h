@@ -145,6 +145,9 @@ int pt_ptycho_fwd_probe(pt_ptycho *h, void *g, const void *psi, const void *prb,
  * wave-count model).  f, g: caller buffers of the adjoint's shapes (f is
  * overwritten).  Allocates the slabs; blocks the host. */
 int pt_ptycho_autotune(pt_ptycho *h, void *f, const void *g, int trials, int *parts_out, void *stream);
+/* Sets the adjoint's split (1 <= parts <= Nscan; detectors below 16 keep
+ * their one split) and allocates its slabs. */
+int pt_ptycho_set_parts(pt_ptycho *h, int parts);
 /* The adjoint's current split. */
 int pt_ptycho_get_parts(const pt_ptycho *h, int *parts);
 

@@ -1458,6 +1458,29 @@ extern "C" int pt_ptycho_autotune(pt_ptycho *h, void *f, const void *g, int tria
     return rc;
 }
 
+extern "C" int pt_ptycho_set_parts(pt_ptycho *h, int parts)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h && parts >= 1 && (size_t)parts <= h->nscan, "ptychofft.set_parts: parts must be in [1, nscan]");
+    if (h->det < 16) {
+        PT_CHECK_ARG(parts == h->parts, "ptychofft.set_parts: the small-detector kernel has no angle split");
+        return PT_OK;
+    }
+    if (h->partial) {
+        cudaFree(h->partial);
+        h->partial = nullptr;
+    }
+    h->parts = parts;
+    if (parts > 1 &&
+        cudaMalloc((void **)&h->partial, (size_t)parts * h->ntheta * h->nz * h->n * sizeof(float2)) != cudaSuccess) {
+        cudaGetLastError();
+        h->parts = 1;
+        pt::set_error("ptychofft.set_parts: the split's slabs could not be allocated");
+        return PT_ERR_ALLOC;
+    }
+    return PT_OK;
+}
+
 extern "C" int pt_ptycho_get_parts(const pt_ptycho *h, int *parts)
 {
     pt::clear_error();

@@ -131,6 +131,10 @@ class ptychofft:  # noqa: N801 - reference class name
         check(lib().pt_ptycho_get_parts(self._h, ctypes.byref(out)), "ptychofft.parts")
         return out.value
 
+    @parts.setter
+    def parts(self, value):
+        check(lib().pt_ptycho_set_parts(self._h, int(value)), "ptychofft.parts")
+
     def adj_resid(self, f, fpsi, data, dscale, model, scale=1.0, stream=None):
         """Gradient of the data term: f = scale * Q* F* residual(fpsi, dscale * data)."""
         check(lib().pt_ptycho_adj_resid(self._h, as_ptr(f), as_ptr(fpsi), as_ptr(data), float(dscale), int(model),
