@@ -297,6 +297,11 @@ def run_ours(args, rank, world, local):
     if args.ptycho_parts:
         ops.ptycho.parts = args.ptycho_parts
         ops.tuned = dict(ops.tuned or {}, ptycho_adj_parts=args.ptycho_parts, parts_source="--ptycho-parts")
+    if args.radon_variant:
+        streams, tiled = (int(v) for v in args.radon_variant.split(","))
+        ops.radon.set_variant(streams, bool(tiled))
+        ops.tuned = dict(ops.tuned or {}, radon_fwd_streams=streams, radon_gather="smem tiles" if tiled else "L1",
+                         radon_source="--radon-variant")
     bytes_op = workload_bytes(c)
     step_bytes = sum(bytes_op.values())
 
@@ -1283,6 +1288,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the operators' default variants")
     ap.add_argument("--ptycho-parts", type=int, default=None, help="fix the ptycho adjoint's angle split")
+    ap.add_argument("--radon-variant", default=None, help="fix the radon forward: STREAMS,TILED (e.g. 2,1)")
     ap.add_argument("--ntheta", type=int, default=None, help="override the angle count (small profiling cases)")
     ap.add_argument("--nz", type=int, default=None, help="override the slice count (small profiling cases)")
     ap.add_argument("--admm", action="store_true", help="ADMM wall time instead of operator throughput")

@@ -150,6 +150,20 @@ int pt_ptycho_autotune(pt_ptycho *h, void *f, const void *g, int trials, int *pa
 int pt_ptycho_set_parts(pt_ptycho *h, int parts);
 /* The adjoint's current split. */
 int pt_ptycho_get_parts(const pt_ptycho *h, int *parts);
+/* Sub-pixel scan model (no counterpart in the reference, which rounds each
+ * scan position to the grid and applies a constant per-scan phase,
+ * kernels.cuh:306-336 / ptychofft.cu:58-93).  quant > 0: the frame of scan
+ * s is F(P(r - d) psi(c + r)) with c = round(s), d = s - c quantised to
+ * multiples of 1/quant pixel, P(r - d) the band-limited (Dirichlet-kernel)
+ * interpolation of the probe, and no per-scan phase; fwd, adj and the fused
+ * residual adjoints all follow it.  quant = 0 restores the reference model.
+ * Builds one shifted probe table per distinct offset pair (at most 2 GiB;
+ * rebuilt by every later setobj), needs setobj first and a detector of 16 or
+ * more; probe retrieval is refused while it is on.  Set-up: allocates,
+ * blocks the host. */
+int pt_ptycho_set_subpixel(pt_ptycho *h, int quant, void *stream);
+/* The sub-pixel model's quantisation (0: off) and its number of tables. */
+int pt_ptycho_get_subpixel(const pt_ptycho *h, int *quant, int *ntables);
 
 
 /* ---- Solver arithmetic (src/ptychotomo/solver.py:48-336) -----------------

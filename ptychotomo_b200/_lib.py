@@ -67,6 +67,8 @@ SIGNATURES = {
     "pt_ptycho_autotune": (_int, [_vp, _vp, _vp, _int, ctypes.POINTER(_int), _vp]),
     "pt_ptycho_get_parts": (_int, [_vp, ctypes.POINTER(_int)]),
     "pt_ptycho_set_parts": (_int, [_vp, _int]),
+    "pt_ptycho_set_subpixel": (_int, [_vp, _int, _vp]),
+    "pt_ptycho_get_subpixel": (_int, [_vp, ctypes.POINTER(_int), ctypes.POINTER(_int)]),
     "pt_radon_autotune": (_int, [_vp, _vp, _vp, _int, ctypes.POINTER(_int), _vp]),
     "pt_radon_set_variant": (_int, [_vp, _int, _int]),
     "pt_reduce_workspace_bytes": (_sz, []),

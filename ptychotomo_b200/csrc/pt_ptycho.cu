@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstdint>
+#include <map>
 #include <vector>
 
 #include "pt_common.cuh"
@@ -58,15 +59,18 @@ template <int DET>
 constexpr int ptycho_block() { return DET * ptycho_fft_threads<DET>(); }
 
 // setobj tables: integer corners (kernels.cuh:255-256) and the per-scan
-// phase shiftx*shifty (takeshifts, kernels.cuh:306-317, same expressions).
+// phase shiftx*shifty (takeshifts, kernels.cuh:306-317, same expressions);
+// frac: the offsets s - round(s) in [-1/2, 1/2] (the sub-pixel model's shifts).
 __global__ void k_ptycho_tables(const float *__restrict__ scan, int *__restrict__ corner,
-                                float2 *__restrict__ phase, int nframes)
+                                float2 *__restrict__ phase, float *__restrict__ frac, int nframes)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nframes) return;
     const float sx = scan[i], sy = scan[nframes + i];
     corner[2 * i] = (int)roundf(sx);
     corner[2 * i + 1] = (int)roundf(sy);
+    frac[2 * i] = sx - roundf(sx);
+    frac[2 * i + 1] = sy - roundf(sy);
     float2 px, py;
     px.x = cosf(2 * PI_REF * (sx - roundf(sx)));
     px.y = sinf(2 * PI_REF * (sx - roundf(sx)));
@@ -204,7 +208,7 @@ template <int DET>
 __global__ void __launch_bounds__(PF<DET>::NT, 1)
     k_ptycho_fwd(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
                  const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                 int nframes, int P, float scale, const float2 *__restrict__ tw)
+                 int nframes, int P, float scale, const float2 *__restrict__ tw, const int *__restrict__ sid = nullptr)
 {
     using F = PF<DET>;
     extern __shared__ float2 sm[];
@@ -224,6 +228,7 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
             continue;
         }
         const float2 *src = psi + ((size_t)th * nz + sty) * n + stx;
+        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
         float2 v[F::CPG][F::N1];
         // along the object row: line = detector column iy, points ix = t + N2 m
 #pragma unroll
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
                 const int px = t + F::N2 * m - off;
                 float2 val = czero();
                 if (py >= 0 && py < P && px >= 0 && px < P)
-                    val = cmul(__ldg(&prbT[py * P + px]), __ldg(&src[(size_t)py * n + px]));
+                    val = cmul(__ldg(&pr[py * P + px]), __ldg(&src[(size_t)py * n + px]));
                 v[c][m] = val;
             }
             line_dft<DET, -1>(v[c], t, sc, tws);
@@ -280,7 +285,8 @@ template <int DET, int RESID>
 __global__ void __launch_bounds__(PF<DET>::NT, 1)
     k_ptycho_adj(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                  const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                 int P, float scale, const float2 *__restrict__ tw, const float *__restrict__ data, float dscale)
+                 int P, float scale, const float2 *__restrict__ tw, const float *__restrict__ data, float dscale,
+                 const int *__restrict__ sid = nullptr)
 {
     using F = PF<DET>;
     extern __shared__ float2 sm[];
@@ -299,6 +305,7 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
         const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
         if (stx < 0 || sty < 0) continue;
         const float2 ph = phase[fid];
+        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;
         const float2 *in = g + (size_t)fid * DET * DET;
         float2 v[F::CPG][F::N1];
         // along the detector row: line = kx, points ky = t + N2 m (contiguous)
@@ -353,7 +360,7 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
                 for (int j = 0; j < F::KPT; ++j) {
                     const int px = t * F::KPT + j + F::N1 * k2 - off;
                     if (px >= 0 && px < P)
-                        row[px] = cur[j * F::N2 + k2] + cmulc(__ldg(&prbT[py * P + px]), v[c][j * F::N2 + k2]);
+                        row[px] = cur[j * F::N2 + k2] + cmulc(__ldg(&pr[py * P + px]), v[c][j * F::N2 + k2]);
                 }
         }
         __syncthreads();
@@ -447,7 +454,8 @@ template <bool FULL>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_fwd128(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                    int nframes, int P, float scale, const float4 *__restrict__ tw)
+                    int nframes, int P, float scale, const float4 *__restrict__ tw,
+                    const int *__restrict__ sid = nullptr)
 {
     extern __shared__ float4 sm4[];
     float4 *fr = sm4;
@@ -468,6 +476,7 @@ __global__ void __launch_bounds__(512, 1)
             continue;
         }
         const float2 *src = psi + ((size_t)th * nz + sty) * n + stx;
+        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
         float2 v[2][16];
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -476,11 +485,11 @@ __global__ void __launch_bounds__(512, 1)
             for (int m = 0; m < 16; ++m) {
                 const int px = t + 8 * m - off;
                 if (FULL) {
-                    v[c][m] = cmul(__ldg(&prbT[py * P + px]), __ldg(&src[(size_t)py * n + px]));
+                    v[c][m] = cmul(__ldg(&pr[py * P + px]), __ldg(&src[(size_t)py * n + px]));
                 } else {
                     float2 val = czero();
                     if (py >= 0 && py < P && px >= 0 && px < P)
-                        val = cmul(__ldg(&prbT[py * P + px]), __ldg(&src[(size_t)py * n + px]));
+                        val = cmul(__ldg(&pr[py * P + px]), __ldg(&src[(size_t)py * n + px]));
                     v[c][m] = val;
                 }
             }
@@ -599,7 +608,7 @@ __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
                     int P, float scale, const float4 *__restrict__ tw, const float *__restrict__ data,
-                    float dscale)
+                    float dscale, const int *__restrict__ sid = nullptr)
 {
     // SLOT2: the second line of a group exchanges through the group's own
     // prefetch row (already in registers), and the next frame's row is
@@ -660,6 +669,7 @@ __global__ void __launch_bounds__(512, 1)
             continue;
         }
         const float2 ph = FOLD ? make_float2(1.f, 0.f) : phase[fid];
+        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
         float2 v[2][16];
         // rows 64..127 from global first, so their latency hides behind row 0..63's work
 #pragma unroll
@@ -715,7 +725,7 @@ __global__ void __launch_bounds__(512, 1)
             if (!FULL && (py < 0 || py >= P)) continue;
             float2 *row = slab + (size_t)(sty + py) * n + stx;
             if (vec && (stx & 1) == 0) {
-                rmw_row16(row, prbT + (size_t)py * 128, v[c], t);
+                rmw_row16(row, pr + (size_t)py * 128, v[c], t);
                 continue;
             }
             // all 16 slab values are loaded before any is stored back, so the
@@ -734,7 +744,7 @@ __global__ void __launch_bounds__(512, 1)
                 for (int j = 0; j < 2; ++j) {
                     const int px = 2 * t + j + 16 * k2 - off;
                     if (FULL || (px >= 0 && px < P))
-                        row[px] = cur[j * 8 + k2] + cmulc(__ldg(&prbT[py * P + px]), v[c][j * 8 + k2]);
+                        row[px] = cur[j * 8 + k2] + cmulc(__ldg(&pr[py * P + px]), v[c][j * 8 + k2]);
                 }
         }
     }
@@ -755,7 +765,8 @@ __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128v(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
                     int P, float scale, const float4 *__restrict__ tw, const float *__restrict__ data,
-                    float dscale, const float2 *__restrict__ psi = nullptr, int nframes = 0)
+                    float dscale, const float2 *__restrict__ psi = nullptr, int nframes = 0,
+                    const int *__restrict__ sid = nullptr)
 {
     extern __shared__ float4 sm4[];
     float4 *fr = sm4;
@@ -810,6 +821,7 @@ __global__ void __launch_bounds__(512, 1)
             continue;
         }
         const float2 ph = FOLD ? make_float2(1.f, 0.f) : phase[fid];
+        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
         float2 v[2][16];
         // rows 64..127 from global first, so their latency hides behind row 0..63's work
 #pragma unroll
@@ -864,7 +876,7 @@ __global__ void __launch_bounds__(512, 1)
             if (!FULL && (py < 0 || py >= P)) continue;
             // object: slab row += conj(c prbT) x; probe: partial row += conj(psi) x
             float2 *row = PROBE ? slab + (size_t)py * P : slab + (size_t)(sty + py) * n + stx;
-            const float2 *mul = PROBE ? psi + ((size_t)th * nz + sty + py) * n + stx : prbT + (size_t)py * P;
+            const float2 *mul = PROBE ? psi + ((size_t)th * nz + sty + py) * n + stx : pr + (size_t)py * P;
             if (vec && (stx & 1) == 0) {
                 rmw_row16(row, mul, v[c], t);
                 continue;
@@ -1012,6 +1024,63 @@ __global__ void k_probe_reduce(const float2 *__restrict__ part, float2 *__restri
 
 }  // namespace
 
+// ---- sub-pixel scan model (no counterpart in the reference) -----------------
+// The reference rounds each scan position s to the object grid and multiplies
+// the frame by a constant phase (kernels.cuh:306-336), which leaves the
+// intensities unchanged.  The sub-pixel model keeps the object on its grid and
+// evaluates the probe at the scan's offset instead: the exit wave is
+// P(r - d) psi(c + r), c = round(s), d = s - c in [-1/2, 1/2]^2, r the patch
+// pixel, with P(r - d) the band-limited (trigonometric) interpolation of the
+// probe's samples, separable in x and y:
+//   P_d[y][x] = sum_{i,j} D(y - dy - i) P[i][j] D(x - dx - j),
+//   D(t) = sin(pi t) / (P tan(pi t / P))  (even P;  P sin(pi t / P) for odd P),
+// the Dirichlet kernel whose spectrum is 1 below Nyquist and cos(pi d) at it.
+// Offsets are quantised to multiples of 1/quant pixel; one shifted table is
+// kept per distinct offset pair and each frame indexes its own.
+
+// tmp[s][i][x] = sum_j prbT[i][j] MxT[kx_s][j][x]   (one thread per (s, i, x))
+__global__ void k_probe_shift_x(const float2 *__restrict__ prbT, const float *__restrict__ mxT,
+                                const int2 *__restrict__ pairs, float2 *__restrict__ tmp, int P, int npairs)
+{
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)npairs * P * P) return;
+    const int x = (int)(e % P), i = (int)((e / P) % P), sidx = (int)(e / ((size_t)P * P));
+    const float *m = mxT + (size_t)pairs[sidx].x * P * P;
+    double re = 0, im = 0;
+    for (int j = 0; j < P; ++j) {
+        const float2 v = prbT[(size_t)i * P + j];
+        const double w = m[(size_t)j * P + x];
+        re += w * v.x;
+        im += w * v.y;
+    }
+    tmp[e] = make_float2((float)re, (float)im);
+}
+
+// out[s][y][x] = sum_i My[ky_s][y][i] tmp[s][i][x]
+__global__ void k_probe_shift_y(const float2 *__restrict__ tmp, const float *__restrict__ my,
+                                const int2 *__restrict__ pairs, float2 *__restrict__ out, int P, int npairs)
+{
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)npairs * P * P) return;
+    const int x = (int)(e % P), y = (int)((e / P) % P), sidx = (int)(e / ((size_t)P * P));
+    const float *m = my + (size_t)pairs[sidx].y * P * P + (size_t)y * P;
+    const float2 *src = tmp + (size_t)sidx * P * P + x;
+    double re = 0, im = 0;
+    for (int i = 0; i < P; ++i) {
+        const float2 v = src[(size_t)i * P];
+        const double w = m[i];
+        re += w * v.x;
+        im += w * v.y;
+    }
+    out[e] = make_float2((float)re, (float)im);
+}
+
+__global__ void k_fill_one(float2 *__restrict__ a, size_t n)
+{
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n) a[e] = make_float2(1.f, 0.f);
+}
+
 struct pt_ptycho {
     int ntheta = 0, nz = 0, n = 0, nscan = 0, det = 0, P = 0, parts = 1;
     int device = -1;
@@ -1024,6 +1093,17 @@ struct pt_ptycho {
     // probe) and one P x P partial per block of the probe adjoint
     float2 *prbT2 = nullptr, *prb_part = nullptr;
     int prb_blocks = 0;
+    // sub-pixel scan model (quant > 0): frac = per-frame offsets s - round(s);
+    // prbS = one shifted probe table per distinct quantised offset pair (prbT
+    // layout), sid = each frame's table, ones = the unit phase the model uses
+    float *frac = nullptr;
+    float2 *prbS = nullptr, *ones = nullptr;
+    int *sid = nullptr;
+    int quant = 0, nshift = 0;
+    // the tables the kernels take
+    const float2 *probe_tab() const { return quant ? prbS : prbT; }
+    const float2 *phase_tab() const { return quant ? ones : phase; }
+    const int *shift_ids() const { return quant ? sid : nullptr; }
 };
 
 namespace {
@@ -1087,21 +1167,22 @@ int ptycho_adj_launch(pt_ptycho *h, float2 *out, const float2 *in, float scale, 
         const int smem = RESID ? P128_SMEM_RESID : P128_SMEM;
         if (fast128 && h->P == DET) {
             if constexpr (RESID == 2)
-                k_ptycho_adj128v<true, RESID, false><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase, h->prbT,
-                                                                             h->nz, h->n, h->nscan, h->P, scale,
-                                                                             h->tw128, data, dscale);
+                k_ptycho_adj128v<true, RESID, false><<<grid, 512, smem, st>>>(
+                    in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale, h->tw128,
+                    data, dscale, nullptr, 0, h->shift_ids());
             else
-                k_ptycho_adj128<true, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz,
-                                                                     h->n, h->nscan, h->P, scale, h->tw128, data,
-                                                                     dscale);
+                k_ptycho_adj128<true, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase_tab(),
+                                                                     h->probe_tab(), h->nz, h->n, h->nscan, h->P,
+                                                                     scale, h->tw128, data, dscale, h->shift_ids());
         }
         else if (fast128)
-            k_ptycho_adj128<false, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz,
-                                                                  h->n, h->nscan, h->P, scale, h->tw128, data,
-                                                                  dscale);
+            k_ptycho_adj128<false, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase_tab(), h->probe_tab(),
+                                                                  h->nz, h->n, h->nscan, h->P, scale, h->tw128, data,
+                                                                  dscale, h->shift_ids());
         else
-            k_ptycho_adj<DET, RESID><<<grid, F::NT, F::SMEM, st>>>(in, dst, h->corner, h->phase, h->prbT, h->nz, h->n,
-                                                                  h->nscan, h->P, scale, h->tw, data, dscale);
+            k_ptycho_adj<DET, RESID><<<grid, F::NT, F::SMEM, st>>>(in, dst, h->corner, h->phase_tab(), h->probe_tab(),
+                                                                  h->nz, h->n, h->nscan, h->P, scale, h->tw, data,
+                                                                  dscale, h->shift_ids());
         PT_LAUNCHED("k_ptycho_adj");
         if (h->parts > 1) {
             const size_t slab = (size_t)h->nz * h->n, total = slab * h->ntheta;
@@ -1132,14 +1213,17 @@ int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scal
         // the det = 128 kernel writes frames with 16-byte stores
         const bool fast128 = DET == 128 && ((uintptr_t)out % 16) == 0;
         if (fast128 && h->P == DET)
-            k_ptycho_fwd128<true><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
-                                                                  h->nscan, nframes, h->P, scale, h->tw128);
+            k_ptycho_fwd128<true><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase_tab(), h->probe_tab(),
+                                                                  h->nz, h->n, h->nscan, nframes, h->P, scale,
+                                                                  h->tw128, h->shift_ids());
         else if (fast128)
-            k_ptycho_fwd128<false><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz,
-                                                                   h->n, h->nscan, nframes, h->P, scale, h->tw128);
+            k_ptycho_fwd128<false><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase_tab(),
+                                                                   h->probe_tab(), h->nz, h->n, h->nscan, nframes,
+                                                                   h->P, scale, h->tw128, h->shift_ids());
         else
-            k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase, h->prbT, h->nz, h->n,
-                                                              h->nscan, nframes, h->P, scale, h->tw);
+            k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase_tab(), h->probe_tab(),
+                                                              h->nz, h->n, h->nscan, nframes, h->P, scale, h->tw,
+                                                              h->shift_ids());
     }
     PT_LAUNCHED("k_ptycho_fwd");
     return PT_OK;
@@ -1221,9 +1305,131 @@ int probe_adj_dispatch(pt_ptycho *h, float2 *gprb, const float2 *in, const float
 
 void ptycho_free(pt_ptycho *h)
 {
-    void *bufs[] = {h->tw, h->tw128, h->prb, h->prbT, h->phase, h->partial, h->corner, h->prbT2, h->prb_part};
+    void *bufs[] = {h->tw,     h->tw128,  h->prb,  h->prbT, h->phase, h->partial, h->corner,
+                    h->prbT2,  h->prb_part, h->frac, h->prbS, h->ones, h->sid};
     for (void *p : bufs)
         if (p) cudaFree(p);
+}
+
+// D(t) of the sub-pixel model in double: 1 at multiples of P, exactly 0 at
+// the other integers (a zero offset leaves the probe unchanged)
+double dirichlet(double t, int P)
+{
+    if (t == std::floor(t)) return std::fmod(t, (double)P) == 0.0 ? 1.0 : 0.0;
+    const double a = M_PI * t / P;
+    return (P % 2 == 0) ? std::sin(M_PI * t) / (P * std::tan(a)) : std::sin(M_PI * t) / (P * std::sin(a));
+}
+
+void subpixel_free(pt_ptycho *h)
+{
+    void *bufs[] = {h->prbS, h->ones, h->sid};
+    for (void *p : bufs)
+        if (p) cudaFree(p);
+    h->prbS = h->ones = nullptr;
+    h->sid = nullptr;
+    h->quant = h->nshift = 0;
+}
+
+// Builds the shifted probe tables from the handle's offsets (setobj) and
+// probe.  Set-up: allocates, blocks the host.
+int subpixel_build(pt_ptycho *h, int quant, cudaStream_t st)
+{
+    const int nf = h->ntheta * h->nscan, P = h->P;
+    std::vector<float> frac(2 * (size_t)nf);
+    std::vector<int> corner(2 * (size_t)nf);
+    PT_CUDA(cudaMemcpyAsync(frac.data(), h->frac, frac.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaMemcpyAsync(corner.data(), h->corner, corner.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaStreamSynchronize(st));
+    std::map<int, int> ux, uy;                   // quantised offset -> axis table index
+    std::map<std::pair<int, int>, int> up;       // (x index, y index) -> shifted table
+    std::vector<int> sid(nf, 0);
+    std::vector<int2> pairs;
+    auto axis = [](std::map<int, int> &m, int q) {
+        auto it = m.find(q);
+        if (it != m.end()) return it->second;
+        const int k = (int)m.size();
+        m.emplace(q, k);
+        return k;
+    };
+    for (int f = 0; f < nf; ++f) {
+        if (corner[2 * f] < 0 || corner[2 * f + 1] < 0) continue;   // skipped scan
+        const int qx = (int)std::lrint((double)frac[2 * f] * quant), qy = (int)std::lrint((double)frac[2 * f + 1] * quant);
+        const int kx = axis(ux, qx), ky = axis(uy, qy);
+        auto it = up.find({kx, ky});
+        if (it == up.end()) {
+            it = up.emplace(std::make_pair(kx, ky), (int)pairs.size()).first;
+            pairs.push_back(make_int2(kx, ky));
+        }
+        sid[f] = it->second;
+    }
+    if (pairs.empty()) pairs.push_back(make_int2(axis(ux, 0), axis(uy, 0)));   // every scan skipped
+    const size_t tab = (size_t)P * P * sizeof(float2);
+    if (pairs.size() * tab > ((size_t)1 << 31)) {
+        pt::set_error("ptychofft.set_subpixel: %zu distinct offsets need %zu MB of probe tables (limit 2048); "
+                      "use a coarser quantisation",
+                      pairs.size(), pairs.size() * tab >> 20);
+        return PT_ERR_ARG;
+    }
+    // axis matrices: MxT[k][j][x] = D(x - dx_k - j), My[k][y][i] = D(y - dy_k - i)
+    std::vector<float> mx(ux.size() * P * P), my(uy.size() * P * P);
+    for (const auto &kv : ux)
+        for (int j = 0; j < P; ++j)
+            for (int x = 0; x < P; ++x)
+                mx[((size_t)kv.second * P + j) * P + x] = (float)dirichlet(x - (double)kv.first / quant - j, P);
+    for (const auto &kv : uy)
+        for (int y = 0; y < P; ++y)
+            for (int i = 0; i < P; ++i)
+                my[((size_t)kv.second * P + y) * P + i] = (float)dirichlet(y - (double)kv.first / quant - i, P);
+    float *dmx = nullptr, *dmy = nullptr;
+    int2 *dpairs = nullptr;
+    float2 *tmp = nullptr, *prbS = nullptr, *ones = nullptr;
+    int *dsid = nullptr;
+    const size_t np = pairs.size();
+    bool ok = cudaMalloc((void **)&dmx, mx.size() * sizeof(float)) == cudaSuccess &&
+              cudaMalloc((void **)&dmy, my.size() * sizeof(float)) == cudaSuccess &&
+              cudaMalloc((void **)&dpairs, np * sizeof(int2)) == cudaSuccess &&
+              cudaMalloc((void **)&tmp, np * tab) == cudaSuccess && cudaMalloc((void **)&prbS, np * tab) == cudaSuccess &&
+              cudaMalloc((void **)&ones, (size_t)nf * sizeof(float2)) == cudaSuccess &&
+              cudaMalloc((void **)&dsid, (size_t)nf * sizeof(int)) == cudaSuccess;
+    int rc = PT_OK;
+    if (!ok) {
+        cudaGetLastError();
+        pt::set_error("ptychofft.set_subpixel: device allocation failed");
+        rc = PT_ERR_ALLOC;
+    }
+    if (rc == PT_OK &&
+        (cudaMemcpyAsync(dmx, mx.data(), mx.size() * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+         cudaMemcpyAsync(dmy, my.data(), my.size() * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+         cudaMemcpyAsync(dpairs, pairs.data(), np * sizeof(int2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+         cudaMemcpyAsync(dsid, sid.data(), (size_t)nf * sizeof(int), cudaMemcpyHostToDevice, st) != cudaSuccess)) {
+        pt::set_error("ptychofft.set_subpixel: table upload failed");
+        rc = PT_ERR_CUDA;
+    }
+    if (rc == PT_OK) {
+        const size_t tot = np * P * P;
+        const unsigned blocks = (unsigned)((tot + 255) / 256);
+        k_probe_shift_x<<<blocks, 256, 0, st>>>(h->prbT, dmx, dpairs, tmp, P, (int)np);
+        k_probe_shift_y<<<blocks, 256, 0, st>>>(tmp, dmy, dpairs, prbS, P, (int)np);
+        k_fill_one<<<(unsigned)((nf + 255) / 256), 256, 0, st>>>(ones, (size_t)nf);
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+            pt::set_error("ptychofft.set_subpixel: table kernels failed");
+            rc = PT_ERR_CUDA;
+        }
+    }
+    for (void *q : {(void *)dmx, (void *)dmy, (void *)dpairs, (void *)tmp})
+        if (q) cudaFree(q);
+    if (rc != PT_OK) {
+        for (void *q : {(void *)prbS, (void *)ones, (void *)dsid})
+            if (q) cudaFree(q);
+        return rc;
+    }
+    subpixel_free(h);
+    h->prbS = prbS;
+    h->ones = ones;
+    h->sid = dsid;
+    h->quant = quant;
+    h->nshift = (int)np;
+    return PT_OK;
 }
 
 }  // namespace
@@ -1286,6 +1492,7 @@ extern "C" int pt_ptycho_create(size_t ntheta, size_t nz, size_t n, size_t nthet
                                     cudaSuccess) &&
               cudaMalloc((void **)&h->phase, ntheta * nscan * sizeof(float2)) == cudaSuccess &&
               cudaMalloc((void **)&h->corner, 2 * ntheta * nscan * sizeof(int)) == cudaSuccess &&
+              cudaMalloc((void **)&h->frac, 2 * ntheta * nscan * sizeof(float)) == cudaSuccess &&
               cudaMalloc((void **)&h->prbT2, nprb * nprb * sizeof(float2)) == cudaSuccess;
     // probe adjoint: one block per SM (two below 64x64 detectors), one partial each
     h->prb_blocks = (int)std::min<size_t>((size_t)nsm * (detx >= 64 ? 1 : 2), ntheta * nscan);
@@ -1346,7 +1553,7 @@ extern "C" int pt_ptycho_setobj(pt_ptycho *h, const float *scan, const void *prb
     const int nf = h->ntheta * h->nscan;
     h->ready = false;
     PT_CUDA(cudaMemcpyAsync(h->prb, prb, (size_t)h->P * h->P * sizeof(float2), cudaMemcpyDefault, st));
-    k_ptycho_tables<<<(nf + 255) / 256, 256, 0, st>>>(scan, h->corner, h->phase, nf);
+    k_ptycho_tables<<<(nf + 255) / 256, 256, 0, st>>>(scan, h->corner, h->phase, h->frac, nf);
     PT_LAUNCHED("k_ptycho_tables");
     k_probe_t<<<(h->P * h->P + 255) / 256, 256, 0, st>>>(h->prb, h->prbT, h->P, h->c);
     PT_LAUNCHED("k_probe_t");
@@ -1364,6 +1571,7 @@ extern "C" int pt_ptycho_setobj(pt_ptycho *h, const float *scan, const void *prb
         }
     }
     h->ready = true;
+    if (h->quant) return subpixel_build(h, h->quant, st);   // new offsets or probe: new shifted tables
     return PT_OK;
 }
 
@@ -1532,6 +1740,10 @@ int probe_checks(pt_ptycho *h, const char *what)
     int dev = -1;
     PT_CUDA(cudaGetDevice(&dev));
     PT_CHECK_ARG(dev == h->device, "ptychofft handle belongs to device %d, current device is %d", h->device, dev);
+    if (h->quant) {
+        pt::set_error("ptychofft.%s: probe retrieval is not available with the sub-pixel scan model", what);
+        return PT_ERR_STATE;
+    }
     return PT_OK;
 }
 }  // namespace
@@ -1575,4 +1787,36 @@ extern "C" int pt_ptycho_fwd_probe(pt_ptycho *h, void *g, const void *psi, const
     const int rc2 = ptycho_dispatch(h, false, (float2 *)g, (const float2 *)psi, scale, st);
     h->prbT = own;
     return rc2;
+}
+
+extern "C" int pt_ptycho_set_subpixel(pt_ptycho *h, int quant, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h != nullptr, "ptychofft.set_subpixel: null handle");
+    PT_CHECK_ARG(quant >= 0 && quant <= 65536, "ptychofft.set_subpixel: quant must be in [0, 65536] (0: off)");
+    if (quant == 0) {
+        subpixel_free(h);
+        return PT_OK;
+    }
+    if (h->det < 16) {
+        pt::set_error("ptychofft.set_subpixel: not compiled for detector %d (16 to 128)", h->det);
+        return PT_ERR_UNSUPPORTED;
+    }
+    if (!h->ready) {
+        pt::set_error("ptychofft.set_subpixel: setobj(scan, prb) has not been called");
+        return PT_ERR_STATE;
+    }
+    int dev = -1;
+    PT_CUDA(cudaGetDevice(&dev));
+    PT_CHECK_ARG(dev == h->device, "ptychofft handle belongs to device %d, current device is %d", h->device, dev);
+    return subpixel_build(h, quant, (cudaStream_t)stream);
+}
+
+extern "C" int pt_ptycho_get_subpixel(const pt_ptycho *h, int *quant, int *ntables)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h && quant && ntables, "ptychofft.get_subpixel: null pointer");
+    *quant = h->quant;
+    *ntables = h->nshift;
+    return PT_OK;
 }

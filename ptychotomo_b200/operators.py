@@ -135,6 +135,22 @@ class ptychofft:  # noqa: N801 - reference class name
     def parts(self, value):
         check(lib().pt_ptycho_set_parts(self._h, int(value)), "ptychofft.parts")
 
+    # ---- sub-pixel scan model (no counterpart in the reference) -------------
+    def set_subpixel(self, quant, stream=None):
+        """quant > 0: frames F(P(r - d) psi(c + r)), c = round(scan), d the
+        offset quantised to 1/quant pixel, P(r - d) the band-limited
+        interpolation of the probe, no per-scan phase; 0: the reference's
+        rounded positions with its constant phase.  Call after setobj (later
+        setobj calls rebuild the shifted probes)."""
+        check(lib().pt_ptycho_set_subpixel(self._h, int(quant), _s(stream)), "ptychofft.set_subpixel")
+
+    @property
+    def subpixel(self):
+        """(quant, number of shifted probe tables); quant 0: off."""
+        q, k = ctypes.c_int(), ctypes.c_int()
+        check(lib().pt_ptycho_get_subpixel(self._h, ctypes.byref(q), ctypes.byref(k)), "ptychofft.subpixel")
+        return q.value, k.value
+
     def adj_resid(self, f, fpsi, data, dscale, model, scale=1.0, stream=None):
         """Gradient of the data term: f = scale * Q* F* residual(fpsi, dscale * data)."""
         check(lib().pt_ptycho_adj_resid(self._h, as_ptr(f), as_ptr(fpsi), as_ptr(data), float(dscale), int(model),

@@ -67,7 +67,7 @@ def _dev_tensor(x, dtype, device):
 
 class Solver:
     def __init__(self, prb, scan, theta, det, voxelsize, energy, ntheta, nz, n, ptheta, pnz, device=None,
-                 _held=None):
+                 subpixel=0, _held=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         dev = self.device
         self.voxelsize = voxelsize
@@ -109,6 +109,12 @@ class Solver:
             self._ptycho_all.setobj(self.scan, self.prb)
         else:
             self._ptycho_all = self.cl_ptycho
+        # sub-pixel scan model (not in the reference): subpixel = quantisation
+        # of the scan offsets in 1/pixel; 0 keeps the reference's rounded scans
+        self.subpixel = int(subpixel)
+        if self.subpixel:
+            for op in {id(o): o for o in self._ptycho + [self._ptycho_all]}.values():
+                op.set_subpixel(self.subpixel)
         # normalization coefficients, solver.py:43-46 (float32 like the reference)
         self._red_local = K.Reducer(dev)   # for quantities every process holds whole (the probe)
         self.red = self._reducer(K.Reducer(dev))
