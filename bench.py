@@ -81,11 +81,12 @@ def config_dict(c, extra=None):
 # from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one
 # launch, --clock-control none) of
 #   python bench.py --ntheta 148 [--no-autotune --ptycho-parts P] --steps 1 --warmup 1 --no-e2e --no-cpu-baseline
-# parts 1: 3,691,507,712 + 500,559,104 bytes for 148 x 169 = 25,012 frames.
+# parts 1: 3,691,507,712 + 500,559,104 bytes for 148 x 169 = 25,012 frames;
+# parts 3: 3,956,107,008 + 983,063,552 bytes for the same frames.
 # 148 angles are one wave of one-slab angle blocks (parts x 148 blocks for a
 # split), the per-wave layout of the 384-angle workload, so the figure is
 # scaled by the frame count of the run.
-PTYCHO_ADJ128_DRAM_PER_FRAME = {1: (3691507712 + 500559104) / 25012}
+PTYCHO_ADJ128_DRAM_PER_FRAME = {1: (3691507712 + 500559104) / 25012, 3: (3956107008 + 983063552) / 25012}
 
 
 def traffic_source(parts):

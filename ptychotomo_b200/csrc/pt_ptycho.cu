@@ -22,6 +22,7 @@
 #include <cstdlib>
 #include <cstdint>
 #include <map>
+#include <type_traits>
 #include <vector>
 
 #include "pt_common.cuh"
@@ -204,7 +205,7 @@ __device__ __forceinline__ void line_dft(float2 (&v)[PF<DET>::N1], int t, float2
     }
 }
 
-template <int DET>
+template <int DET, bool SUB = false>
 __global__ void __launch_bounds__(PF<DET>::NT, 1)
     k_ptycho_fwd(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
                  const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
@@ -228,7 +229,7 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
             continue;
         }
         const float2 *src = psi + ((size_t)th * nz + sty) * n + stx;
-        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
+        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
         float2 v[F::CPG][F::N1];
         // along the object row: line = detector column iy, points ix = t + N2 m
 #pragma unroll
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
 }
 
 // grid (parts, ntheta): block (part, angle) owns slab dst[angle][part]
-template <int DET, int RESID>
+template <int DET, int RESID, bool SUB = false>
 __global__ void __launch_bounds__(PF<DET>::NT, 1)
     k_ptycho_adj(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                  const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
         const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
         if (stx < 0 || sty < 0) continue;
         const float2 ph = phase[fid];
-        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;
+        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;
         const float2 *in = g + (size_t)fid * DET * DET;
         float2 v[F::CPG][F::N1];
         // along the detector row: line = kx, points ky = t + N2 m (contiguous)
@@ -450,7 +451,7 @@ __device__ __forceinline__ void fold_twiddles(float4 *twf, const float4 *__restr
     }
 }
 
-template <bool FULL>
+template <bool FULL, bool SUB = false>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_fwd128(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
@@ -476,7 +477,7 @@ __global__ void __launch_bounds__(512, 1)
             continue;
         }
         const float2 *src = psi + ((size_t)th * nz + sty) * n + stx;
-        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
+        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
         float2 v[2][16];
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -603,7 +604,7 @@ __device__ __forceinline__ void rmw_row16(float2 *row, const float2 *__restrict_
 // grid (parts, ntheta): block (part, angle) owns slab dst[angle][part].
 // While the current frame finishes, the next frame's rows 0..63 are already
 // on their way into the idle half of the shared frame buffer.
-template <bool FULL, int RESID>
+template <bool FULL, int RESID, bool SUB = false>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
@@ -669,7 +670,7 @@ __global__ void __launch_bounds__(512, 1)
             continue;
         }
         const float2 ph = FOLD ? make_float2(1.f, 0.f) : phase[fid];
-        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
+        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
         float2 v[2][16];
         // rows 64..127 from global first, so their latency hides behind row 0..63's work
 #pragma unroll
@@ -760,7 +761,7 @@ __global__ void __launch_bounds__(512, 1)
 // measured faster for the Gaussian residual (11.0 ms for k_ptycho_adj128's)
 // and the probe adjoint (12.3 ms for k_ptycho_adj_probe) and slower for the
 // plain and Poisson object adjoints, so each launch takes the faster one.
-template <bool FULL, int RESID, bool PROBE>
+template <bool FULL, int RESID, bool PROBE, bool SUB = false>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128v(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
@@ -821,7 +822,7 @@ __global__ void __launch_bounds__(512, 1)
             continue;
         }
         const float2 ph = FOLD ? make_float2(1.f, 0.f) : phase[fid];
-        const float2 *pr = sid ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
+        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
         float2 v[2][16];
         // rows 64..127 from global first, so their latency hides behind row 0..63's work
 #pragma unroll
@@ -1129,6 +1130,20 @@ int ptycho_attrs()
         PT_ATTR((k_ptycho_adj_probe<DET, 0>), s);
         PT_ATTR((k_ptycho_adj_probe<DET, 1>), s);
         PT_ATTR((k_ptycho_adj_probe<DET, 2>), s);
+        PT_ATTR((k_ptycho_fwd<DET, true>), s);
+        PT_ATTR((k_ptycho_adj<DET, 0, true>), s);
+        PT_ATTR((k_ptycho_adj<DET, 1, true>), s);
+        PT_ATTR((k_ptycho_adj<DET, 2, true>), s);
+        if constexpr (DET == 128) {
+            PT_ATTR((k_ptycho_fwd128<true, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_fwd128<false, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 0, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<false, 0, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 1, true>), P128_SMEM_RESID);
+            PT_ATTR((k_ptycho_adj128<false, 1, true>), P128_SMEM_RESID);
+            PT_ATTR((k_ptycho_adj128<false, 2, true>), P128_SMEM_RESID);
+            PT_ATTR((k_ptycho_adj128v<true, 2, false, true>), P128_SMEM_RESID);
+        }
         if constexpr (DET == 128) {
             PT_ATTR(k_ptycho_fwd128<true>, P128_SMEM);
             PT_ATTR(k_ptycho_fwd128<false>, P128_SMEM);
@@ -1165,24 +1180,33 @@ int ptycho_adj_launch(pt_ptycho *h, float2 *out, const float2 *in, float scale, 
         // the det = 128 adjoint prefetches frames (and counts) with 16-byte async copies
         const bool fast128 = DET == 128 && ((uintptr_t)in % 16) == 0 && (RESID == 0 || (uintptr_t)data % 16 == 0);
         const int smem = RESID ? P128_SMEM_RESID : P128_SMEM;
-        if (fast128 && h->P == DET) {
-            if constexpr (RESID == 2)
-                k_ptycho_adj128v<true, RESID, false><<<grid, 512, smem, st>>>(
+        // SUB: the sub-pixel model's per-frame probe tables (a separate
+        // instantiation, so the reference model's kernels are unchanged)
+        auto go = [&](auto sub) {
+            constexpr bool S = decltype(sub)::value;
+            if (fast128 && h->P == DET) {
+                if constexpr (RESID == 2)
+                    k_ptycho_adj128v<true, RESID, false, S><<<grid, 512, smem, st>>>(
+                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
+                        h->tw128, data, dscale, nullptr, 0, h->shift_ids());
+                else
+                    k_ptycho_adj128<true, RESID, S><<<grid, 512, smem, st>>>(
+                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
+                        h->tw128, data, dscale, h->shift_ids());
+            }
+            else if (fast128)
+                k_ptycho_adj128<false, RESID, S><<<grid, 512, smem, st>>>(
                     in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale, h->tw128,
-                    data, dscale, nullptr, 0, h->shift_ids());
+                    data, dscale, h->shift_ids());
             else
-                k_ptycho_adj128<true, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase_tab(),
-                                                                     h->probe_tab(), h->nz, h->n, h->nscan, h->P,
-                                                                     scale, h->tw128, data, dscale, h->shift_ids());
-        }
-        else if (fast128)
-            k_ptycho_adj128<false, RESID><<<grid, 512, smem, st>>>(in, dst, h->corner, h->phase_tab(), h->probe_tab(),
-                                                                  h->nz, h->n, h->nscan, h->P, scale, h->tw128, data,
-                                                                  dscale, h->shift_ids());
+                k_ptycho_adj<DET, RESID, S><<<grid, F::NT, F::SMEM, st>>>(
+                    in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale, h->tw,
+                    data, dscale, h->shift_ids());
+        };
+        if (h->quant)
+            go(std::true_type{});
         else
-            k_ptycho_adj<DET, RESID><<<grid, F::NT, F::SMEM, st>>>(in, dst, h->corner, h->phase_tab(), h->probe_tab(),
-                                                                  h->nz, h->n, h->nscan, h->P, scale, h->tw, data,
-                                                                  dscale, h->shift_ids());
+            go(std::false_type{});
         PT_LAUNCHED("k_ptycho_adj");
         if (h->parts > 1) {
             const size_t slab = (size_t)h->nz * h->n, total = slab * h->ntheta;
@@ -1212,18 +1236,27 @@ int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scal
         using F = PF<DET>;
         // the det = 128 kernel writes frames with 16-byte stores
         const bool fast128 = DET == 128 && ((uintptr_t)out % 16) == 0;
-        if (fast128 && h->P == DET)
-            k_ptycho_fwd128<true><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase_tab(), h->probe_tab(),
-                                                                  h->nz, h->n, h->nscan, nframes, h->P, scale,
-                                                                  h->tw128, h->shift_ids());
-        else if (fast128)
-            k_ptycho_fwd128<false><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase_tab(),
-                                                                   h->probe_tab(), h->nz, h->n, h->nscan, nframes,
-                                                                   h->P, scale, h->tw128, h->shift_ids());
+        auto go = [&](auto sub) {
+            constexpr bool S = decltype(sub)::value;
+            if (fast128 && h->P == DET)
+                k_ptycho_fwd128<true, S><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase_tab(),
+                                                                         h->probe_tab(), h->nz, h->n, h->nscan,
+                                                                         nframes, h->P, scale, h->tw128,
+                                                                         h->shift_ids());
+            else if (fast128)
+                k_ptycho_fwd128<false, S><<<nframes, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase_tab(),
+                                                                          h->probe_tab(), h->nz, h->n, h->nscan,
+                                                                          nframes, h->P, scale, h->tw128,
+                                                                          h->shift_ids());
+            else
+                k_ptycho_fwd<DET, S><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase_tab(),
+                                                                     h->probe_tab(), h->nz, h->n, h->nscan, nframes,
+                                                                     h->P, scale, h->tw, h->shift_ids());
+        };
+        if (h->quant)
+            go(std::true_type{});
         else
-            k_ptycho_fwd<DET><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase_tab(), h->probe_tab(),
-                                                              h->nz, h->n, h->nscan, nframes, h->P, scale, h->tw,
-                                                              h->shift_ids());
+            go(std::false_type{});
     }
     PT_LAUNCHED("k_ptycho_fwd");
     return PT_OK;

@@ -165,7 +165,7 @@ def test_boundary_crossing_is_continuous():
 
 def test_solver_option():
     from ptychotomo_b200 import Solver, synthetic
-    nt, n, P = 4, 48, 16
+    nt, n, P = 4, 64, 16
     theta = synthetic.angles(nt)
     scan = synthetic.raster_scan(nt, 3, n, n, P) + np.float32(0.3)
     slv = Solver(synthetic.probe(P, seed=1), scan, theta, [P, P], 1e-6, 5.0, nt, n, n, nt, n, subpixel=32)
