@@ -23,6 +23,7 @@ Pass-model algorithmic bytes per call (complex64 = 8 B):
     python bench.py --uneven      # uneven scans: one launch for all angles vs one per angle
     python bench.py --precond     # learned preconditioner of the tomography CG (360 angles, missing wedge)
     python bench.py --time-to-target   # time to the plain ADMM's reconstruction: plain vs graph-captured variants
+    python bench.py --pcie        # pinned host<->device copy rates (the bound of the e2e leg)
 
 ``--impl reference`` times the reference's operators: by default the CPU
 restatement of the reference (oracle/, all host cores, a bounded sample of
@@ -55,6 +56,9 @@ def usfft_bytes(n, nz, ntheta):
 
 def ptycho_bytes(S, nprb, det):
     return 8 * S * (nprb * nprb + det * det)
+
+
+GATHER_NAMES = {0: "L1", 1: "smem tiles", 2: "TMA smem tiles"}
 
 
 def workload_bytes(c):
@@ -204,9 +208,9 @@ class Ops:
         """The operators' autotuners (set-up, untimed): the radon forward's
         streams and gather variant, the ptycho adjoint's angle split."""
         self.ptycho.fwd(self.frames, self.psi)
-        streams, tiled = self.radon.autotune(self.proj_out, self.u, trials=3)
+        streams, gather = self.radon.autotune(self.proj_out, self.u, trials=3)
         parts = self.ptycho.autotune(self.psi_out, self.frames, trials=3)
-        self.tuned = {"radon_fwd_streams": streams, "radon_gather": "smem tiles" if tiled else "L1",
+        self.tuned = {"radon_fwd_streams": streams, "radon_gather": GATHER_NAMES[gather],
                       "ptycho_adj_parts": parts}
         return self.tuned
 
@@ -299,9 +303,9 @@ def run_ours(args, rank, world, local):
         ops.ptycho.parts = args.ptycho_parts
         ops.tuned = dict(ops.tuned or {}, ptycho_adj_parts=args.ptycho_parts, parts_source="--ptycho-parts")
     if args.radon_variant:
-        streams, tiled = (int(v) for v in args.radon_variant.split(","))
-        ops.radon.set_variant(streams, bool(tiled))
-        ops.tuned = dict(ops.tuned or {}, radon_fwd_streams=streams, radon_gather="smem tiles" if tiled else "L1",
+        streams, gather = (int(v) for v in args.radon_variant.split(","))
+        ops.radon.set_variant(streams, gather)
+        ops.tuned = dict(ops.tuned or {}, radon_fwd_streams=streams, radon_gather=GATHER_NAMES[gather],
                          radon_source="--radon-variant")
     bytes_op = workload_bytes(c)
     step_bytes = sum(bytes_op.values())
@@ -1269,6 +1273,44 @@ def run_time_to_target(args, local):
             "speedup_to_plain_quality": q_ratios}
 
 
+def run_pcie(args, local):
+    """Host<->device copy rates with pinned buffers (the e2e leg's bound):
+    8 GiB each way alone, then both directions at once on two streams."""
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n = 8 * 1024 ** 3 // 8
+    h1 = torch.empty(n, dtype=torch.complex64, pin_memory=True)
+    h2 = torch.empty(n, dtype=torch.complex64, pin_memory=True)
+    d1 = torch.empty(n, dtype=torch.complex64, device=dev)
+    d2 = torch.empty(n, dtype=torch.complex64, device=dev)
+    s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    def both():
+        with torch.cuda.stream(s1):
+            d1.copy_(h1, non_blocking=True)
+        with torch.cuda.stream(s2):
+            h2.copy_(d2, non_blocking=True)
+
+    B = n * 8
+    for _ in range(2):   # the second round is reported
+        th = timed(lambda: d1.copy_(h1, non_blocking=True))
+        td = timed(lambda: h2.copy_(d2, non_blocking=True))
+        tb = timed(both)
+    link = subprocess.run(["nvidia-smi", "-i", str(local), "--query-gpu=pcie.link.gen.current,pcie.link.width.current",
+                           "--format=csv,noheader"], capture_output=True, text=True).stdout.strip()
+    return {"metric": "pinned host<->device copy rate", "unit": "GB/s", "n_gpus": 1, "bytes_each_way": B,
+            "h2d": round(B / th / 1e9, 1), "d2h": round(B / td / 1e9, 1), "concurrent_each_way": round(B / tb / 1e9, 1),
+            "pcie_link": link}
+
+
 def _precond_harvest_solver(slv, dev):
     """A Solver with the same angles and width on 8 slices (training targets)."""
     from ptychotomo_b200 import Solver, synthetic
@@ -1289,7 +1331,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the operators' default variants")
     ap.add_argument("--ptycho-parts", type=int, default=None, help="fix the ptycho adjoint's angle split")
-    ap.add_argument("--radon-variant", default=None, help="fix the radon forward: STREAMS,TILED (e.g. 2,1)")
+    ap.add_argument("--radon-variant", default=None,
+                    help="fix the radon forward: STREAMS,GATHER (gather 0 L1, 1 smem tiles, 2 TMA tiles; e.g. 2,1)")
     ap.add_argument("--ntheta", type=int, default=None, help="override the angle count (small profiling cases)")
     ap.add_argument("--nz", type=int, default=None, help="override the slice count (small profiling cases)")
     ap.add_argument("--admm", action="store_true", help="ADMM wall time instead of operator throughput")
@@ -1298,6 +1341,7 @@ def main():
     ap.add_argument("--uneven", action="store_true", help="uneven scans: batched vs per-angle launches")
     ap.add_argument("--precond", action="store_true", help="learned preconditioner of the tomography CG")
     ap.add_argument("--time-to-target", action="store_true", help="time to the plain ADMM's reconstruction")
+    ap.add_argument("--pcie", action="store_true", help="pinned host<->device copy rates (the e2e bound)")
     ap.add_argument("--ttt-iters", type=int, default=None)
     ap.add_argument("--ttt-size", type=int, default=None)
     ap.add_argument("--ttt-alpha", type=float, default=None)
@@ -1316,11 +1360,12 @@ def main():
         if rank == 0:
             print(json.dumps(line), flush=True)
         return 0
-    if args.admm or args.cg_kernels or args.precision or args.uneven or args.precond or args.time_to_target:
+    if (args.admm or args.cg_kernels or args.precision or args.uneven or args.precond or args.time_to_target
+            or args.pcie):
         if rank == 0:
             fn = (run_admm if args.admm else run_cg_kernels if args.cg_kernels else
                   run_precision if args.precision else run_precond if args.precond else
-                  run_time_to_target if args.time_to_target else run_uneven)
+                  run_time_to_target if args.time_to_target else run_pcie if args.pcie else run_uneven)
             print(json.dumps(fn(args, local)), flush=True)
         return 0
     if args.impl == "reference":

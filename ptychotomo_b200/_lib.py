@@ -71,6 +71,7 @@ SIGNATURES = {
     "pt_ptycho_get_subpixel": (_int, [_vp, ctypes.POINTER(_int), ctypes.POINTER(_int)]),
     "pt_radon_autotune": (_int, [_vp, _vp, _vp, _int, ctypes.POINTER(_int), _vp]),
     "pt_radon_set_variant": (_int, [_vp, _int, _int]),
+    "pt_radon_status": (_int, [_vp, ctypes.POINTER(_int), ctypes.POINTER(_int)]),
     "pt_reduce_workspace_bytes": (_sz, []),
     "pt_reduce_c64": (_int, [_int, _vp, _vp, _sz, _int, _int, _int, _vp, _vp, _vp]),
     "pt_ls_frames": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp, _int, _vp, _vp, _vp]),

@@ -36,6 +36,9 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "pt_common.cuh"
 #include "pt_fft.cuh"
 
@@ -257,25 +260,15 @@ constexpr int tile_pairs() { return (GTILE - 2) / 2 + (2 * M + 3) / 2; }
 template <int M>
 constexpr size_t tile_smem() { return (size_t)tile_rows<M>() * tile_pairs<M>() * ZC * sizeof(float4); }
 
+// The gather of one chunk's points from its staged tile (both tiled kernels).
 template <int N, int M>
-__global__ void __launch_bounds__(GPB *ZC, 3)
-    k_fwd_gather_tile(const float2 *__restrict__ fg, float2 *__restrict__ lines, const float *__restrict__ xt,
-                      const float *__restrict__ yt, float a, float pre, const int *__restrict__ perm,
-                      const int4 *__restrict__ chunks)
+__device__ __forceinline__ void tile_gather(const float4 *__restrict__ tsm, int4 ch, int ty0, int px0,
+                                            float2 *__restrict__ lines, const float *__restrict__ xt,
+                                            const float *__restrict__ yt, float a, float pre,
+                                            const int *__restrict__ perm)
 {
     constexpr int G = 2 * N, W = 2 * M + 1, NP = (W + 2) / 2;
-    constexpr int PS = G / 2 + GH_PAIRS, NROWS = G + GH_ROWS;   // the haloed grid's pair pitch and rows
-    constexpr int TR = tile_rows<M>(), TP = tile_pairs<M>();
-    extern __shared__ float4 tsm[];
-    const int4 ch = chunks[blockIdx.x];   // (tile row, tile column, first, count)
-    const int ty0 = ch.x * GTILE, px0 = ch.y * GTILE / 2;
-    const int rows = min(TR, NROWS - ty0), pairs = min(TP, PS - px0);
-    const float4 *g4 = reinterpret_cast<const float4 *>(fg);
-    for (int e = threadIdx.x; e < rows * pairs * ZC; e += blockDim.x) {
-        const int r = e / (pairs * ZC), rem = e % (pairs * ZC), pj = rem / ZC, q = rem % ZC;
-        tsm[(r * TP + pj) * ZC + q] = __ldg(&g4[((size_t)(ty0 + r) * PS + px0 + pj) * ZC + q]);
-    }
-    __syncthreads();
+    constexpr int TP = tile_pairs<M>();
     const int lane = threadIdx.x % ZC;
     for (int t = threadIdx.x / ZC; t < ch.w; t += GPB) {
         const int p = __ldg(&perm[ch.z + t]);
@@ -324,6 +317,87 @@ __global__ void __launch_bounds__(GPB *ZC, 3)
         }
         lines[((size_t)th * N + k) * ZC + lane] = ((k & 1) ? pre : -pre) * acc;
     }
+}
+
+template <int N, int M>
+__global__ void __launch_bounds__(GPB *ZC, 3)
+    k_fwd_gather_tile(const float2 *__restrict__ fg, float2 *__restrict__ lines, const float *__restrict__ xt,
+                      const float *__restrict__ yt, float a, float pre, const int *__restrict__ perm,
+                      const int4 *__restrict__ chunks)
+{
+    constexpr int G = 2 * N;
+    constexpr int PS = G / 2 + GH_PAIRS, NROWS = G + GH_ROWS;   // the haloed grid's pair pitch and rows
+    constexpr int TR = tile_rows<M>(), TP = tile_pairs<M>();
+    extern __shared__ float4 tsm[];
+    const int4 ch = chunks[blockIdx.x];   // (tile row, tile column, first, count)
+    const int ty0 = ch.x * GTILE, px0 = ch.y * GTILE / 2;
+    const int rows = min(TR, NROWS - ty0), pairs = min(TP, PS - px0);
+    const float4 *g4 = reinterpret_cast<const float4 *>(fg);
+    for (int e = threadIdx.x; e < rows * pairs * ZC; e += blockDim.x) {
+        const int r = e / (pairs * ZC), rem = e % (pairs * ZC), pj = rem / ZC, q = rem % ZC;
+        tsm[(r * TP + pj) * ZC + q] = __ldg(&g4[((size_t)(ty0 + r) * PS + px0 + pj) * ZC + q]);
+    }
+    __syncthreads();
+    tile_gather<N, M>(tsm, ch, ty0, px0, lines, xt, yt, a, pre, perm);
+}
+
+// The same with the tile staged by the Tensor Memory Accelerator: one
+// cp.async.bulk.tensor 3-D box load (32 floats = one column pair of ZC
+// slices, TP pairs, TR rows) of the haloed grid into shared memory, completed
+// on an mbarrier.  The box lands in exactly the layout of k_fwd_gather_tile's
+// copy (and is zero-filled past the grid's end, where no window reads), so
+// the results are bit-identical.  The wait is bounded: after TMA_SPIN polls
+// the block records the failure in *err and returns without writing.  The
+// mbarrier sits after the tile in dynamic shared memory (no static shared
+// memory, so the tile starts at the 128-byte aligned base; checked, and a
+// misaligned base is recorded in *err instead of issuing the copy).
+constexpr int TMA_SPIN = 1 << 24;
+template <int M>
+constexpr size_t tma_smem() { return tile_smem<M>() + 16; }
+template <int N, int M>
+__global__ void __launch_bounds__(GPB *ZC, 3)
+    k_fwd_gather_tma(const __grid_constant__ CUtensorMap tmap, float2 *__restrict__ lines,
+                     const float *__restrict__ xt, const float *__restrict__ yt, float a, float pre,
+                     const int *__restrict__ perm, const int4 *__restrict__ chunks, int *__restrict__ err)
+{
+    constexpr unsigned BYTES = (unsigned)tile_smem<M>();
+    static_assert(BYTES % 128 == 0, "the mbarrier follows the tile");
+    extern __shared__ __align__(128) float4 tsm_tma[];
+    float4 *tsm = tsm_tma;
+    const int4 ch = chunks[blockIdx.x];
+    const int ty0 = ch.x * GTILE, px0 = ch.y * GTILE / 2;   // >= 0; the column coordinate is 0
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(tsm);
+    const unsigned bar_a = dst + BYTES;
+    if (dst & 127) {
+        if (threadIdx.x == 0) atomicExch(err, 2);
+        return;
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(BYTES) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+            "%4}], [%5];" ::"r"(dst),
+            "l"(reinterpret_cast<unsigned long long>(&tmap)), "r"(0), "r"(px0), "r"(ty0), "r"(bar_a)
+            : "memory");
+    }
+    unsigned done = 0;
+    for (int it = 0; it < TMA_SPIN && !done; ++it)
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(bar_a), "r"(0)
+            : "memory");
+    if (!done) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;
+    }
+    tile_gather<N, M>(tsm, ch, ty0, px0, lines, xt, yt, a, pre, perm);
 }
 
 // ---- K3b: fftshift1c / 1-D inverse FFT / fftshift1c + crop + scale --------
@@ -625,7 +699,12 @@ struct pt_radon {
     int *perm = nullptr;   // the forward gather's point order (grid tiles)
     int4 *chunks = nullptr;   // the tiled gather's blocks: (tile row, tile column, first, count)
     int nchunks = 0, chunks_cap = 0;
-    int gather = 0;           // 0: gather through L1 (k_fwd_gather_pts), 1: shared-memory tiles
+    int gather = 0;           // 0: gather through L1 (k_fwd_gather_pts), 1: shared-memory tiles, 2: TMA-staged tiles
+    // gather 2: one 3-D tensor map per grid buffer (fgrid, fgrid2), and a
+    // device flag the TMA kernel sets if a tile load did not complete
+    CUtensorMap tmap[2];
+    bool tma_ok = false;
+    int *tma_err = nullptr;
     // forward (per chunk of ZC slices)
     float2 *rbuf = nullptr, *fgrid = nullptr;
     // a second chunk buffer set and a side stream: alternate chunks of the
@@ -648,7 +727,7 @@ namespace {
 void radon_free(pt_radon *h)
 {
     void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->perm, h->chunks, h->rbuf, h->fgrid, h->rbuf2,
-                    h->fgrid2,
+                    h->fgrid2, h->tma_err,
                     h->lines, h->rbuf_adj, h->mbuf, h->goff, h->col_order, h->gpt, h->gw, h->deap};
     for (void *p : bufs)
         if (p) cudaFree(p);
@@ -676,6 +755,43 @@ void radon_params(int n, int m_override, int *N, int *M, float *mu)
 
 typedef int (*radon_run_fn)(pt_radon *, float2 *, const float2 *, float, cudaStream_t);
 
+// Tensor maps of the two haloed grid buffers for k_fwd_gather_tma: float32,
+// dims (innermost first) {ZC * 4 floats = one column pair of the chunk's
+// slices, G/2 + GH_PAIRS pairs, G + GH_ROWS rows}, row-major strides
+// {ZC * 16, (G/2 + GH_PAIRS) * ZC * 16} bytes, box {ZC * 4, TP, TR}: the
+// box's inner extent is 128 bytes and its first coordinate is always 0, so
+// every load starts on a 16-byte boundary.  cuTensorMapEncodeTiled comes
+// from the driver through the runtime's entry-point query (no link against
+// libcuda); false if it or any encode fails.
+bool encode_grid_maps(pt_radon *h)
+{
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || fn == nullptr) {
+        cudaGetLastError();
+        return false;
+    }
+    auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    const int G = h->G;
+    const cuuint64_t pairs = (cuuint64_t)(G / 2 + GH_PAIRS), rows = (cuuint64_t)(G + GH_ROWS);
+    const cuuint64_t dims[3] = {(cuuint64_t)ZC * 4, pairs, rows};
+    const cuuint64_t strides[2] = {(cuuint64_t)ZC * 16, pairs * ZC * 16};
+    const cuuint32_t tr = (cuuint32_t)(GTILE + 2 * h->M), tp = (cuuint32_t)((GTILE - 2) / 2 + (2 * h->M + 3) / 2);
+    const cuuint32_t box[3] = {(cuuint32_t)ZC * 4, tp, tr};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    float2 *bufs[2] = {h->fgrid, h->fgrid2};
+    for (int b = 0; b < 2; ++b) {
+        if (((uintptr_t)bufs[b] & 127) != 0) return false;
+        if (encode(&h->tmap[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, bufs[b], dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
+
 template <int G>
 int set_attrs()
 {
@@ -695,6 +811,10 @@ int set_attrs()
                                  (int)tile_smem<7>()));
     PT_CUDA(cudaFuncSetAttribute(k_fwd_gather_tile<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)tile_smem<4>()));
+    PT_CUDA(cudaFuncSetAttribute(k_fwd_gather_tma<N, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tma_smem<7>()));
+    PT_CUDA(cudaFuncSetAttribute(k_fwd_gather_tma<N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tma_smem<4>()));
     PT_CUDA(cudaFuncSetAttribute(k_adj_lines<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     PT_CUDA(cudaFuncSetAttribute(k_adj_lines<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s3));
     return PT_OK;
@@ -728,7 +848,11 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
         k_fwd_cols<G><<<G / CK, CK * ZC * T, s2, s>>>(rb, fg, h->tw_G);
         PT_LAUNCHED("k_fwd_cols");
         const int npts = h->ntheta * N;
-        if (h->gather == 1) {
+        if (h->gather == 2) {
+            k_fwd_gather_tma<N, M><<<h->nchunks, GPB * ZC, tma_smem<M>(), s>>>(
+                h->tmap[odd ? 1 : 0], ln, h->x, h->y, a, pre, h->perm, h->chunks, h->tma_err);
+            PT_LAUNCHED("k_fwd_gather_tma");
+        } else if (h->gather == 1) {
             k_fwd_gather_tile<N, M><<<h->nchunks, GPB * ZC, tile_smem<M>(), s>>>(fg, ln, h->x, h->y, a, pre, h->perm,
                                                                               h->chunks);
             PT_LAUNCHED("k_fwd_gather_tile");
@@ -890,6 +1014,9 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     if (rc == PT_OK) rc = dmalloc(&h->deap, (size_t)N * N);
     if (rc == PT_OK) rc = dmalloc(&h->fgrid, (size_t)(G + GH_ROWS) * (G + 2 * GH_PAIRS) * ZC);
     if (rc == PT_OK) rc = dmalloc(&h->fgrid2, (size_t)(G + GH_ROWS) * (G + 2 * GH_PAIRS) * ZC);
+    if (rc == PT_OK && cudaMalloc((void **)&h->tma_err, sizeof(int)) == cudaSuccess &&
+        cudaMemset(h->tma_err, 0, sizeof(int)) == cudaSuccess)
+        h->tma_ok = encode_grid_maps(h);   // gather 2 is offered only if both maps encode
     if (rc == PT_OK && (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
                         cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
                         cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess)) {
@@ -1130,7 +1257,8 @@ extern "C" int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials
     PT_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     int best_s = h->streams, best_g = h->gather, rc = PT_OK;
-    for (int combo = 0; combo < 4 && rc == PT_OK; ++combo) {
+    const int ncombo = h->tma_ok ? 6 : 4;   // streams {1, 2} x gather {L1, tiles, TMA tiles}
+    for (int combo = 0; combo < ncombo && rc == PT_OK; ++combo) {
         const int sc = 1 + (combo & 1);
         h->streams = sc;
         h->gather = combo >> 1;
@@ -1158,7 +1286,30 @@ extern "C" int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials
     h->streams = best_s;
     h->gather = best_g;
     if (streams_out) *streams_out = best_s + 2 * best_g;
+    if (rc == PT_OK && h->tma_ok) {   // a TMA tile load that never completed
+        int flag = 0;
+        PT_CUDA(cudaMemcpy(&flag, h->tma_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (flag) {
+            h->gather = 1;
+            pt::set_error("radonusfft.autotune: a TMA tile load did not complete; TMA gather disabled");
+            h->tma_ok = false;
+            return PT_ERR_CUDA;
+        }
+    }
     return rc;
+}
+
+extern "C" int pt_radon_status(pt_radon *h, int *tma_timeouts, int *tma_available)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h && tma_timeouts && tma_available, "radonusfft.status: null pointer");
+    *tma_available = h->tma_ok ? 1 : 0;
+    *tma_timeouts = 0;
+    if (h->tma_err) {
+        PT_CUDA(cudaMemcpy(tma_timeouts, h->tma_err, sizeof(int), cudaMemcpyDeviceToHost));
+        PT_CUDA(cudaMemset(h->tma_err, 0, sizeof(int)));
+    }
+    return PT_OK;
 }
 
 int pt::radon_dims(const pt_radon *h, int *nz, int *ntheta)
@@ -1176,8 +1327,12 @@ int pt::radon_dims(const pt_radon *h, int *nz, int *ntheta)
 extern "C" int pt_radon_set_variant(pt_radon *h, int streams, int gather)
 {
     pt::clear_error();
-    PT_CHECK_ARG(h && (streams == 1 || streams == 2) && (gather == 0 || gather == 1),
-                 "radonusfft.set_variant: streams 1 or 2, gather 0 or 1");
+    PT_CHECK_ARG(h && (streams == 1 || streams == 2) && (gather >= 0 && gather <= 2),
+                 "radonusfft.set_variant: streams 1 or 2, gather 0 (L1), 1 (tiles) or 2 (TMA tiles)");
+    if (gather == 2 && !h->tma_ok) {
+        pt::set_error("radonusfft.set_variant: the TMA gather is not available (tensor map encoding failed)");
+        return PT_ERR_UNSUPPORTED;
+    }
     h->streams = streams;
     h->gather = gather;
     return PT_OK;

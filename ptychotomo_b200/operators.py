@@ -57,17 +57,26 @@ class radonusfft:  # noqa: N801 - reference class name
 
     def autotune(self, g, f, trials=3, stream=None):
         """Time the forward on one stream and pipelined on two, each with the
-        gather through L1 and from shared-memory tiles; keep the fastest for
-        this operator.  g, f: buffers of fwd's shapes (g is overwritten).
-        Returns (streams, tiled)."""
+        gather through L1, from shared-memory tiles and from TMA-staged
+        tiles; keep the fastest for this operator.  g, f: buffers of fwd's
+        shapes (g is overwritten).  Returns (streams, gather), gather 0 (L1),
+        1 (tiles) or 2 (TMA tiles)."""
         out = ctypes.c_int()
         check(lib().pt_radon_autotune(self._h, as_ptr(g), as_ptr(f), int(trials), ctypes.byref(out), _s(stream)),
               "radonusfft.autotune")
-        return out.value % 2 if out.value % 2 else 2, out.value // 2
+        return (out.value - 1) % 2 + 1, (out.value - 1) // 2
 
-    def set_variant(self, streams=2, tiled=False):
-        """The forward's variant without timing (results are identical)."""
-        check(lib().pt_radon_set_variant(self._h, int(streams), int(bool(tiled))), "radonusfft.set_variant")
+    def set_variant(self, streams=2, gather=0):
+        """The forward's variant without timing (results are identical):
+        gather 0 (L1), 1 or True (shared-memory tiles), 2 (TMA-staged tiles)."""
+        check(lib().pt_radon_set_variant(self._h, int(streams), int(gather)), "radonusfft.set_variant")
+
+    def status(self):
+        """(TMA gather failure code since the last call: 0 none, 1 a tile load
+        timed out, 2 a misaligned staging buffer; TMA gather available)."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        check(lib().pt_radon_status(self._h, ctypes.byref(a), ctypes.byref(b)), "radonusfft.status")
+        return a.value, bool(b.value)
 
     def get_xy(self, x, y, stream=None):
         """Copy the polar coordinate tables (each float32 [Ntheta, N])."""

@@ -1,8 +1,9 @@
 """The autotuners: ptychofft.autotune picks the adjoint's angle split and
 radonusfft.autotune the forward's stream count and gather variant by timing;
 every choice keeps the operators' results (against the oracle, rel-L2 <=
-1e-5), and the four radon forward variants (one or two streams, gather
-through L1 or from shared-memory tiles) give bit-identical projections."""
+1e-5), and the six radon forward variants (one or two streams; gather
+through L1, from shared-memory tiles copied by the threads, or from tiles
+loaded by the TMA) give bit-identical projections."""
 import numpy as np
 import pytest
 
@@ -52,16 +53,19 @@ def test_radon_autotune_keeps_the_forward():
     op.setobj(T(theta))
     f = T(crand(rng, (nz, n, n)))
     g = torch.empty((nt, nz, n), dtype=torch.complex64, device="cuda")
-    op.set_variant(1, False)
+    op.set_variant(1, 0)
     before = torch.empty_like(g)
     op.fwd(before, f)
+    timeouts, tma = op.status()
+    assert tma and timeouts == 0
     for streams in (1, 2):
-        for tiled in (False, True):
-            op.set_variant(streams, tiled)
+        for gather in (0, 1, 2):
+            op.set_variant(streams, gather)
             op.fwd(g, f)
-            assert torch.equal(g, before), (streams, tiled)
-    streams, tiled = op.autotune(g, f, trials=2)
-    assert streams in (1, 2) and tiled in (0, 1)
+            assert torch.equal(g, before), (streams, gather)
+    assert op.status() == (0, True)
+    streams, gather = op.autotune(g, f, trials=2)
+    assert streams in (1, 2) and gather in (0, 1, 2)
     op.fwd(g, f)
     assert torch.equal(g, before)
     x = torch.empty((nt, op.N), dtype=torch.float32, device="cuda")
@@ -72,21 +76,25 @@ def test_radon_autotune_keeps_the_forward():
     assert rel(g.cpu().numpy(), orc.fwd(f.cpu().numpy())) <= 1e-5
 
 
-@pytest.mark.parametrize("n,nz,nt", [(16, 5, 12), (32, 9, 24), (256, 3, 384)])
-def test_tiled_gather_is_bit_identical(n, nz, nt):
-    """The shared-memory tiled gather against the L1 gather at small grids
-    (where the staged region is clipped to the haloed grid) and at the
-    bench's width and angle count."""
+@pytest.mark.parametrize("n,nz,nt,m", [(16, 5, 12, 0), (32, 9, 24, 0), (256, 3, 384, 0), (64, 8, 40, 4)])
+def test_tiled_gathers_are_bit_identical(n, nz, nt, m):
+    """The shared-memory tiled gather and its TMA-staged form against the
+    L1 gather at small grids (where the staged region runs past the haloed
+    grid: clipped by the threads, zero-filled by the TMA), at the bench's
+    width and angle count, and with the M = 4 kernel."""
     from ptychotomo_b200 import radonusfft
     rng = np.random.default_rng(n)
     theta = np.sort(rng.uniform(0, np.pi, nt)).astype(np.float32)
-    op = radonusfft(nt, nz, n)
+    op = radonusfft(nt, nz, n, m) if m else radonusfft(nt, nz, n)
     op.setobj(T(theta))
     f = T(crand(rng, (nz, n, n)))
     a = torch.empty((nt, nz, n), dtype=torch.complex64, device="cuda")
-    b = torch.empty_like(a)
-    op.set_variant(1, False)
+    b, c = torch.empty_like(a), torch.empty_like(a)
+    op.set_variant(1, 0)
     op.fwd(a, f)
-    op.set_variant(1, True)
+    op.set_variant(1, 1)
     op.fwd(b, f)
-    assert torch.equal(a, b)
+    op.set_variant(2, 2)
+    op.fwd(c, f)
+    assert op.status() == (0, True)
+    assert torch.equal(a, b) and torch.equal(a, c)
