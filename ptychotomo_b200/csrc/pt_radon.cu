@@ -189,15 +189,16 @@ constexpr int GTILE = 16;   // grid cells per tile edge of the visiting order
 template <int N, int M>
 __global__ void __launch_bounds__(GPB *ZC, 3)
     k_fwd_gather_pts(const float2 *__restrict__ fg, float2 *__restrict__ lines, const float *__restrict__ xt,
-                     const float *__restrict__ yt, float a, float pre, const int *__restrict__ perm, int npts)
+                     const float *__restrict__ yt, float a, float pre, const float4 *__restrict__ ptab, int npts)
 {
     constexpr int G = 2 * N, W = 2 * M + 1, NP = (W + 2) / 2;  // column pairs covering the window
     const int lane = threadIdx.x % ZC;
     const int pi = blockIdx.x * GPB + threadIdx.x / ZC;
     if (pi >= npts) return;
-    const int p = __ldg(&perm[pi]);
+    const float4 q = __ldg(&ptab[pi]);   // (x, y, point index) in visiting order
+    const int p = __float_as_int(q.z);
     const int th = p / N, k = p % N;
-    const float x0 = xt[th * N + k], y0 = yt[th * N + k];
+    const float x0 = q.x, y0 = q.y;
     // x0, y0 in [-1/2, 1/2) (validated at setobj); clamp keeps reads in bounds
     const int fx = min(max((int)floorf((float)G * x0), -N), N - 1);
     const int fy = min(max((int)floorf((float)G * y0), -N), N - 1);
@@ -261,19 +262,23 @@ template <int M>
 constexpr size_t tile_smem() { return (size_t)tile_rows<M>() * tile_pairs<M>() * ZC * sizeof(float4); }
 
 // The gather of one chunk's points from its staged tile (both tiled kernels).
+// Each thread's next point is loaded before the current one is gathered.
 template <int N, int M>
 __device__ __forceinline__ void tile_gather(const float4 *__restrict__ tsm, int4 ch, int ty0, int px0,
-                                            float2 *__restrict__ lines, const float *__restrict__ xt,
-                                            const float *__restrict__ yt, float a, float pre,
-                                            const int *__restrict__ perm)
+                                            float2 *__restrict__ lines, float a, float pre,
+                                            const float4 *__restrict__ ptab)
 {
     constexpr int G = 2 * N, W = 2 * M + 1, NP = (W + 2) / 2;
     constexpr int TP = tile_pairs<M>();
     const int lane = threadIdx.x % ZC;
-    for (int t = threadIdx.x / ZC; t < ch.w; t += GPB) {
-        const int p = __ldg(&perm[ch.z + t]);
+    int t = threadIdx.x / ZC;
+    float4 nq = t < ch.w ? __ldg(&ptab[ch.z + t]) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (; t < ch.w; t += GPB) {
+        const float4 q = nq;
+        if (t + GPB < ch.w) nq = __ldg(&ptab[ch.z + t + GPB]);
+        const int p = __float_as_int(q.z);
         const int th = p / N, k = p % N;
-        const float x0 = xt[th * N + k], y0 = yt[th * N + k];
+        const float x0 = q.x, y0 = q.y;
         const int fx = min(max((int)floorf((float)G * x0), -N), N - 1);
         const int fy = min(max((int)floorf((float)G * y0), -N), N - 1);
         const int c0 = wrapG(N + fx - M, G);
@@ -322,7 +327,7 @@ __device__ __forceinline__ void tile_gather(const float4 *__restrict__ tsm, int4
 template <int N, int M>
 __global__ void __launch_bounds__(GPB *ZC, 3)
     k_fwd_gather_tile(const float2 *__restrict__ fg, float2 *__restrict__ lines, const float *__restrict__ xt,
-                      const float *__restrict__ yt, float a, float pre, const int *__restrict__ perm,
+                      const float *__restrict__ yt, float a, float pre, const float4 *__restrict__ ptab,
                       const int4 *__restrict__ chunks)
 {
     constexpr int G = 2 * N;
@@ -338,7 +343,7 @@ __global__ void __launch_bounds__(GPB *ZC, 3)
         tsm[(r * TP + pj) * ZC + q] = __ldg(&g4[((size_t)(ty0 + r) * PS + px0 + pj) * ZC + q]);
     }
     __syncthreads();
-    tile_gather<N, M>(tsm, ch, ty0, px0, lines, xt, yt, a, pre, perm);
+    tile_gather<N, M>(tsm, ch, ty0, px0, lines, a, pre, ptab);
 }
 
 // The same with the tile staged by the Tensor Memory Accelerator: one
@@ -358,7 +363,7 @@ template <int N, int M>
 __global__ void __launch_bounds__(GPB *ZC, 3)
     k_fwd_gather_tma(const __grid_constant__ CUtensorMap tmap, float2 *__restrict__ lines,
                      const float *__restrict__ xt, const float *__restrict__ yt, float a, float pre,
-                     const int *__restrict__ perm, const int4 *__restrict__ chunks, int *__restrict__ err)
+                     const float4 *__restrict__ ptab, const int4 *__restrict__ chunks, int *__restrict__ err)
 {
     constexpr unsigned BYTES = (unsigned)tile_smem<M>();
     static_assert(BYTES % 128 == 0, "the mbarrier follows the tile");
@@ -397,7 +402,7 @@ __global__ void __launch_bounds__(GPB *ZC, 3)
         if (threadIdx.x == 0) atomicExch(err, 1);
         return;
     }
-    tile_gather<N, M>(tsm, ch, ty0, px0, lines, xt, yt, a, pre, perm);
+    tile_gather<N, M>(tsm, ch, ty0, px0, lines, a, pre, ptab);
 }
 
 // ---- K3b: fftshift1c / 1-D inverse FFT / fftshift1c + crop + scale --------
@@ -697,6 +702,7 @@ struct pt_radon {
     float *theta = nullptr, *x = nullptr, *y = nullptr;
     int *fxy = nullptr;
     int *perm = nullptr;   // the forward gather's point order (grid tiles)
+    float4 *ptab = nullptr;   // (x, y, point index as bits, 0) of each point in that order
     int4 *chunks = nullptr;   // the tiled gather's blocks: (tile row, tile column, first, count)
     int nchunks = 0, chunks_cap = 0;
     int gather = 0;           // 0: gather through L1 (k_fwd_gather_pts), 1: shared-memory tiles, 2: TMA-staged tiles
@@ -726,7 +732,8 @@ namespace {
 
 void radon_free(pt_radon *h)
 {
-    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->perm, h->chunks, h->rbuf, h->fgrid, h->rbuf2,
+    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->perm, h->ptab, h->chunks, h->rbuf, h->fgrid,
+                    h->rbuf2,
                     h->fgrid2, h->tma_err,
                     h->lines, h->rbuf_adj, h->mbuf, h->goff, h->col_order, h->gpt, h->gw, h->deap};
     for (void *p : bufs)
@@ -850,14 +857,14 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
         const int npts = h->ntheta * N;
         if (h->gather == 2) {
             k_fwd_gather_tma<N, M><<<h->nchunks, GPB * ZC, tma_smem<M>(), s>>>(
-                h->tmap[odd ? 1 : 0], ln, h->x, h->y, a, pre, h->perm, h->chunks, h->tma_err);
+                h->tmap[odd ? 1 : 0], ln, h->x, h->y, a, pre, h->ptab, h->chunks, h->tma_err);
             PT_LAUNCHED("k_fwd_gather_tma");
         } else if (h->gather == 1) {
-            k_fwd_gather_tile<N, M><<<h->nchunks, GPB * ZC, tile_smem<M>(), s>>>(fg, ln, h->x, h->y, a, pre, h->perm,
+            k_fwd_gather_tile<N, M><<<h->nchunks, GPB * ZC, tile_smem<M>(), s>>>(fg, ln, h->x, h->y, a, pre, h->ptab,
                                                                               h->chunks);
             PT_LAUNCHED("k_fwd_gather_tile");
         } else {
-            k_fwd_gather_pts<N, M><<<(npts + GPB - 1) / GPB, GPB * ZC, 0, s>>>(fg, ln, h->x, h->y, a, pre, h->perm,
+            k_fwd_gather_pts<N, M><<<(npts + GPB - 1) / GPB, GPB * ZC, 0, s>>>(fg, ln, h->x, h->y, a, pre, h->ptab,
                                                                              npts);
             PT_LAUNCHED("k_fwd_gather_pts");
         }
@@ -1009,6 +1016,7 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     if (rc == PT_OK) rc = dmalloc(&h->y, ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->fxy, 2 * ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->perm, ntheta * N);
+    if (rc == PT_OK) rc = dmalloc(&h->ptab, ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->rbuf, N * G * ZC);
     if (rc == PT_OK) rc = dmalloc(&h->rbuf2, N * G * ZC);
     if (rc == PT_OK) rc = dmalloc(&h->deap, (size_t)N * N);
@@ -1110,6 +1118,16 @@ extern "C" int pt_radon_setobj(pt_radon *h, const float *theta, void *stream)
         }
         std::stable_sort(perm.begin(), perm.end(), [&](int i, int j) { return tile[i] < tile[j]; });
         PT_CUDA(cudaMemcpy(h->perm, perm.data(), npts * sizeof(int), cudaMemcpyHostToDevice));
+        std::vector<float4> ptab(npts);
+        for (size_t i = 0; i < npts; ++i) {
+            const int q = perm[i];
+            int bits;
+            std::memcpy(&bits, &q, sizeof(int));
+            float qf;
+            std::memcpy(&qf, &bits, sizeof(float));
+            ptab[i] = make_float4(xs[q], ys[q], qf, 0.f);
+        }
+        PT_CUDA(cudaMemcpy(h->ptab, ptab.data(), npts * sizeof(float4), cudaMemcpyHostToDevice));
         // the tiled gather's blocks: runs of one tile in perm order, at most TCH points each
         std::vector<int4> chunks;
         for (size_t i = 0; i < npts;) {
