@@ -1255,12 +1255,6 @@ def run_time_to_target(args, local):
     def reach(us, ts):
         r = {}
         for m, (u, t) in enumerate(zip(us, ts)):
-            if max(_rel_parts(u, ref)) <= floor:
-                r["within_floor"] = {"iteration": m, "seconds": round(t, 3)}
-                break
-        else:
-            r["within_floor"] = {"iteration": None, "seconds": None}
-        for m, (u, t) in enumerate(zip(us, ts)):
             ed, eb = _rel_parts(u, ref)
             if max(ed, eb) <= c["tol"]:
                 r = {"iteration": m, "seconds": round(t, 3)}
@@ -1276,6 +1270,12 @@ def run_time_to_target(args, local):
                 break
         else:
             r["plain_quality"] = {"iteration": None, "seconds": None}
+        for m, (u, t) in enumerate(zip(us, ts)):
+            if max(_rel_parts(u, ref)) <= floor:
+                r["within_floor"] = {"iteration": m, "seconds": round(t, 3)}
+                break
+        else:
+            r["within_floor"] = {"iteration": None, "seconds": None}
         qd, qb = _rel_parts(us[-1], u_true)
         r["final_error_vs_truth"] = {"delta": float("%.4g" % qd), "beta": float("%.4g" % qb)}
         return r
