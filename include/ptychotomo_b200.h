@@ -168,7 +168,8 @@ int pt_ptycho_get_parts(const pt_ptycho *h, int *parts);
  * interpolation of the probe, and no per-scan phase; fwd, adj and the fused
  * residual adjoints all follow it.  quant = 0 restores the reference model.
  * Builds one shifted probe table per distinct offset pair (at most 2 GiB;
- * rebuilt by every later setobj), needs setobj first and a detector of 16 or
+ * rebuilt by every later setobj, which switches the model off if that
+ * fails), needs setobj first and a detector of 16 or
  * more; probe retrieval is refused while it is on.  Set-up: allocates,
  * blocks the host. */
 int pt_ptycho_set_subpixel(pt_ptycho *h, int quant, void *stream);

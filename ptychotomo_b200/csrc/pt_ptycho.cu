@@ -1604,7 +1604,11 @@ extern "C" int pt_ptycho_setobj(pt_ptycho *h, const float *scan, const void *prb
         }
     }
     h->ready = true;
-    if (h->quant) return subpixel_build(h, h->quant, st);   // new offsets or probe: new shifted tables
+    if (h->quant) {   // new offsets or probe: new shifted tables (on failure the model is switched off)
+        const int rc = subpixel_build(h, h->quant, st);
+        if (rc != PT_OK) subpixel_free(h);
+        return rc;
+    }
     return PT_OK;
 }
 

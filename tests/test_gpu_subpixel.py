@@ -170,3 +170,36 @@ def test_solver_option():
     scan = synthetic.raster_scan(nt, 3, n, n, P) + np.float32(0.3)
     slv = Solver(synthetic.probe(P, seed=1), scan, theta, [P, P], 1e-6, 5.0, nt, n, n, nt, n, subpixel=32)
     assert slv.subpixel == 32 and slv.cl_ptycho.subpixel[0] == 32
+
+
+def test_solver_with_subpixel_scans_matches_oracle():
+    """The Solver's ptycho forward and its Poisson CG under the sub-pixel
+    model against the oracle Solver whose operator runs the same model
+    (the CG to 1e-3, as for the reference model)."""
+    from oracle.solver import Solver as OSolver
+    from ptychotomo_b200 import Solver, synthetic
+    n = nz = 32
+    nt, P, quant = 8, 16, 64
+    theta = synthetic.angles(nt)
+    prb = synthetic.probe(P, seed=1)
+    scan = synthetic.raster_scan(nt, 3, n, nz, P)
+    scan[0] += np.float32(0.3)
+    scan[1] += np.float32(0.45)
+    obj = synthetic.phantom(n, nz, seed=2)
+    args = (prb, scan, theta, [P, P], 1e-6, 5.0, nt, nz, n, nt, nz)
+    gs = Solver(*args, subpixel=quant)
+    x = torch.empty((nt, gs.cl_tomo.N), dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    gs._tomo_all.get_xy(x, y)
+    os_ = OSolver(*args, xy=(x.cpu().numpy(), y.cpu().numpy()))
+    os_.cl_ptycho.set_subpixel(quant)
+    psi = os_.exptomo(os_.fwd_tomo_batch(obj))
+    want = os_.fwd_ptycho_batch(psi)
+    got = gs.fwd_ptycho_batch(T(psi))
+    assert rel(got.cpu().numpy(), want) <= 1e-5
+    data = np.random.default_rng(3).poisson(want * 1e3).astype(np.float32) / np.float32(1e3)
+    psi0 = np.ones((nt, nz, n), np.complex64)
+    h, lamd = np.ones_like(psi0), np.zeros_like(psi0)
+    pg = gs.cg_ptycho_batch(T(data), T(psi0), T(h), T(lamd), 0.5, 4, "poisson")
+    po = os_.cg_ptycho_batch(data, psi0, h, lamd, 0.5, 4, "poisson")
+    assert rel(pg.cpu().numpy(), po) < 1e-3
