@@ -460,7 +460,9 @@ def cpu_baseline(c, workers=1, slices_per_worker=2, angles_per_worker=8):
             "sample": f"{workers} process(es) x ({slices_per_worker} of {c['nz']} slices radonusfft fwd+adj + "
                       f"{angles_per_worker} of {c['ntheta']} angles ptychofft fwd+adj), NumPy oracle; "
                       f"extrapolated: {t_slice:.2f} s/slice, {t_angle:.3f} s/angle",
-            "seconds": round(wall, 2), "est_full_step_s": round(t_full, 1)}
+            "seconds": round(wall, 2), "est_full_step_s": round(t_full, 1),
+            "est_per_operator_s": {"radonusfft_fwd_adj": round(t_slice * c["nz"] / workers, 2),
+                                   "ptychofft_fwd_adj": round(t_angle * c["ntheta"] / workers, 2)}}
 
 
 def run_reference_cpu(args):
