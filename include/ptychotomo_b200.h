@@ -266,6 +266,13 @@ int pt_mlp_param_count(void);
 size_t pt_mlp_workspace_bytes(void);
 /* z[p] = MLP(x[p][0..2]) for p < npts. */
 int pt_mlp_forward(const float *params, int bf16, const float *x, float *z, size_t npts, void *stream);
+/* The same forward with the 64 x 64 layer on the tensor cores: per tile of
+ * 128 points one chain of tcgen05.mma (kind::f16, bf16 A = h1 rounded from
+ * FP32, bf16 B = W2, FP32 accumulators in tensor memory), read back with
+ * tcgen05.ld; layer 1 and the epilogue in FP32 with bf16 weights.  *err (a
+ * device int) is set nonzero if a tile's bounded wait for its MMAs ran out
+ * (that tile's z is then not written). */
+int pt_mlp_forward_tc(const float *params, const float *x, float *z, size_t npts, int *err, void *stream);
 /* Least-squares loss inv_wsum * sum_p w[p] (z[p] - y[p])^2 into *loss (device
  * double) and its gradient with respect to the parameters into grad
  * (device float[param_count]).  Deterministic: fixed per-block tiles, fixed

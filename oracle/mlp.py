@@ -66,11 +66,16 @@ def _dsilu(s):
     return sg * (1.0 + s * (1.0 - sg))
 
 
-def forward(params, x, bf16=True):
+def forward(params, x, bf16=True, act_bf16=False):
+    """act_bf16: the hidden layer h1 enters the 64 x 64 layer rounded to
+    bfloat16 (from its float32 value), as in the tensor-core forward."""
     d = unpack(effective(params, bf16))
     x = np.asarray(x, np.float64).reshape(-1, DIN)
     s1 = x @ d["W1"].T + d["b1"]
-    s2 = _silu(s1) @ d["W2"].T + d["b2"]
+    h1 = _silu(s1)
+    if act_bf16:
+        h1 = bf16_round(h1.astype(np.float32)).astype(np.float64)
+    s2 = h1 @ d["W2"].T + d["b2"]
     return _silu(s2) @ d["W3"] + d["b3"][0]
 
 

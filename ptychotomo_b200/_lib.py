@@ -126,6 +126,7 @@ SIGNATURES = {
     "pt_mlp_param_count": (_int, []),
     "pt_mlp_workspace_bytes": (_sz, []),
     "pt_mlp_forward": (_int, [_vp, _int, _vp, _vp, _sz, _vp]),
+    "pt_mlp_forward_tc": (_int, [_vp, _vp, _vp, _sz, _vp, _vp]),
     "pt_mlp_grad": (_int, [_vp, _int, _vp, _vp, _vp, _sz, _f, _vp, _vp, _vp, _vp]),
     "pt_mlp_adam": (_int, [_vp, _vp, _vp, _vp, _int, _f, _f, _f, _f, _vp]),
 }

@@ -298,6 +298,169 @@ int grad_blocks()
 
 }  // namespace
 
+namespace {
+
+// ---- forward on the 5th-generation tensor cores ---------------------------
+// The 64 x 64 layer as one tcgen05 MMA chain per tile of 128 points: A = the
+// tile's h1 (bf16, 128 x 64, K-major), B = W2 (bf16, 64 x 64, K-major), D =
+// the FP32 accumulators in tensor memory (128 lanes x 64 columns), read back
+// with tcgen05.ld for the epilogue (+ b2, SiLU, W3, b3) in FP32.  Layer 1 and
+// the epilogue run on the CUDA cores as in k_mlp_forward; the difference is
+// that h1 enters the MMA rounded to bf16 (the weights are bf16 in both).
+//
+// Shared-memory operands use the no-swizzle K-major canonical layout: core
+// matrices of 8 rows x 16 bytes (8 bf16 of K), row group g and K chunk c at
+// byte (8 g + c) * 128, row r of the group at + 16 r.  One MMA covers K = 16,
+// i.e. chunks 2s and 2s + 1: leading (K) byte offset 128, stride (row group)
+// byte offset 1024.  Descriptor and instruction-descriptor bit layouts follow
+// the sm_100 UMMA definitions (CUTLASS cute/arch/mma_sm100_desc.hpp).
+constexpr int TCM = 128;                          // points (MMA rows) per tile
+constexpr int TC_A = 0, TC_B = TCM * H * 2;       // byte offsets: A 16 KB, B 8 KB
+constexpr int TC_NET = TC_B + H * H * 2;          // FP32 parameters
+constexpr int TC_BAR = TC_NET + ((NPAR + 3) / 4) * 16;
+constexpr int TC_SMEM = TC_BAR + 16;              // + mbarrier (8 B) and the TMEM address (4 B)
+constexpr int TC_SPIN = 1 << 22;
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
+{
+    // start address >> 4 [0,14), leading byte offset >> 4 [16,30), stride byte
+    // offset >> 4 [32,46), version 1 [46,48), layout SWIZZLE_NONE (0) [61,64)
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46);
+}
+// c_format F32 [4,6) = 1, a_format BF16 [7,10) = 1, b_format BF16 [10,13) = 1,
+// K-major A and B, n_dim = N >> 3 [17,23), m_dim = M >> 4 [24,29)
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(H >> 3) << 17) | ((uint32_t)(TCM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);   // .x = a (low half), .y = b
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+__global__ void __launch_bounds__(TCM) k_mlp_forward_tc(const float *__restrict__ params, const float *__restrict__ x,
+                                                        float *__restrict__ z, size_t npts, int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) unsigned char smc[];
+    float *net = reinterpret_cast<float *>(smc + TC_NET);
+    const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smc);
+    const uint32_t bar = sbase + TC_BAR, slot = sbase + TC_BAR + 8;
+    stage_params(net, params, 1);
+    // B: W2 rows (outputs) x K chunks of 8, bf16
+    for (int e = t; e < H * (H / 8); e += TCM) {
+        const int n = e / (H / 8), c = e % (H / 8);
+        const float *w = params + OW2 + n * H + 8 * c;
+        const uint4 q = make_uint4(pack_bf16x2(w[0], w[1]), pack_bf16x2(w[2], w[3]), pack_bf16x2(w[4], w[5]),
+                                   pack_bf16x2(w[6], w[7]));
+        *reinterpret_cast<uint4 *>(smc + TC_B + ((n / 8) * 8 + c) * 128 + (n % 8) * 16) = q;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot), "r"(H));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const uint32_t tmem = *reinterpret_cast<const uint32_t *>(smc + TC_BAR + 8);
+    // layer 1 for this thread's point (row t of A)
+    const size_t pidx = (size_t)blockIdx.x * TCM + t;
+    float x0 = 0.f, x1 = 0.f, x2 = 0.f;
+    if (pidx < npts) {
+        x0 = x[3 * pidx];
+        x1 = x[3 * pidx + 1];
+        x2 = x[3 * pidx + 2];
+    }
+#pragma unroll
+    for (int c = 0; c < H / 8; ++c) {
+        float h[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) h[i] = silu(layer1(net, 8 * c + i, x0, x1, x2));
+        const uint4 q = make_uint4(pack_bf16x2(h[0], h[1]), pack_bf16x2(h[2], h[3]), pack_bf16x2(h[4], h[5]),
+                                   pack_bf16x2(h[6], h[7]));
+        *reinterpret_cast<uint4 *>(smc + TC_A + ((t / 8) * 8 + c) * 128 + (t % 8) * 16) = q;
+    }
+    // the threads' shared-memory writes, then the MMAs (async proxy) that read them
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int s = 0; s < H / 16; ++s) {
+            const uint64_t da = umma_desc(sbase + TC_A + s * 256), db = umma_desc(sbase + TC_B + s * 256);
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                "l"(da), "l"(db), "r"(TC_IDESC), "r"(s), "r"(0), "r"(0), "r"(0), "r"(0)
+                : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                     : "memory");
+    }
+    unsigned done = 0;
+    for (int it = 0; it < TC_SPIN && !done; ++it)
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(bar)
+                     : "memory");
+    if (done) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t row = tmem + ((uint32_t)(32 * warp) << 16);   // this warp's lane quarter
+        float acc = net[OB3];
+#pragma unroll
+        for (int q = 0; q < H / 16; ++q) {
+            uint32_t r[16];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                         "%12, %13, %14, %15}, [%16];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                           "=r"(r[14]), "=r"(r[15])
+                         : "r"(row + 16 * q));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int j = 16 * q + i;
+                acc = fmaf(net[OW3 + j], silu(__uint_as_float(r[i]) + net[OB2 + j]), acc);
+            }
+        }
+        if (pidx < npts) z[pidx] = acc;
+    } else {
+        if (t == 0) atomicExch(err, 1);
+        // let the MMAs (if any are still running) finish before the memory is released
+        for (int it = 0; it < TC_SPIN && !done; ++it)
+            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                         "selp.u32 %0, 1, 0, p;\n\t}\n"
+                         : "=r"(done)
+                         : "r"(bar)
+                         : "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(H));
+}
+
+}  // namespace
+
+extern "C" int pt_mlp_forward_tc(const float *params, const float *x, float *z, size_t npts, int *err, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(params && x && z && err, "mlp_forward_tc: null pointer");
+    if (npts == 0) return PT_OK;
+    static bool attr = false;
+    if (!attr) {
+        PT_CUDA(cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+        attr = true;
+    }
+    const size_t blocks = (npts + TCM - 1) / TCM;
+    PT_CHECK_ARG(blocks < (1u << 31), "mlp_forward_tc: too many points");
+    k_mlp_forward_tc<<<(unsigned)blocks, TCM, TC_SMEM, (cudaStream_t)stream>>>(params, x, z, npts, err);
+    PT_LAUNCHED("k_mlp_forward_tc");
+    return PT_OK;
+}
+
 extern "C" int pt_mlp_param_count(void) { return NPAR; }
 
 extern "C" size_t pt_mlp_workspace_bytes(void) { return (size_t)1024 * NSLOT * sizeof(float); }

@@ -43,6 +43,7 @@ class MLP:
         self.loss = torch.zeros(1, dtype=torch.float64, device=self.device)
         self.work = torch.empty(lib().pt_mlp_workspace_bytes() // 4, dtype=torch.float32, device=self.device)
         self.step = 0
+        self._tc_err = None
 
     @classmethod
     def init_params(cls, seed=0):
@@ -61,6 +62,27 @@ class MLP:
         check(lib().pt_mlp_forward(_p(self.params), int(self.bf16), _p(x), _p(out), n, current_stream()),
               "mlp_forward")
         return out
+
+    def forward_tc(self, x, out=None):
+        """The same network on the tensor cores: the 64 x 64 layer as tcgen05
+        MMAs (bf16 weights and bf16-rounded h1, FP32 accumulation in tensor
+        memory), layer 1 and the rest in FP32.  Raises if a tile's MMA did not
+        complete within its bounded wait."""
+        n = x.shape[0]
+        out = torch.empty(n, dtype=torch.float32, device=self.device) if out is None else out
+        if self._tc_err is None:
+            self._tc_err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        check(lib().pt_mlp_forward_tc(_p(self.params), _p(x), _p(out), n, _p(self._tc_err), current_stream()),
+              "mlp_forward_tc")
+        return out
+
+    def tc_status(self):
+        """Nonzero if a tensor-core forward's MMA wait ran out (then cleared)."""
+        if self._tc_err is None:
+            return 0
+        v = int(self._tc_err.item())
+        self._tc_err.zero_()
+        return v
 
     def loss_grad(self, x, y, w, inv_wsum):
         """Loss (device double, kept in self.loss) and gradient (self.grad)."""
