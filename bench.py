@@ -1070,6 +1070,23 @@ def run_precond(args, local):
     est_log = ((ys * ws).sum(0) / ws.sum(0).clamp(min=1)).contiguous()
     del hs, hpre, tg
     torch.cuda.empty_cache()
+    # the network's forward over a 512^2 frequency grid (262,144 points): CUDA
+    # cores (FP32 h1) against the tensor cores (tcgen05 64 x 64 layer)
+    xq = torch.rand((512 * 512, 3), device=dev)
+    fwd_ms = {}
+    for label, fn in (("cuda_cores", net.forward), ("tensor_cores", net.forward_tc)):
+        for _ in range(3):
+            fn(xq)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            fn(xq)
+        e1.record()
+        torch.cuda.synchronize()
+        fwd_ms[label] = round(e0.elapsed_time(e1) / 20, 4)
+    if net.tc_status():
+        raise RuntimeError("tensor-core forward: an MMA wait ran out")
+    del xq
     # the subproblem at 256^3
     slv, th = _precond_setup(c, torch, dev, c["nz"])
     pre = FourierPreconditioner(slv._tomo_all, th, slv.coeftomo, dev)
@@ -1114,6 +1131,7 @@ def run_precond(args, local):
             "config": {"workload": json.dumps({k: (round(v, 6) if isinstance(v, float) else v) for k, v in c.items()})},
             "training": {"harvest_s": round(t_harvest, 2), "train_s": round(t_train, 2), "steps": c["steps"],
                          "loss_first": hist[0][1], "train_loss": train_loss, "held_out_loss": held},
+            "network_forward_ms_262144_points": fwd_ms,
             "subproblem": out}
 
 

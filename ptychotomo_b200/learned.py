@@ -138,9 +138,16 @@ class FourierPreconditioner:
               "precond features")
         self.net = None
 
-    def set_network(self, net):
-        """Symbol a = exp(net(features)) for every frequency."""
-        z = net.forward(self.x)
+    def set_network(self, net, tensor_cores=True):
+        """Symbol a = exp(net(features)) for every frequency, evaluated on the
+        tensor cores (MLP.forward_tc) when the network has bf16 weights and
+        tensor_cores is set, else on the CUDA cores (MLP.forward)."""
+        if tensor_cores and net.bf16:
+            z = net.forward_tc(self.x)
+            if net.tc_status():
+                raise RuntimeError("precond: a tensor-core MMA wait ran out while evaluating the symbol")
+        else:
+            z = net.forward(self.x)
         check(lib().pt_precond_set_log_symbol(self._h, _p(z), current_stream()), "precond set_log_symbol")
         self.net = net
 
