@@ -98,6 +98,13 @@ int pt_radon_set_variant(pt_radon *h, int streams, int gather);
  * its points without issuing or waiting) and whether the TMA gather is
  * available.  Blocks the host. */
 int pt_radon_status(pt_radon *h, int *tma_timeouts, int *tma_available);
+/* Tests the TMA gather's bounded wait: one launch over the first slice
+ * chunk's grid whose blocks wait, with a short spin limit, on an mbarrier
+ * that nothing arrives at, so every wait runs out and records the failure
+ * instead of hanging; each block then waits for its real tile copy before
+ * returning.  *code receives the recorded code (1 expected) and the flag is
+ * cleared.  Writes no output.  Blocks the host. */
+int pt_radon_check_tma_wait(pt_radon *h, int *code, void *stream);
 /* Internal parameters: N, kernel half-width M, mu. */
 int pt_radon_get_params(const pt_radon *h, int *N, int *M, float *mu);
 /* Copies the polar coordinate tables x, y (device float[Ntheta][N] each). */
@@ -273,6 +280,12 @@ int pt_mlp_forward(const float *params, int bf16, const float *x, float *z, size
  * device int) is set nonzero if a tile's bounded wait for its MMAs ran out
  * (that tile's z is then not written). */
 int pt_mlp_forward_tc(const float *params, const float *x, float *z, size_t npts, int *err, void *stream);
+/* Tests that kernel's bounded wait: one tile of 128 points (x: 128 x 3,
+ * z: 128) whose threads first wait, with a short spin limit, on an mbarrier
+ * that nothing arrives at; the wait runs out, *err is set to 1, the MMAs'
+ * own barrier is awaited before the tensor memory is released, and z is not
+ * written. */
+int pt_mlp_check_tc_wait(const float *params, const float *x, float *z, int *err, void *stream);
 /* Least-squares loss inv_wsum * sum_p w[p] (z[p] - y[p])^2 into *loss (device
  * double) and its gradient with respect to the parameters into grad
  * (device float[param_count]).  Deterministic: fixed per-block tiles, fixed

@@ -72,6 +72,7 @@ SIGNATURES = {
     "pt_radon_autotune": (_int, [_vp, _vp, _vp, _int, ctypes.POINTER(_int), _vp]),
     "pt_radon_set_variant": (_int, [_vp, _int, _int]),
     "pt_radon_status": (_int, [_vp, ctypes.POINTER(_int), ctypes.POINTER(_int)]),
+    "pt_radon_check_tma_wait": (_int, [_vp, ctypes.POINTER(_int), _vp]),
     "pt_reduce_workspace_bytes": (_sz, []),
     "pt_reduce_c64": (_int, [_int, _vp, _vp, _sz, _int, _int, _int, _vp, _vp, _vp]),
     "pt_ls_frames": (_int, [_vp, _vp, _vp, _f, _sz, _int, _vp, _int, _vp, _vp, _vp]),
@@ -127,6 +128,7 @@ SIGNATURES = {
     "pt_mlp_workspace_bytes": (_sz, []),
     "pt_mlp_forward": (_int, [_vp, _int, _vp, _vp, _sz, _vp]),
     "pt_mlp_forward_tc": (_int, [_vp, _vp, _vp, _sz, _vp, _vp]),
+    "pt_mlp_check_tc_wait": (_int, [_vp, _vp, _vp, _vp, _vp]),
     "pt_mlp_grad": (_int, [_vp, _int, _vp, _vp, _vp, _sz, _f, _vp, _vp, _vp, _vp]),
     "pt_mlp_adam": (_int, [_vp, _vp, _vp, _vp, _int, _f, _f, _f, _f, _vp]),
 }

@@ -318,7 +318,7 @@ constexpr int TCM = 128;                          // points (MMA rows) per tile
 constexpr int TC_A = 0, TC_B = TCM * H * 2;       // byte offsets: A 16 KB, B 8 KB
 constexpr int TC_NET = TC_B + H * H * 2;          // FP32 parameters
 constexpr int TC_BAR = TC_NET + ((NPAR + 3) / 4) * 16;
-constexpr int TC_SMEM = TC_BAR + 16;              // + mbarrier (8 B) and the TMEM address (4 B)
+constexpr int TC_SMEM = TC_BAR + 32;              // + mbarrier, the TMEM address, the check's mbarrier
 constexpr int TC_SPIN = 1 << 22;
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
@@ -339,13 +339,18 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
 }
 
 __global__ void __launch_bounds__(TCM) k_mlp_forward_tc(const float *__restrict__ params, const float *__restrict__ x,
-                                                        float *__restrict__ z, size_t npts, int *__restrict__ err)
+                                                        float *__restrict__ z, size_t npts, int *__restrict__ err,
+                                                        int spin = TC_SPIN, int check = 0)
 {
+    // check != 0 (the status test only): the threads first wait on a second
+    // barrier that nothing arrives at, so that wait runs out on purpose; the
+    // failure path then waits for the MMAs' own barrier before the tensor
+    // memory is released
     extern __shared__ __align__(1024) unsigned char smc[];
     float *net = reinterpret_cast<float *>(smc + TC_NET);
     const int t = threadIdx.x, warp = t >> 5;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smc);
-    const uint32_t bar = sbase + TC_BAR, slot = sbase + TC_BAR + 8;
+    const uint32_t bar = sbase + TC_BAR, slot = sbase + TC_BAR + 8, bar2 = sbase + TC_BAR + 16;
     stage_params(net, params, 1);
     // B: W2 rows (outputs) x K chunks of 8, bf16
     for (int e = t; e < H * (H / 8); e += TCM) {
@@ -361,6 +366,7 @@ __global__ void __launch_bounds__(TCM) k_mlp_forward_tc(const float *__restrict_
     }
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar2) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -399,13 +405,17 @@ __global__ void __launch_bounds__(TCM) k_mlp_forward_tc(const float *__restrict_
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                      : "memory");
     }
-    unsigned done = 0;
-    for (int it = 0; it < TC_SPIN && !done; ++it)
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-                     "selp.u32 %0, 1, 0, p;\n\t}\n"
-                     : "=r"(done)
-                     : "r"(bar)
-                     : "memory");
+    auto wait = [&](uint32_t b, int limit) {
+        unsigned ok = 0;
+        for (int it = 0; it < limit && !ok; ++it)
+            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                         "selp.u32 %0, 1, 0, p;\n\t}\n"
+                         : "=r"(ok)
+                         : "r"(b)
+                         : "memory");
+        return ok;
+    };
+    const unsigned done = wait(check ? bar2 : bar, spin);
     if (done) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t row = tmem + ((uint32_t)(32 * warp) << 16);   // this warp's lane quarter
@@ -429,13 +439,7 @@ __global__ void __launch_bounds__(TCM) k_mlp_forward_tc(const float *__restrict_
         if (pidx < npts) z[pidx] = acc;
     } else {
         if (t == 0) atomicExch(err, 1);
-        // let the MMAs (if any are still running) finish before the memory is released
-        for (int it = 0; it < TC_SPIN && !done; ++it)
-            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-                         "selp.u32 %0, 1, 0, p;\n\t}\n"
-                         : "=r"(done)
-                         : "r"(bar)
-                         : "memory");
+        wait(bar, TC_SPIN);   // the MMAs still write tensor memory: let them finish before it is released
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -443,6 +447,16 @@ __global__ void __launch_bounds__(TCM) k_mlp_forward_tc(const float *__restrict_
 }
 
 }  // namespace
+
+extern "C" int pt_mlp_check_tc_wait(const float *params, const float *x, float *z, int *err, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(params && x && z && err, "mlp_check_tc_wait: null pointer");
+    PT_CUDA(cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    k_mlp_forward_tc<<<1, TCM, TC_SMEM, (cudaStream_t)stream>>>(params, x, z, TCM, err, 256, 1);
+    PT_LAUNCHED("k_mlp_forward_tc");
+    return PT_OK;
+}
 
 extern "C" int pt_mlp_forward_tc(const float *params, const float *x, float *z, size_t npts, int *err, void *stream)
 {

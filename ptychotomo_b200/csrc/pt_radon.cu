@@ -352,10 +352,11 @@ __global__ void __launch_bounds__(GPB *ZC, 3)
 // on an mbarrier.  The box lands in exactly the layout of k_fwd_gather_tile's
 // copy (and is zero-filled past the grid's end, where no window reads), so
 // the results are bit-identical.  The wait is bounded: after TMA_SPIN polls
-// the block records the failure in *err and returns without writing.  The
-// mbarrier sits after the tile in dynamic shared memory (no static shared
-// memory, so the tile starts at the 128-byte aligned base; checked, and a
-// misaligned base is recorded in *err instead of issuing the copy).
+// the block records the failure in *err, waits (bounded again) for its tile
+// copy and returns without writing.  The mbarriers sit after the tile in
+// dynamic shared memory (no static shared memory, so the tile starts at the
+// 128-byte aligned base; checked, and a misaligned base is recorded in *err
+// instead of issuing the copy).
 constexpr int TMA_SPIN = 1 << 24;
 template <int M>
 constexpr size_t tma_smem() { return tile_smem<M>() + 16; }
@@ -363,22 +364,27 @@ template <int N, int M>
 __global__ void __launch_bounds__(GPB *ZC, 3)
     k_fwd_gather_tma(const __grid_constant__ CUtensorMap tmap, float2 *__restrict__ lines,
                      const float *__restrict__ xt, const float *__restrict__ yt, float a, float pre,
-                     const float4 *__restrict__ ptab, const int4 *__restrict__ chunks, int *__restrict__ err)
+                     const float4 *__restrict__ ptab, const int4 *__restrict__ chunks, int *__restrict__ err,
+                     int spin = TMA_SPIN, int check = 0)
 {
+    // check != 0 (the status test only): the blocks first wait on a second
+    // barrier that nothing arrives at, so that wait runs out on purpose; the
+    // failure path then waits for the tile copy itself before returning
     constexpr unsigned BYTES = (unsigned)tile_smem<M>();
-    static_assert(BYTES % 128 == 0, "the mbarrier follows the tile");
+    static_assert(BYTES % 128 == 0, "the mbarriers follow the tile");
     extern __shared__ __align__(128) float4 tsm_tma[];
     float4 *tsm = tsm_tma;
     const int4 ch = chunks[blockIdx.x];
     const int ty0 = ch.x * GTILE, px0 = ch.y * GTILE / 2;   // >= 0; the column coordinate is 0
     const unsigned dst = (unsigned)__cvta_generic_to_shared(tsm);
-    const unsigned bar_a = dst + BYTES;
+    const unsigned bar_a = dst + BYTES, bar_b = dst + BYTES + 8;
     if (dst & 127) {
         if (threadIdx.x == 0) atomicExch(err, 2);
         return;
     }
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_b) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -391,15 +397,19 @@ __global__ void __launch_bounds__(GPB *ZC, 3)
             "l"(reinterpret_cast<unsigned long long>(&tmap)), "r"(0), "r"(px0), "r"(ty0), "r"(bar_a)
             : "memory");
     }
-    unsigned done = 0;
-    for (int it = 0; it < TMA_SPIN && !done; ++it)
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(done)
-            : "r"(bar_a), "r"(0)
-            : "memory");
-    if (!done) {
+    auto wait = [&](unsigned bar, int limit) {
+        unsigned ok = 0;
+        for (int it = 0; it < limit && !ok; ++it)
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                : "=r"(ok)
+                : "r"(bar), "r"(0)
+                : "memory");
+        return ok;
+    };
+    if (!wait(check ? bar_b : bar_a, spin)) {
         if (threadIdx.x == 0) atomicExch(err, 1);
+        wait(bar_a, TMA_SPIN);   // the tile copy lands in this block's memory: let it finish first
         return;
     }
     tile_gather<N, M>(tsm, ch, ty0, px0, lines, a, pre, ptab);
@@ -949,6 +959,35 @@ int radon_dispatch(pt_radon *h, bool adj, float2 *out, const float2 *in, float s
     return PT_ERR_UNSUPPORTED;
 }
 
+// The TMA gather of the first slice chunk whose blocks first wait, 256 polls
+// at most, on a barrier that nothing arrives at: every block's wait runs out,
+// records code 1, waits for its own tile copy and returns without writing
+// (the status test of pt_radon_check_tma_wait).
+template <int G, int M>
+int run_tma_wait_check(pt_radon *h, cudaStream_t st)
+{
+    constexpr int N = G / 2;
+    const float a = (float)(PI_REF * PI_REF / h->mu);
+    const float pre = (float)(PI_REF / std::fabs(h->mu)) / (float)N;
+    k_fwd_gather_tma<N, M><<<h->nchunks, GPB * ZC, tma_smem<M>(), st>>>(h->tmap[0], h->lines, h->x, h->y, a, pre,
+                                                                        h->ptab, h->chunks, h->tma_err, 256, 1);
+    PT_LAUNCHED("k_fwd_gather_tma");
+    return PT_OK;
+}
+
+int radon_tma_wait_check(pt_radon *h, cudaStream_t st)
+{
+#define PT_CASE(GG)                                                         \
+    if (h->G == GG) {                                                       \
+        if (h->M == 7) return run_tma_wait_check<GG, 7>(h, st);             \
+        if (h->M == 4) return run_tma_wait_check<GG, 4>(h, st);             \
+    }
+    PT_RADON_GRIDS(PT_CASE)
+#undef PT_CASE
+    pt::set_error("radonusfft: no kernel for grid %d with half-width M=%d", h->G, h->M);
+    return PT_ERR_UNSUPPORTED;
+}
+
 template <typename T>
 int dmalloc(T **p, size_t count)
 {
@@ -1315,6 +1354,25 @@ extern "C" int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials
         }
     }
     return rc;
+}
+
+extern "C" int pt_radon_check_tma_wait(pt_radon *h, int *code, void *stream)
+{
+    pt::clear_error();
+    PT_CHECK_ARG(h && code, "radonusfft.check_tma_wait: null pointer");
+    if (!h->ready || !h->tma_ok) {
+        pt::set_error("radonusfft.check_tma_wait: needs setobj and the TMA gather");
+        return PT_ERR_STATE;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    PT_CUDA(cudaMemsetAsync(h->tma_err, 0, sizeof(int), st));
+    int rc = radon_tma_wait_check(h, st);
+    if (rc != PT_OK) return rc;
+    PT_CUDA(cudaMemcpyAsync(code, h->tma_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PT_CUDA(cudaStreamSynchronize(st));
+    PT_CUDA(cudaMemsetAsync(h->tma_err, 0, sizeof(int), st));
+    PT_CUDA(cudaStreamSynchronize(st));
+    return PT_OK;
 }
 
 extern "C" int pt_radon_status(pt_radon *h, int *tma_timeouts, int *tma_available)

@@ -76,6 +76,18 @@ class MLP:
               "mlp_forward_tc")
         return out
 
+    def check_tc_wait(self):
+        """Run one tile of the tensor-core forward whose wait cannot complete
+        (a barrier nothing arrives at, short limit); returns the recorded
+        failure code (1) and clears it."""
+        x = torch.zeros((128, 3), dtype=torch.float32, device=self.device)
+        z = torch.zeros(128, dtype=torch.float32, device=self.device)
+        if self._tc_err is None:
+            self._tc_err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        check(lib().pt_mlp_check_tc_wait(_p(self.params), _p(x), _p(z), _p(self._tc_err), current_stream()),
+              "mlp_check_tc_wait")
+        return self.tc_status()
+
     def tc_status(self):
         """Nonzero if a tensor-core forward's MMA wait ran out (then cleared)."""
         if self._tc_err is None:

@@ -71,6 +71,13 @@ class radonusfft:  # noqa: N801 - reference class name
         gather 0 (L1), 1 or True (shared-memory tiles), 2 (TMA-staged tiles)."""
         check(lib().pt_radon_set_variant(self._h, int(streams), int(gather)), "radonusfft.set_variant")
 
+    def check_tma_wait(self, stream=None):
+        """Run the TMA gather with a barrier that cannot complete and a short
+        wait limit; returns the failure code the blocks recorded (1)."""
+        code = ctypes.c_int()
+        check(lib().pt_radon_check_tma_wait(self._h, ctypes.byref(code), _s(stream)), "radonusfft.check_tma_wait")
+        return code.value
+
     def status(self):
         """(TMA gather failure code since the last call: 0 none, 1 a tile load
         timed out, 2 a misaligned staging buffer; TMA gather available)."""
