@@ -203,3 +203,31 @@ def test_solver_with_subpixel_scans_matches_oracle():
     pg = gs.cg_ptycho_batch(T(data), T(psi0), T(h), T(lamd), 0.5, 4, "poisson")
     po = os_.cg_ptycho_batch(data, psi0, h, lamd, 0.5, 4, "poisson")
     assert rel(pg.cpu().numpy(), po) < 1e-3
+
+
+def test_subpixel_with_skipped_scans():
+    """Sentinel scans (-1, the reference's 'no frame') under the sub-pixel
+    model: their frames stay zero and the rest match the oracle."""
+    from ptychotomo_b200 import ptychofft
+    rng = np.random.default_rng(9)
+    nt, ns, det, P = 2, 6, 128, 128
+    nz = n = 150
+    scan, prb = setup(rng, nt, ns, nz, n, det, P)
+    scan[:, 0, 2] = -1
+    scan[:, 1, 4] = -1
+    op = ptychofft(nt, nz, n, nt, ns, det, det, P)
+    op.setobj(T(scan), T(prb))
+    op.set_subpixel(32)
+    orc = PtychoFFT(nt, nz, n, nt, ns, det, det, P)
+    orc.setobj(scan, prb)
+    orc.set_subpixel(32)
+    f = crand(rng, (nt, nz, n))
+    g = torch.empty((nt, ns, det, det), dtype=torch.complex64, device="cuda")
+    op.fwd(g, T(f))
+    gn = g.cpu().numpy()
+    assert not gn[0, 2].any() and not gn[1, 4].any()
+    assert rel(gn, orc.fwd(f)) <= 1e-5
+    fa = torch.empty((nt, nz, n), dtype=torch.complex64, device="cuda")
+    d = crand(rng, (nt, ns, det, det))
+    op.adj(fa, T(d))
+    assert rel(fa.cpu().numpy(), orc.adj(d)) <= 1e-5
