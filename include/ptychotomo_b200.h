@@ -78,19 +78,19 @@ int pt_radon_adj_scaled(pt_radon *h, void *f, const void *g, float scale, void *
  * tomography CG, which needs the true gradient of its quadratic. */
 int pt_radon_adj_exact(pt_radon *h, void *f, const void *g, float scale, void *stream);
 /* Autotuner (no counterpart in the reference): times the forward with its
- * 8-slice chunks on the caller's stream alone and pipelined on two streams
- * (one chunk's FFTs under the previous chunk's gather), each with the
+ * 8-slice chunks on the caller's stream alone and pipelined on two and on
+ * four streams (one chunk's FFTs under another chunk's gather), each with the
  * Gaussian gather reading the grid through L1, from shared-memory tiles
  * (16 x 16 window origins per tile) copied by the threads, and from the same
  * tiles loaded by the Tensor Memory Accelerator (one 3-D box per block,
  * completed on an mbarrier; offered when the tensor maps encode), `trials`
  * runs each after a warm-up, and keeps the fastest for this handle
- * (*out = streams + 2 * gather).  g, f: caller buffers of the forward's
+ * (*out = streams + 8 * gather).  g, f: caller buffers of the forward's
  * shapes (overwritten).  Blocks the host.  Every variant gives
  * bit-identical results.  Fails, and withdraws the TMA variant, if a TMA
  * tile load timed out. */
 int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials, int *out, void *stream);
-/* Sets the forward's variant directly: streams 1 or 2, gather 0 (L1),
+/* Sets the forward's variant directly: streams 1, 2 or 4, gather 0 (L1),
  * 1 (tiles) or 2 (TMA tiles; PT_ERR_UNSUPPORTED if unavailable). */
 int pt_radon_set_variant(pt_radon *h, int streams, int gather);
 /* Reads (and clears) the TMA gather's failure code (0 none; 1 a tile load's

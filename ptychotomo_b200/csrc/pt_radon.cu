@@ -45,6 +45,7 @@
 namespace {
 
 constexpr int ZC = 8;   // slices per chunk (slice-minor lanes)
+constexpr int RSETS = 4;   // forward chunk buffer sets (chunks in flight at most)
 constexpr int CK = 2;   // grid columns per block in the column kernels
 constexpr double PI_REF = 3.1415926535;  // kernels.cuh:1
 
@@ -716,20 +717,20 @@ struct pt_radon {
     int4 *chunks = nullptr;   // the tiled gather's blocks: (tile row, tile column, first, count)
     int nchunks = 0, chunks_cap = 0;
     int gather = 0;           // 0: gather through L1 (k_fwd_gather_pts), 1: shared-memory tiles, 2: TMA-staged tiles
-    // gather 2: one 3-D tensor map per grid buffer (fgrid, fgrid2), and a
-    // device flag the TMA kernel sets if a tile load did not complete
-    CUtensorMap tmap[2];
+    // gather 2: one 3-D tensor map per grid buffer set, and a device flag the
+    // TMA kernel sets if a tile load did not complete
+    CUtensorMap tmap[RSETS];
     bool tma_ok = false;
     int *tma_err = nullptr;
-    // forward (per chunk of ZC slices)
-    float2 *rbuf = nullptr, *fgrid = nullptr;
-    // a second chunk buffer set and a side stream: alternate chunks of the
-    // forward run on the caller's stream and on `side`, so one chunk's FFTs
-    // overlap the previous chunk's gather (fork/join by events)
-    float2 *rbuf2 = nullptr, *fgrid2 = nullptr;
-    int streams = 2;   // 1: every chunk on the caller's stream (pt_radon_autotune chooses)
-    cudaStream_t side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // forward: per chunk of ZC slices, a row-FFT buffer and a Fourier grid.
+    // RSETS buffer sets and RSETS - 1 side streams: chunk c runs on set and
+    // stream c % streams (set 0 on the caller's stream), so up to `streams`
+    // chunks are in flight and one chunk's FFTs overlap another's gather
+    // (fork/join by events)
+    float2 *rbuf[RSETS] = {}, *fgrid[RSETS] = {};
+    int streams = 2;   // 1, 2 or 4 (pt_radon_autotune chooses)
+    cudaStream_t side[RSETS - 1] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[RSETS - 1] = {};
     // adjoint (all slices, slice-minor with nzp lanes)
     float2 *lines = nullptr, *rbuf_adj = nullptr, *mbuf = nullptr;
     int *goff = nullptr, *col_order = nullptr, *gpt = nullptr;
@@ -742,15 +743,19 @@ namespace {
 
 void radon_free(pt_radon *h)
 {
-    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->perm, h->ptab, h->chunks, h->rbuf, h->fgrid,
-                    h->rbuf2,
-                    h->fgrid2, h->tma_err,
+    void *bufs[] = {h->tw_G, h->tw_N, h->theta, h->x, h->y, h->fxy, h->perm, h->ptab, h->chunks, h->tma_err,
                     h->lines, h->rbuf_adj, h->mbuf, h->goff, h->col_order, h->gpt, h->gw, h->deap};
     for (void *p : bufs)
         if (p) cudaFree(p);
-    if (h->side) cudaStreamDestroy(h->side);
+    for (int k = 0; k < RSETS; ++k) {
+        if (h->rbuf[k]) cudaFree(h->rbuf[k]);
+        if (h->fgrid[k]) cudaFree(h->fgrid[k]);
+    }
+    for (int k = 0; k < RSETS - 1; ++k) {
+        if (h->side[k]) cudaStreamDestroy(h->side[k]);
+        if (h->ev_join[k]) cudaEventDestroy(h->ev_join[k]);
+    }
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-    if (h->ev_join) cudaEventDestroy(h->ev_join);
 }
 
 // Kernel half-width for a forced M: choose -log(eps) so that the reference's
@@ -798,10 +803,9 @@ bool encode_grid_maps(pt_radon *h)
     const cuuint32_t tr = (cuuint32_t)(GTILE + 2 * h->M), tp = (cuuint32_t)((GTILE - 2) / 2 + (2 * h->M + 3) / 2);
     const cuuint32_t box[3] = {(cuuint32_t)ZC * 4, tp, tr};
     const cuuint32_t estr[3] = {1, 1, 1};
-    float2 *bufs[2] = {h->fgrid, h->fgrid2};
-    for (int b = 0; b < 2; ++b) {
-        if (((uintptr_t)bufs[b] & 127) != 0) return false;
-        if (encode(&h->tmap[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, bufs[b], dims, strides, box, estr,
+    for (int b = 0; b < RSETS; ++b) {
+        if (((uintptr_t)h->fgrid[b] & 127) != 0) return false;
+        if (encode(&h->tmap[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, h->fgrid[b], dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return false;
@@ -847,19 +851,22 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
     const float a = (float)(PI_REF * PI_REF / h->mu);
     const float pre = (float)(PI_REF / std::fabs(h->mu)) / (float)N;
     const int nchunks = (h->nz + ZC - 1) / ZC;
-    const bool two = nchunks > 1 && h->streams == 2;
-    if (two) {   // fork: the side stream starts after everything queued on st so far
+    // buffer sets in use: at most `streams`, the chunk count, and the number
+    // of ZC-slice line blocks the lines buffer holds (nzp / ZC)
+    const int sets = std::max(1, std::min(std::min(h->streams, nchunks), h->nzp / ZC));
+    if (sets > 1) {   // fork: the side streams start after everything queued on st so far
         PT_CUDA(cudaEventRecord(h->ev_fork, st));
-        PT_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+        for (int k = 1; k < sets; ++k) PT_CUDA(cudaStreamWaitEvent(h->side[k - 1], h->ev_fork, 0));
     }
     for (int c = 0; c < nchunks; ++c) {
         const int z0 = c * ZC;
-        // chunk buffers: set c % 2 on stream c % 2 (a set is reused only by its
-        // own stream, in order); gathered lines at offset (c % 2) of the lines buffer
-        const bool odd = two && (c & 1);
-        cudaStream_t s = odd ? h->side : st;
-        float2 *rb = odd ? h->rbuf2 : h->rbuf, *fg = odd ? h->fgrid2 : h->fgrid;
-        float2 *ln = h->lines + (odd ? (size_t)h->ntheta * N * ZC : 0);
+        // chunk buffers: set c % sets on stream c % sets (a set is reused only
+        // by its own stream, in order); gathered lines at block (c % sets) of
+        // the lines buffer
+        const int k = c % sets;
+        cudaStream_t s = k ? h->side[k - 1] : st;
+        float2 *rb = h->rbuf[k], *fg = h->fgrid[k];
+        float2 *ln = h->lines + (size_t)k * h->ntheta * N * ZC;
         k_fwd_rows<G><<<N, ZC * T, s1, s>>>(f, rb, h->nz, z0, h->deap, h->tw_G);
         PT_LAUNCHED("k_fwd_rows");
         k_fwd_cols<G><<<G / CK, CK * ZC * T, s2, s>>>(rb, fg, h->tw_G);
@@ -867,7 +874,7 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
         const int npts = h->ntheta * N;
         if (h->gather == 2) {
             k_fwd_gather_tma<N, M><<<h->nchunks, GPB * ZC, tma_smem<M>(), s>>>(
-                h->tmap[odd ? 1 : 0], ln, h->x, h->y, a, pre, h->ptab, h->chunks, h->tma_err);
+                h->tmap[k], ln, h->x, h->y, a, pre, h->ptab, h->chunks, h->tma_err);
             PT_LAUNCHED("k_fwd_gather_tma");
         } else if (h->gather == 1) {
             k_fwd_gather_tile<N, M><<<h->nchunks, GPB * ZC, tile_smem<M>(), s>>>(fg, ln, h->x, h->y, a, pre, h->ptab,
@@ -881,9 +888,9 @@ int run_fwd(pt_radon *h, float2 *g, const float2 *f, float scale, cudaStream_t s
         k_fwd_lines<N><<<h->ntheta, ZC * 32, s3, s>>>(ln, g, h->nz, z0, scale, h->tw_N);
         PT_LAUNCHED("k_fwd_lines");
     }
-    if (two) {   // join: st continues after the side stream's chunks
-        PT_CUDA(cudaEventRecord(h->ev_join, h->side));
-        PT_CUDA(cudaStreamWaitEvent(st, h->ev_join, 0));
+    for (int k = 1; k < sets; ++k) {   // join: st continues after every side stream's chunks
+        PT_CUDA(cudaEventRecord(h->ev_join[k - 1], h->side[k - 1]));
+        PT_CUDA(cudaStreamWaitEvent(st, h->ev_join[k - 1], 0));
     }
     return PT_OK;
 }
@@ -1056,20 +1063,20 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     if (rc == PT_OK) rc = dmalloc(&h->fxy, 2 * ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->perm, ntheta * N);
     if (rc == PT_OK) rc = dmalloc(&h->ptab, ntheta * N);
-    if (rc == PT_OK) rc = dmalloc(&h->rbuf, N * G * ZC);
-    if (rc == PT_OK) rc = dmalloc(&h->rbuf2, N * G * ZC);
+    for (int k = 0; k < RSETS && rc == PT_OK; ++k) {
+        rc = dmalloc(&h->rbuf[k], N * G * ZC);
+        if (rc == PT_OK) rc = dmalloc(&h->fgrid[k], (size_t)(G + GH_ROWS) * (G + 2 * GH_PAIRS) * ZC);
+    }
     if (rc == PT_OK) rc = dmalloc(&h->deap, (size_t)N * N);
-    if (rc == PT_OK) rc = dmalloc(&h->fgrid, (size_t)(G + GH_ROWS) * (G + 2 * GH_PAIRS) * ZC);
-    if (rc == PT_OK) rc = dmalloc(&h->fgrid2, (size_t)(G + GH_ROWS) * (G + 2 * GH_PAIRS) * ZC);
     if (rc == PT_OK && cudaMalloc((void **)&h->tma_err, sizeof(int)) == cudaSuccess &&
         cudaMemset(h->tma_err, 0, sizeof(int)) == cudaSuccess)
-        h->tma_ok = encode_grid_maps(h);   // gather 2 is offered only if both maps encode
-    if (rc == PT_OK && (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
-                        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-                        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess)) {
-        pt::set_error("radonusfft: stream/event creation failed");
-        rc = PT_ERR_CUDA;
-    }
+        h->tma_ok = encode_grid_maps(h);   // gather 2 is offered only if every map encodes
+    if (rc == PT_OK && cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess) rc = PT_ERR_CUDA;
+    for (int k = 0; k < RSETS - 1 && rc == PT_OK; ++k)
+        if (cudaStreamCreateWithFlags(&h->side[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_join[k], cudaEventDisableTiming) != cudaSuccess)
+            rc = PT_ERR_CUDA;
+    if (rc == PT_ERR_CUDA) pt::set_error("radonusfft: stream/event creation failed");
     h->nzp = (int)((nz + ZQ - 1) / ZQ * ZQ);
     const size_t nzp = h->nzp;
     if (rc == PT_OK) rc = dmalloc(&h->lines, ntheta * N * nzp);
@@ -1314,11 +1321,11 @@ extern "C" int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials
     PT_CUDA(cudaEventCreate(&e1));
     float best = 1e30f;
     int best_s = h->streams, best_g = h->gather, rc = PT_OK;
-    const int ncombo = h->tma_ok ? 6 : 4;   // streams {1, 2} x gather {L1, tiles, TMA tiles}
-    for (int combo = 0; combo < ncombo && rc == PT_OK; ++combo) {
-        const int sc = 1 + (combo & 1);
+    const int ngather = h->tma_ok ? 3 : 2;   // streams {1, 2, 4} x gather {L1, tiles, TMA tiles}
+    for (int combo = 0; combo < 3 * ngather && rc == PT_OK; ++combo) {
+        const int sc = 1 << (combo % 3);
         h->streams = sc;
-        h->gather = combo >> 1;
+        h->gather = combo / 3;
         std::vector<float> ts;
         for (int k = 0; k <= trials && rc == PT_OK; ++k) {
             cudaEventRecord(e0, st);
@@ -1342,7 +1349,7 @@ extern "C" int pt_radon_autotune(pt_radon *h, void *g, const void *f, int trials
     cudaEventDestroy(e1);
     h->streams = best_s;
     h->gather = best_g;
-    if (streams_out) *streams_out = best_s + 2 * best_g;
+    if (streams_out) *streams_out = best_s + 8 * best_g;
     if (rc == PT_OK && h->tma_ok) {   // a TMA tile load that never completed
         int flag = 0;
         PT_CUDA(cudaMemcpy(&flag, h->tma_err, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1403,8 +1410,8 @@ int pt::radon_dims(const pt_radon *h, int *nz, int *ntheta)
 extern "C" int pt_radon_set_variant(pt_radon *h, int streams, int gather)
 {
     pt::clear_error();
-    PT_CHECK_ARG(h && (streams == 1 || streams == 2) && (gather >= 0 && gather <= 2),
-                 "radonusfft.set_variant: streams 1 or 2, gather 0 (L1), 1 (tiles) or 2 (TMA tiles)");
+    PT_CHECK_ARG(h && (streams == 1 || streams == 2 || streams == 4) && (gather >= 0 && gather <= 2),
+                 "radonusfft.set_variant: streams 1, 2 or 4, gather 0 (L1), 1 (tiles) or 2 (TMA tiles)");
     if (gather == 2 && !h->tma_ok) {
         pt::set_error("radonusfft.set_variant: the TMA gather is not available (tensor map encoding failed)");
         return PT_ERR_UNSUPPORTED;

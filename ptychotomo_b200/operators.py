@@ -56,15 +56,15 @@ class radonusfft:  # noqa: N801 - reference class name
               "radonusfft.adj_exact")
 
     def autotune(self, g, f, trials=3, stream=None):
-        """Time the forward on one stream and pipelined on two, each with the
-        gather through L1, from shared-memory tiles and from TMA-staged
-        tiles; keep the fastest for this operator.  g, f: buffers of fwd's
-        shapes (g is overwritten).  Returns (streams, gather), gather 0 (L1),
-        1 (tiles) or 2 (TMA tiles)."""
+        """Time the forward with its slice chunks on one stream and pipelined
+        on two and on four, each with the gather through L1, from
+        shared-memory tiles and from TMA-staged tiles; keep the fastest for
+        this operator.  g, f: buffers of fwd's shapes (g is overwritten).
+        Returns (streams, gather), gather 0 (L1), 1 (tiles) or 2 (TMA tiles)."""
         out = ctypes.c_int()
         check(lib().pt_radon_autotune(self._h, as_ptr(g), as_ptr(f), int(trials), ctypes.byref(out), _s(stream)),
               "radonusfft.autotune")
-        return (out.value - 1) % 2 + 1, (out.value - 1) // 2
+        return out.value % 8, out.value // 8
 
     def set_variant(self, streams=2, gather=0):
         """The forward's variant without timing (results are identical):

@@ -1,7 +1,7 @@
 """The autotuners: ptychofft.autotune picks the adjoint's angle split and
 radonusfft.autotune the forward's stream count and gather variant by timing;
 every choice keeps the operators' results (against the oracle, rel-L2 <=
-1e-5), and the six radon forward variants (one or two streams; gather
+1e-5), and the nine radon forward variants (one, two or four streams; gather
 through L1, from shared-memory tiles copied by the threads, or from tiles
 loaded by the TMA) give bit-identical projections."""
 import numpy as np
@@ -58,14 +58,14 @@ def test_radon_autotune_keeps_the_forward():
     op.fwd(before, f)
     timeouts, tma = op.status()
     assert tma and timeouts == 0
-    for streams in (1, 2):
+    for streams in (1, 2, 4):
         for gather in (0, 1, 2):
             op.set_variant(streams, gather)
             op.fwd(g, f)
             assert torch.equal(g, before), (streams, gather)
     assert op.status() == (0, True)
     streams, gather = op.autotune(g, f, trials=2)
-    assert streams in (1, 2) and gather in (0, 1, 2)
+    assert streams in (1, 2, 4) and gather in (0, 1, 2)
     op.fwd(g, f)
     assert torch.equal(g, before)
     x = torch.empty((nt, op.N), dtype=torch.float32, device="cuda")
@@ -98,3 +98,6 @@ def test_tiled_gathers_are_bit_identical(n, nz, nt, m):
     op.fwd(c, f)
     assert op.status() == (0, True)
     assert torch.equal(a, b) and torch.equal(a, c)
+    op.set_variant(4, 2)
+    op.fwd(c, f)
+    assert torch.equal(a, c)
