@@ -716,7 +716,7 @@ struct pt_radon {
     float4 *ptab = nullptr;   // (x, y, point index as bits, 0) of each point in that order
     int4 *chunks = nullptr;   // the tiled gather's blocks: (tile row, tile column, first, count)
     int nchunks = 0, chunks_cap = 0;
-    int gather = 0;           // 0: gather through L1 (k_fwd_gather_pts), 1: shared-memory tiles, 2: TMA-staged tiles
+    int gather = 2;           // 0: gather through L1 (k_fwd_gather_pts), 1: shared-memory tiles, 2: TMA-staged tiles
     // gather 2: one 3-D tensor map per grid buffer set, and a device flag the
     // TMA kernel sets if a tile load did not complete
     CUtensorMap tmap[RSETS];
@@ -728,7 +728,7 @@ struct pt_radon {
     // chunks are in flight and one chunk's FFTs overlap another's gather
     // (fork/join by events)
     float2 *rbuf[RSETS] = {}, *fgrid[RSETS] = {};
-    int streams = 2;   // 1, 2 or 4 (pt_radon_autotune chooses)
+    int streams = 4;   // 1, 2 or 4 (pt_radon_autotune chooses)
     cudaStream_t side[RSETS - 1] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[RSETS - 1] = {};
     // adjoint (all slices, slice-minor with nzp lanes)
@@ -1071,6 +1071,10 @@ extern "C" int pt_radon_create_ex(size_t ntheta, size_t nz, size_t n, int m_over
     if (rc == PT_OK && cudaMalloc((void **)&h->tma_err, sizeof(int)) == cudaSuccess &&
         cudaMemset(h->tma_err, 0, sizeof(int)) == cudaSuccess)
         h->tma_ok = encode_grid_maps(h);   // gather 2 is offered only if every map encodes
+    // default variant (the autotuner's usual choice from 128^3 up, within a
+    // few percent at 64^3): four chunk pipelines, TMA-staged tiles
+    h->streams = 4;
+    h->gather = h->tma_ok ? 2 : 1;
     if (rc == PT_OK && cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess) rc = PT_ERR_CUDA;
     for (int k = 0; k < RSETS - 1 && rc == PT_OK; ++k)
         if (cudaStreamCreateWithFlags(&h->side[k], cudaStreamNonBlocking) != cudaSuccess ||
