@@ -24,6 +24,7 @@ Pass-model algorithmic bytes per call (complex64 = 8 B):
     python bench.py --precond     # learned preconditioner of the tomography CG (360 angles, missing wedge)
     python bench.py --time-to-target   # time to the plain ADMM's reconstruction: plain vs graph-captured variants
     python bench.py --pcie        # pinned host<->device copy rates (the bound of the e2e leg)
+    python bench.py --radon-variants   # radon forward time by chunk pipeline count and gather
 
 ``--impl reference`` times the reference's operators: by default the CPU
 restatement of the reference (oracle/, all host cores, a bounded sample of
@@ -1345,6 +1346,42 @@ def run_time_to_target(args, local):
             "speedup_to_within_floor": f_ratios}
 
 
+def run_radon_variants(args, local):
+    """The radon forward alone (10 calls after 3 warm-ups, CUDA events) for
+    every chunk pipeline count and gather at 64^3 / 96, 128^3 / 192 and
+    256^3 / 384 angles: the table the autotuner chooses from."""
+    import torch
+    from ptychotomo_b200 import radonusfft
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    out = {}
+    for n, nt in ((64, 96), (128, 192), (256, 384)):
+        theta = np.linspace(0, np.pi, nt, endpoint=False).astype(np.float32)
+        op = radonusfft(nt, n, n)
+        op.setobj(torch.from_numpy(theta).to(dev))
+        f = torch.randn((n, n, n), dtype=torch.complex64, device=dev)
+        g = torch.empty((nt, n, n), dtype=torch.complex64, device=dev)
+        row = {}
+        for st in (1, 2, 4):
+            for ga in (0, 1, 2):
+                op.set_variant(st, ga)
+                for _ in range(3):
+                    op.fwd(g, f)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                for _ in range(10):
+                    op.fwd(g, f)
+                e1.record()
+                torch.cuda.synchronize()
+                row["streams %d, %s" % (st, GATHER_NAMES[ga])] = round(e0.elapsed_time(e1) / 10, 4)
+        out["n%d_%dangles" % (n, nt)] = row
+        del op, f, g
+    return {"metric": "radonusfft forward ms by variant", "unit": "ms", "n_gpus": 1, "higher_is_better": False,
+            "data": "synthetic", "config": {"workload": "n = nz in {64, 128, 256}, 3n/2 angles, M = 7"},
+            "variants": out}
+
+
 def run_pcie(args, local):
     """Host<->device copy rates with pinned buffers (the e2e leg's bound):
     8 GiB each way alone, then both directions at once on two streams."""
@@ -1414,6 +1451,7 @@ def main():
     ap.add_argument("--precond", action="store_true", help="learned preconditioner of the tomography CG")
     ap.add_argument("--time-to-target", action="store_true", help="time to the plain ADMM's reconstruction")
     ap.add_argument("--pcie", action="store_true", help="pinned host<->device copy rates (the e2e bound)")
+    ap.add_argument("--radon-variants", action="store_true", help="radon forward time by pipeline count and gather")
     ap.add_argument("--ttt-iters", type=int, default=None)
     ap.add_argument("--ttt-size", type=int, default=None)
     ap.add_argument("--ttt-alpha", type=float, default=None)
@@ -1436,11 +1474,12 @@ def main():
             print(json.dumps(line), flush=True)
         return 0
     if (args.admm or args.cg_kernels or args.precision or args.uneven or args.precond or args.time_to_target
-            or args.pcie):
+            or args.pcie or args.radon_variants):
         if rank == 0:
             fn = (run_admm if args.admm else run_cg_kernels if args.cg_kernels else
                   run_precision if args.precision else run_precond if args.precond else
-                  run_time_to_target if args.time_to_target else run_pcie if args.pcie else run_uneven)
+                  run_time_to_target if args.time_to_target else run_pcie if args.pcie else
+                  run_radon_variants if args.radon_variants else run_uneven)
             print(json.dumps(fn(args, local)), flush=True)
         return 0
     if args.impl == "reference":
