@@ -200,6 +200,61 @@ __device__ __forceinline__ void fft(float2 *buf, int es, int t, const float2 *__
     }
 }
 
+// The same transform for NQ interleaved sequences: element i of sequence q
+// at buf[i * NQ + q] (one row of NQ values per index).  Thread (q, b) of the
+// block, q = t % NQ, b = t / NQ, runs butterflies b, b + TB, ... of sequence
+// q, so a warp reads and writes rows of consecutive values (no bank
+// conflicts) and the lanes of one row share their twiddle (one broadcast
+// load).  Same butterflies, twiddles and order as pass/fft: bit-identical
+// results.
+template <int L, int R, int NS, int DIR, int TB, int NQ>
+__device__ __forceinline__ void pass_iq(float2 *buf, int q, int b, const float2 *__restrict__ tw)
+{
+    constexpr int NB = L / R;
+    constexpr int PER = (NB + TB - 1) / TB;
+    float2 v[PER][R];
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int j = b + p * TB;
+        if ((NB % TB == 0) || j < NB) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[p][r] = buf[(j + r * NB) * NQ + q];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int j = b + p * TB;
+        if ((NB % TB == 0) || j < NB) {
+            const int k = j % NS;
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    float2 w = __ldg(&tw[r * k * (L / (NS * R))]);
+                    if (DIR > 0) w.y = -w.y;
+                    v[p][r] = cmul(v[p][r], w);
+                }
+            }
+            Dft<R, DIR>::run(v[p]);
+            const int base = (j / NS) * NS * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[(base + r * NS) * NQ + q] = v[p][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <int L, int DIR, int TB, int NQ, int I = 0, int NS = 1>
+__device__ __forceinline__ void fft_iq(float2 *buf, int q, int b, const float2 *__restrict__ tw)
+{
+    static_assert(supported_len(L), "FFT length must be 2^a 3^b");
+    if constexpr (I < num_passes(L)) {
+        constexpr int R = radix_at(L, I);
+        pass_iq<L, R, NS, DIR, TB, NQ>(buf, q, b, tw);
+        fft_iq<L, DIR, TB, NQ, I + 1, NS * R>(buf, q, b, tw);
+    }
+}
+
 }  // namespace ptfft
 
 // Host helper: fill tw[m] = exp(-2 pi i m / L), m < L (double precision).

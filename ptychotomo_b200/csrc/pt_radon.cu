@@ -138,24 +138,29 @@ constexpr int GH_ROWS = 14;   // 2M for the largest compiled M (7)
 constexpr int GH_PAIRS = 8;   // (2M + 2) / 2 column pairs for M = 7
 
 // ---- K2: column FFT of the 2N grid, centring sign folded in ----------------
+// The block's CK columns x ZC slices are NF interleaved transforms: shared
+// row i holds element i of all NF (column c, slice z at c * ZC + z), so the
+// input rows (one 128-byte line of the row-FFT buffer per y) and the output
+// rows (one 128-byte line of the grid per ky) are straight copies, and the
+// passes (ptfft::fft_iq) are free of bank conflicts.
 template <int G>
 __global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
     k_fwd_cols(const float2 *__restrict__ rbuf, float2 *__restrict__ fg, const float2 *__restrict__ tw)
 {
-    constexpr int T = fft_threads<G>(), N = G / 2, PITCH = G + 1, NF = CK * ZC;
+    constexpr int T = fft_threads<G>(), N = G / 2, NF = CK * ZC;
     extern __shared__ float2 sm[];
     const int kx0 = blockIdx.x * CK;
-    const int f = threadIdx.x / T, t = threadIdx.x % T;
+    const int q = threadIdx.x % NF, b = threadIdx.x / NF;
     for (int e = threadIdx.x; e < N * NF; e += blockDim.x) {
-        const int y = e / NF, q = e % NF;
-        sm[q * PITCH + N / 2 + y] = rbuf[((size_t)y * G + kx0) * ZC + q];
+        const int y = e / NF, r = e % NF;
+        sm[(N / 2 + y) * NF + r] = rbuf[((size_t)y * G + kx0) * ZC + r];
     }
     for (int e = threadIdx.x; e < N * NF; e += blockDim.x) {
-        const int q = e / N, i = e % N;
-        sm[q * PITCH + (i < N / 2 ? i : i + N)] = czero();
+        const int i = e / NF, r = e % NF;
+        sm[(i < N / 2 ? i : i + N) * NF + r] = czero();
     }
     __syncthreads();
-    ptfft::fft<G, -1, T>(sm + f * PITCH, 1, t, tw);
+    ptfft::fft_iq<G, -1, T, NF>(sm, q, b, tw);
     // column-pair layout [ky][kx/2][z][kx&1]: one 128-byte line per (ky, pair),
     // plus the halo copies (rows < GH_ROWS again at G + ky, pairs < GH_PAIRS
     // again at G/2 + pair)
@@ -167,7 +172,7 @@ __global__ void __launch_bounds__(CK *ZC *fft_threads<G>())
         const int ky = kyh < G ? kyh : kyh - G;
         const int z = r >> 1, c = r & 1;
         const int kx = kx0 + c;
-        float2 v = sm[(c * ZC + z) * PITCH + ky];
+        float2 v = sm[ky * NF + c * ZC + z];
         if ((kx + ky) & 1) v = -1.f * v;
         fg[((size_t)kyh * PS + pr) * (2 * ZC) + r] = v;
         if (pr < GH_PAIRS) fg[((size_t)kyh * PS + G / 2 + pr) * (2 * ZC) + r] = v;
