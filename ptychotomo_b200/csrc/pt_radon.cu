@@ -102,16 +102,18 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
     k_fwd_rows(const float2 *__restrict__ u, float2 *__restrict__ rbuf, int nz, int z0,
                const float *__restrict__ fac, const float2 *__restrict__ tw)
 {
-    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, PITCH = G + 1;
+    // the block's ZC slices are interleaved transforms: shared row X holds
+    // element X of every slice (ptfft::fft_iq), so the output is a straight
+    // copy into the slice-minor row buffer
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3;
     constexpr int c0 = N / 6, c1 = 5 * N / 6 - 1;
     extern __shared__ float2 sm[];
     const int y = blockIdx.x;
-    const int f = threadIdx.x / T, t = threadIdx.x % T;
-    const int z = z0 + f;
+    const int q = threadIdx.x % ZC, b = threadIdx.x / ZC;
+    const int z = z0 + q;
     const int sr = min(max(y, c0), c1) - c0;
     const int Y = y + N / 2;
-    float2 *b = sm + f * PITCH;
-    for (int X = t; X < G; X += T) {
+    for (int X = b; X < G; X += T) {
         float2 v = czero();
         const int tx = X - N / 2;
         if (tx >= 0 && tx < N && z < nz) {
@@ -119,14 +121,12 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
             v = __ldg(&fac[(size_t)y * N + tx]) * u[((size_t)z * n + sr) * n + sc];
             if ((X + Y) & 1) v = -1.f * v;
         }
-        b[X] = v;
+        sm[X * ZC + q] = v;
     }
     __syncthreads();
-    ptfft::fft<G, -1, T>(b, 1, t, tw);
-    for (int e = threadIdx.x; e < G * ZC; e += blockDim.x) {
-        const int kx = e / ZC, q = e % ZC;
-        rbuf[((size_t)y * G + kx) * ZC + q] = sm[q * PITCH + kx];
-    }
+    ptfft::fft_iq<G, -1, T, ZC>(sm, q, b, tw);
+    float2 *dst = rbuf + (size_t)y * G * ZC;
+    for (int e = threadIdx.x; e < G * ZC; e += blockDim.x) dst[e] = sm[e];
 }
 
 // The forward's Fourier grid carries a halo, like the reference's (G+2M)^2
@@ -427,22 +427,19 @@ __global__ void __launch_bounds__(ZC * 32)
     k_fwd_lines(const float2 *__restrict__ lines, float2 *__restrict__ out, int nz, int z0, float scale,
                 const float2 *__restrict__ tw)
 {
-    constexpr int n = 2 * N / 3, c0 = N / 6, PITCH = N + 1, T = 32;
+    constexpr int n = 2 * N / 3, c0 = N / 6, T = 32;
     extern __shared__ float2 sm[];
     const int th = blockIdx.x;
-    for (int e = threadIdx.x; e < N * ZC; e += blockDim.x) {
-        const int k = e / ZC, q = e % ZC;
-        sm[q * PITCH + k] = lines[((size_t)th * N + k) * ZC + q];
-    }
+    const float2 *src = lines + (size_t)th * N * ZC;   // [k][slice]: the interleaved layout already
+    for (int e = threadIdx.x; e < N * ZC; e += blockDim.x) sm[e] = src[e];
     __syncthreads();
-    const int f = threadIdx.x / T, t = threadIdx.x % T;
-    ptfft::fft<N, +1, T>(sm + f * PITCH, 1, t, tw);
+    ptfft::fft_iq<N, +1, T, ZC>(sm, threadIdx.x % ZC, threadIdx.x / ZC, tw);
     for (int e = threadIdx.x; e < ZC * n; e += blockDim.x) {
-        const int q = e / n, j = e % n;
+        const int q = e % ZC, j = e / ZC;
         const int z = z0 + q;
         if (z < nz) {
             const int k = c0 + j;
-            out[((size_t)th * nz + z) * n + j] = ((k & 1) ? scale : -scale) * sm[q * PITCH + k];
+            out[((size_t)th * nz + z) * n + j] = ((k & 1) ? scale : -scale) * sm[k * ZC + q];
         }
     }
 }
@@ -456,25 +453,24 @@ __global__ void __launch_bounds__(ZC * 32)
     k_adj_lines(const float2 *__restrict__ g, float2 *__restrict__ lines, int nz, int nzp, float pre,
                 const float2 *__restrict__ tw)
 {
-    constexpr int n = 2 * N / 3, c0 = N / 6, c1 = 5 * N / 6 - 1, PITCH = N + 1, T = 32;
+    constexpr int n = 2 * N / 3, c0 = N / 6, c1 = 5 * N / 6 - 1, T = 32;
     extern __shared__ float2 sm[];
     const int th = blockIdx.x, z0 = blockIdx.y * ZC;
-    const int f = threadIdx.x / T, t = threadIdx.x % T;
-    const int z = z0 + f;
-    float2 *b = sm + f * PITCH;
-    for (int k = t; k < N; k += T) {
+    const int q = threadIdx.x % ZC, b = threadIdx.x / ZC;
+    const int z = z0 + q;
+    for (int k = b; k < N; k += T) {
         float2 v = czero();
         if (z < nz) {
             if (!ZP) v = g[((size_t)th * nz + z) * n + (min(max(k, c0), c1) - c0)];
             else if (k >= c0 && k <= c1) v = g[((size_t)th * nz + z) * n + (k - c0)];
         }
-        b[k] = (k & 1) ? v : -1.f * v;
+        sm[k * ZC + q] = (k & 1) ? v : -1.f * v;
     }
     __syncthreads();
-    ptfft::fft<N, -1, T>(b, 1, t, tw);
+    ptfft::fft_iq<N, -1, T, ZC>(sm, q, b, tw);
     for (int e = threadIdx.x; e < N * ZC; e += blockDim.x) {
-        const int k = e / ZC, q = e % ZC;
-        lines[((size_t)th * N + k) * nzp + z0 + q] = ((k & 1) ? pre : -pre) * sm[q * PITCH + k];
+        const int k = e / ZC, qq = e % ZC;
+        lines[((size_t)th * N + k) * nzp + z0 + qq] = ((k & 1) ? pre : -pre) * sm[e];
     }
 }
 
@@ -495,7 +491,7 @@ __global__ void __launch_bounds__(ZQ *fft_threads<G>(), (G >= 1024 ? 1 : 2))
                     const int *__restrict__ gpt, const float4 *__restrict__ gw, const int *__restrict__ col_order,
                     int nzp, const float2 *__restrict__ tw)
 {
-    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, PITCH = G + 1, NG4 = G / CG;
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, NG4 = G / CG;
     constexpr int Y0 = N / 2 + N / 6;
     constexpr int U = 4;  // entries in flight per lane
     extern __shared__ float2 sm[];
@@ -565,18 +561,18 @@ __global__ void __launch_bounds__(ZQ *fft_threads<G>(), (G >= 1024 ? 1 : 2))
             for (int c = 0; c < CG; ++c) {
                 const int ky = gi * CG + c;
                 const float sg = ((kx + ky) & 1) ? -1.f : 1.f;  // fftshiftc
-                sm[(2 * zl) * PITCH + ky] = make_float2(sg * acc[c].x, sg * acc[c].y);
-                sm[(2 * zl + 1) * PITCH + ky] = make_float2(sg * acc[c].z, sg * acc[c].w);
+                sm[ky * ZQ + 2 * zl] = make_float2(sg * acc[c].x, sg * acc[c].y);
+                sm[ky * ZQ + 2 * zl + 1] = make_float2(sg * acc[c].z, sg * acc[c].w);
             }
         }
     }
     __syncthreads();
-    const int f = threadIdx.x / T, t = threadIdx.x % T;
-    ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
+    // the 16 slices' column transforms interleaved (shared row ky = element ky of each)
+    ptfft::fft_iq<G, +1, T, ZQ>(sm, threadIdx.x % ZQ, threadIdx.x / ZQ, tw);
     constexpr int ROWS = ALL ? N : n, YB = ALL ? N / 2 : Y0;
     for (int e = threadIdx.x; e < ROWS * ZQ; e += blockDim.x) {
         const int r = e / ZQ, q = e % ZQ;
-        rbuf[((size_t)r * G + kx) * nzp + z0 + q] = sm[q * PITCH + YB + r];
+        rbuf[((size_t)r * G + kx) * nzp + z0 + q] = sm[(YB + r) * ZQ + q];
     }
 }
 
@@ -617,23 +613,22 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
     k_adj_rows(const float2 *__restrict__ rbuf, float2 *__restrict__ out, int nz, int nzp,
                const float *__restrict__ fac, float scale, const float2 *__restrict__ tw)
 {
-    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, c0 = N / 6, PITCH = G + 1;
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, c0 = N / 6;
     extern __shared__ float2 sm[];
     const int r = blockIdx.x, z0 = blockIdx.y * ZC;
-    const int f = threadIdx.x / T, t = threadIdx.x % T;
     for (int e = threadIdx.x; e < G * ZC; e += blockDim.x) {
         const int kx = e / ZC, q = e % ZC;
-        sm[q * PITCH + kx] = rbuf[((size_t)r * G + kx) * nzp + z0 + q];
+        sm[e] = rbuf[((size_t)r * G + kx) * nzp + z0 + q];
     }
     __syncthreads();
-    ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
+    ptfft::fft_iq<G, +1, T, ZC>(sm, threadIdx.x % ZC, threadIdx.x / ZC, tw);
     for (int e = threadIdx.x; e < ZC * n; e += blockDim.x) {
-        const int q = e / n, c = e % n;
+        const int q = e % ZC, c = e / ZC;
         const int z = z0 + q;
         if (z < nz) {
             const int tx = c0 + c, ty = c0 + r;
             const int X = N / 2 + tx, Y = N / 2 + ty;
-            float2 v = sm[q * PITCH + X];
+            float2 v = sm[X * ZC + q];
             if ((X + Y) & 1) v = -1.f * v;
             out[((size_t)z * n + r) * n + c] = scale * (__ldg(&fac[(size_t)ty * N + tx]) * v);
         }
@@ -655,20 +650,19 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
     k_adj_rows_exact(const float2 *__restrict__ rbuf, float2 *__restrict__ out, float2 *__restrict__ mbuf, int nz,
                      int nzp, const float *__restrict__ fac, float scale, const float2 *__restrict__ tw)
 {
-    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, c0 = N / 6, PITCH = G + 1;
+    constexpr int T = fft_threads<G>(), N = G / 2, n = G / 3, c0 = N / 6;
     extern __shared__ float2 sm[];
     const int ty = blockIdx.x, z0 = blockIdx.y * ZC;
-    const int f = threadIdx.x / T, t = threadIdx.x % T;
     for (int e = threadIdx.x; e < G * ZC; e += blockDim.x) {
         const int kx = e / ZC, q = e % ZC;
-        sm[q * PITCH + kx] = rbuf[((size_t)ty * G + kx) * nzp + z0 + q];
+        sm[e] = rbuf[((size_t)ty * G + kx) * nzp + z0 + q];
     }
     __syncthreads();
-    ptfft::fft<G, +1, T>(sm + f * PITCH, 1, t, tw);
+    ptfft::fft_iq<G, +1, T, ZC>(sm, threadIdx.x % ZC, threadIdx.x / ZC, tw);
     const int Y = N / 2 + ty;
     const float *facr = fac + (size_t)ty * N;
     for (int e = threadIdx.x; e < ZC * n; e += blockDim.x) {
-        const int q = e / n, c = e % n;
+        const int q = e % ZC, c = e / ZC;
         const int z = z0 + q;
         if (z >= nz) continue;
         // columns tx of the padded row that copy pixel c (fixed order)
@@ -676,7 +670,7 @@ __global__ void __launch_bounds__(ZC *fft_threads<G>())
         float2 acc = czero();
         for (int tx = lo; tx <= hi; ++tx) {
             const int X = N / 2 + tx;
-            float2 v = sm[q * PITCH + X];
+            float2 v = sm[X * ZC + q];
             if ((X + Y) & 1) v = -1.f * v;
             acc = acc + __ldg(&facr[tx]) * v;
         }
