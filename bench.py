@@ -1248,6 +1248,7 @@ def run_time_to_target(args, local):
         g.capture()            # set-up, counted in the wall time
         torch.cuda.synchronize()
         t = time.perf_counter() - t0
+        graphed_run.capture_s = t
         us, ts = [], []
         for m in range(c["iters"]):
             torch.cuda.synchronize()
@@ -1306,7 +1307,9 @@ def run_time_to_target(args, local):
     out["plain"] = dict(reach(us_p, ts_p), ms_per_iteration_steady=round(1e3 * (ts_p[-1] - ts_p[2]) / max(len(ts_p) - 3, 1), 2))
     del us_p
     us_g, ts_g = graphed_run(None)
-    out["graphed"] = dict(reach(us_g, ts_g), ms_per_iteration_steady=round(1e3 * (ts_g[-1] - ts_g[2]) / max(len(ts_g) - 3, 1), 2))
+    out["graphed"] = dict(reach(us_g, ts_g), ms_per_iteration_steady=round(1e3 * (ts_g[-1] - ts_g[2]) / max(len(ts_g) - 3, 1), 2),
+                          capture_s=round(graphed_run.capture_s, 3),
+                          first_iterations_s=[round(v, 3) for v in ts_g[:4]])
     del us_g
     torch.cuda.empty_cache()
     if not args.ttt_no_precond:
