@@ -518,10 +518,12 @@ __global__ void __launch_bounds__(512, 1)
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             line_dft128<-1, true>(v[c], t, c ? sb : sa, twf);
+            // streaming stores: the frames are not read again by this kernel
+            // (3.95 against 3.97 ms at 256^3)
             float4 *row = reinterpret_cast<float4 *>(out + (2 * grp + c) * 128);
 #pragma unroll
             for (int k2 = 0; k2 < 8; ++k2)   // ky = 2t + 16 k2, +1
-                row[t + 8 * k2] = make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y);
+                __stcs(&row[t + 8 * k2], make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y));
         }
         __syncthreads();
     }
