@@ -149,6 +149,60 @@ struct Dft<16, DIR> {
     }
 };
 
+// cos(j pi / 16) for j = 0..8
+__host__ __device__ constexpr float cos_pi16(int j)
+{
+    return j == 0   ? 1.0f
+           : j == 1 ? 0.98078528040323044913f
+           : j == 2 ? 0.92387953251128675613f
+           : j == 3 ? 0.83146961230254523708f
+           : j == 4 ? 0.70710678118654752440f
+           : j == 5 ? 0.55557023301960222474f
+           : j == 6 ? 0.38268343236508977173f
+           : j == 7 ? 0.19509032201612826785f
+                    : 0.0f;
+}
+
+// z * W32^j, W32 = exp(DIR 2 pi i / 32), for a compile-time 0 <= j < 24
+template <int DIR>
+__device__ __forceinline__ float2 mul_w32(float2 z, int j)
+{
+    if (j == 0) return z;
+    if (j == 8) return mul_i<DIR>(z);
+    if (j == 16) return make_float2(-z.x, -z.y);
+    // angle j pi / 16 by quadrant: (cos, sin)
+    const float c = j < 8 ? cos_pi16(j) : j < 16 ? -cos_pi16(16 - j) : -cos_pi16(j - 16);
+    const float s = j < 8 ? cos_pi16(8 - j) : j < 16 ? cos_pi16(j - 8) : -cos_pi16(24 - j);
+    return cmul(z, make_float2(c, DIR * s));
+}
+
+// 32-point DFT as 4 x 8 (n = 4 n1 + n2, k = k1 + 8 k2), natural-order output.
+template <int DIR>
+struct Dft<32, DIR> {
+    static __device__ __forceinline__ void run(float2 *v)
+    {
+        float2 a[4][8];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+#pragma unroll
+            for (int n1 = 0; n1 < 8; ++n1) a[n2][n1] = v[4 * n1 + n2];
+            Dft<8, DIR>::run(a[n2]);
+        }
+#pragma unroll
+        for (int n2 = 1; n2 < 4; ++n2)
+#pragma unroll
+            for (int k1 = 1; k1 < 8; ++k1) a[n2][k1] = mul_w32<DIR>(a[n2][k1], n2 * k1);
+#pragma unroll
+        for (int k1 = 0; k1 < 8; ++k1) {
+            dft4<DIR>(a[0][k1], a[1][k1], a[2][k1], a[3][k1]);
+            v[k1] = a[0][k1];
+            v[k1 + 8] = a[1][k1];
+            v[k1 + 16] = a[2][k1];
+            v[k1 + 24] = a[3][k1];
+        }
+    }
+};
+
 // One Stockham pass, in place in shared memory.  `buf` is this FFT's base,
 // `es` the element stride, `t` the thread's index among the T threads that
 // share this FFT.  All threads of the block must call it (it synchronises).

@@ -375,6 +375,8 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
 // reading (c varies).  The group exchange uses the same trick.
 // frame buffer 128 KB, then a 1 KB twiddle table
 constexpr int P128_SMEM = (64 * 128) * 16 + 128 * 8;
+// the two-exchange det-128 kernels: the 128 KB exchange buffer alone
+constexpr int P128X_SMEM = 128 * 128 * 8;
 // the fused-residual adjoint also stages the frame's 128 x 128 counts.  The
 // plain adjoint stays at P128_SMEM: the remaining ~125 KB of L1 keeps the
 // 128 KB probe table it rereads for every frame mostly resident (with 64 KB
@@ -526,6 +528,159 @@ __global__ void __launch_bounds__(512, 1)
                 __stcs(&row[t + 8 * k2], make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y));
         }
         __syncthreads();
+    }
+}
+
+// ---- det-128 frames with two shared-memory exchanges --------------------
+// B[u][v] = f sum_{r,q} A[r][q] w128^(DIR (u r + v q)) for a 128 x 128 array
+// A whose q runs along memory, in three register rounds:
+//   R1  thread (q = tid & 127, rt = (tid >> 7) + 4 c, c = 0, 1): 16-point
+//       DFTs over m of r = rt + 8 m, times w128^(rt k1)   -> (k1, q, rt)
+//   R2  thread (k1 = warp, qb = lane): the 8-point DFT over rt gives
+//       u = k1 + 16 k2; the 4-point DFT over qa of q = qb + 32 qa gives v1;
+//       times w128^(qb v1) and the frame factor f        -> (v1, u, qb)
+//   R3  thread (u = tid & 127, v1 = tid >> 7): the 32-point DFT over qb
+//       gives v = v1 + 4 v2.
+// R1's lanes load 32 consecutive q (256 B of one row) and R3's lanes hold 32
+// consecutive u.  The forward takes A = probe x patch [y][x] and stores
+// frame[kx = v][ky = u]; the adjoint takes A = frame[kx][ky] and adds
+// pixel [y = v][x = u] into the slab, so both touch 256 consecutive bytes per
+// warp access.  Between the rounds the frame goes once through the 128 KB
+// buffer ex, as E1[k1][qa][rt][qb] and E2[v1][u][qb]; E2's rows of 32 values
+// (256 B) have their 16-byte slots permuted by an XOR with u & 7, so that
+// every exchange access of a warp takes the minimum number of shared
+// wavefronts (two for 8-byte, four for 16-byte accesses).
+__device__ __forceinline__ int e1_at(int k1, int qa, int rt, int qb) { return ((k1 * 4 + qa) * 8 + rt) * 32 + qb; }
+__device__ __forceinline__ int e2_at(int v1, int u, int qb)
+{
+    return (v1 * 128 + u) * 32 + 2 * ((qb >> 1) ^ (u & 7)) + (qb & 1);
+}
+
+// R1 of one frame: v[c][m] holds A[rt + 8 m][q], rt = (tid >> 7) + 4 c;
+// transformed and written to E1.  The caller synchronises before and after.
+// tw4 is line_dft128's pair table; rt is the same across a warp, so its
+// loads are broadcasts.
+template <int DIR>
+__device__ __forceinline__ void frame_r1(float2 (&v)[2][16], float2 *ex, const float4 *__restrict__ tw4)
+{
+    const int q = threadIdx.x & 127;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const int rt = (threadIdx.x >> 7) + 4 * c;
+        ptfft::Dft<16, DIR>::run(v[c]);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) twiddle16<DIR, false>(v[c], __ldg(&tw4[k * 8 + rt]), k);
+#pragma unroll
+        for (int k1 = 0; k1 < 16; ++k1) ex[e1_at(k1, q >> 5, rt, q & 31)] = v[c][k1];
+    }
+}
+
+// R2 of one frame for thread (k1 = warp, qb = lane): reads E1, synchronises
+// (E1 fully read), transforms, and writes E2.  The twiddles w128^(qb j)
+// (j = 1..3, in direction DIR; w128[m] = exp(-2 pi i m / 128)) times the
+// frame factor f, and f itself for j = 0: the factor rides on the twiddles.
+template <int DIR>
+__device__ __forceinline__ void frame_r2(float2 *ex, float2 f, const float2 *__restrict__ w128)
+{
+    const int k1 = threadIdx.x >> 5, qb = threadIdx.x & 31;
+    float2 rw1 = __ldg(&w128[qb]), rw2 = __ldg(&w128[2 * qb]), rw3 = __ldg(&w128[3 * qb]);
+    if (DIR > 0) {
+        rw1.y = -rw1.y;
+        rw2.y = -rw2.y;
+        rw3.y = -rw3.y;
+    }
+    float2 a[4][8];
+#pragma unroll
+    for (int qa = 0; qa < 4; ++qa)
+#pragma unroll
+        for (int rt = 0; rt < 8; ++rt) a[qa][rt] = ex[e1_at(k1, qa, rt, qb)];
+    __syncthreads();
+#pragma unroll
+    for (int qa = 0; qa < 4; ++qa) ptfft::Dft<8, DIR>::run(a[qa]);
+    const float2 r1 = cmul(rw1, f), r2 = cmul(rw2, f), r3 = cmul(rw3, f);
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) {
+        ptfft::dft4<DIR>(a[0][k2], a[1][k2], a[2][k2], a[3][k2]);
+        const int u = k1 + 16 * k2;
+        ex[e2_at(0, u, qb)] = cmul(a[0][k2], f);
+        ex[e2_at(1, u, qb)] = cmul(a[1][k2], r1);
+        ex[e2_at(2, u, qb)] = cmul(a[2][k2], r2);
+        ex[e2_at(3, u, qb)] = cmul(a[3][k2], r3);
+    }
+}
+
+// R3's read of E2 for thread (u = tid & 127, v1 = tid >> 7): w[qb], qb = 0..31.
+__device__ __forceinline__ void frame_r3_read(float2 (&w)[32], const float2 *ex)
+{
+    const int u = threadIdx.x & 127, v1 = threadIdx.x >> 7;
+    const float4 *e4 = reinterpret_cast<const float4 *>(ex) + (v1 * 128 + u) * 16;
+#pragma unroll
+    for (int s = 0; s < 16; ++s) {
+        const float4 q = e4[s ^ (u & 7)];
+        w[2 * s] = make_float2(q.x, q.y);
+        w[2 * s + 1] = make_float2(q.z, q.w);
+    }
+}
+
+// The forward with two exchanges (see above); grid-stride over frames, one
+// resident block per SM.  w128[m] = exp(-2 pi i m / 128).
+template <bool FULL, bool SUB = false>
+__global__ void __launch_bounds__(512, 1)
+    k_ptycho_fwd128x(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
+                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
+                     int nframes, int P, float scale, const float4 *__restrict__ tw4,
+                     const float2 *__restrict__ w128, const int *__restrict__ sid = nullptr)
+{
+    extern __shared__ float4 sm4[];
+    float2 *ex = reinterpret_cast<float2 *>(sm4);
+    const int q = threadIdx.x & 127, r0 = threadIdx.x >> 7;  // R1: x = q, y = r0 + 4 c + 8 m; R3: ky = q
+    const int off = FULL ? 0 : (128 - P) / 2;
+    for (int fid = blockIdx.x; fid < nframes; fid += gridDim.x) {
+        const int th = fid / nscan;
+        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
+        float2 *out = g + (size_t)fid * 128 * 128;
+        if (stx < 0 || sty < 0) {
+            for (int e = threadIdx.x; e < 128 * 128 / 2; e += 512) reinterpret_cast<float4 *>(out)[e] = make_float4(0, 0, 0, 0);
+            continue;
+        }
+        const float2 *src = psi + ((size_t)th * nz + sty) * n + stx;
+        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
+        // an opaque per-frame copy of the probe pointer and window offset: the
+        // 32 probe addresses and window tests are formed here, not hoisted out
+        // of the frame loop into registers
+        int offf = off;
+        asm volatile("mov.b64 %0, %0;" : "+l"(pr));
+        asm volatile("mov.b32 %0, %0;" : "+r"(offf));
+        const int PS = FULL ? 128 : P;  // a constant row stride: the probe rows are immediate offsets
+        {
+            float2 v[2][16];
+            const int px = q - offf;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const int py = r0 + 4 * c + 8 * m - offf;
+                    if (FULL) {
+                        v[c][m] = cmul(__ldg(&pr[py * PS + px]), __ldg(&src[(size_t)py * n + px]));
+                    } else {
+                        float2 val = czero();
+                        if (py >= 0 && py < P && px >= 0 && px < P)
+                            val = cmul(__ldg(&pr[py * PS + px]), __ldg(&src[(size_t)py * n + px]));
+                        v[c][m] = val;
+                    }
+                }
+            }
+            frame_r1<-1>(v, ex, tw4);
+        }
+        __syncthreads();
+        frame_r2<-1>(ex, scale * phase[fid], w128);
+        __syncthreads();
+        float2 w[32];
+        frame_r3_read(w, ex);
+        __syncthreads();  // E2 fully read: the next frame's R1 may write
+        ptfft::Dft<32, -1>::run(w);
+#pragma unroll
+        for (int v2 = 0; v2 < 32; ++v2) __stcs(&out[(r0 + 4 * v2) * 128 + q], w[v2]);  // frame[kx = r0 + 4 v2][ky = q]
     }
 }
 
@@ -752,6 +907,85 @@ __global__ void __launch_bounds__(512, 1)
         }
     }
     cp_async_wait_all();
+}
+
+// The adjoint with two exchanges (see k_ptycho_fwd128x); grid (parts,
+// ntheta) as k_ptycho_adj128: block (part, angle) owns slab dst[angle][part].
+// R3's thread adds pixel column x = kx, rows y = ky1 + 4 ky2, into the slab,
+// so the 32 lanes of a warp touch 256 consecutive bytes of one slab row
+// whatever the frame's column parity.  w128[m] = exp(-2 pi i m / 128).
+template <bool FULL, int RESID, bool SUB = false>
+__global__ void __launch_bounds__(512, 1)
+    k_ptycho_adj128x(const float2 *__restrict__ g, float2 *dst, const int *__restrict__ corner,
+                     const float2 *__restrict__ phase, const float2 *prbT, int nz, int n, int nscan,
+                     int P, float scale, const float4 *__restrict__ tw4, const float2 *__restrict__ w128,
+                     const float *__restrict__ data, float dscale, const int *__restrict__ sid = nullptr)
+{
+    extern __shared__ float4 sm4[];
+    float2 *ex = reinterpret_cast<float2 *>(sm4);
+    const int part = blockIdx.x, parts = gridDim.x, th = blockIdx.y;
+    float2 *slab = dst + ((size_t)th * parts + part) * nz * n;
+    for (int e = threadIdx.x; e < nz * n; e += 512) slab[e] = czero();
+    const int q = threadIdx.x & 127, r0 = threadIdx.x >> 7;  // R1: ky = q, kx = r0 + 4 c + 8 m; R3: x = q
+    const int off = FULL ? 0 : (128 - P) / 2;
+    const float2 *gth = g + (size_t)th * nscan * 128 * 128;
+    const float *dth = RESID ? data + (size_t)th * nscan * 128 * 128 : nullptr;
+    for (int s = part; s < nscan; s += parts) {
+        const int fid = th * nscan + s;
+        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
+        if (stx < 0 || sty < 0) continue;
+        {
+            const float2 *in = gth + (size_t)s * 128 * 128;
+            float2 v[2][16];
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const int e = (r0 + 4 * c + 8 * m) * 128 + q;
+                    float2 x = __ldg(&in[e]);
+                    if constexpr (RESID != 0) x = resid_of<RESID>(x, __ldg(&dth[(size_t)s * 128 * 128 + e]) * dscale);
+                    v[c][m] = x;
+                }
+            frame_r1<+1>(v, ex, tw4);
+        }
+        __syncthreads();
+        const float2 ph = phase[fid];
+        frame_r2<+1>(ex, make_float2(scale * ph.x, -scale * ph.y), w128);
+        __syncthreads();
+        float2 w[32];
+        frame_r3_read(w, ex);
+        __syncthreads();  // E2 fully read: the next frame's R1 may write
+        ptfft::Dft<32, +1>::run(w);
+        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
+        // an opaque per-frame copy of the probe pointer: the 32 row addresses
+        // are formed here, not hoisted out of the frame loop into registers
+        int offf = off;  // likewise the row window's offset and its 32 tests
+        asm volatile("mov.b64 %0, %0;" : "+l"(pr));
+        asm volatile("mov.b32 %0, %0;" : "+r"(offf));
+        const int px = q - offf;
+        if (!FULL && (px < 0 || px >= P)) continue;
+        float2 *col = slab + (size_t)sty * n + stx + px;
+        // RB rows at a time: their probe and slab loads are issued before the
+        // first store
+        constexpr int RB = 8;
+        const int PS = FULL ? 128 : P;  // a constant row stride: the probe rows are immediate offsets
+#pragma unroll
+        for (int h = 0; h < 32; h += RB) {
+            float2 cur[RB], pv[RB];
+#pragma unroll
+            for (int j = 0; j < RB; ++j) {
+                const int py = r0 + 4 * (h + j) - offf;
+                const bool ok = FULL || (py >= 0 && py < P);
+                pv[j] = ok ? pr[py * PS + px] : czero();
+                cur[j] = ok ? col[(size_t)py * n] : czero();
+            }
+#pragma unroll
+            for (int j = 0; j < RB; ++j) {
+                const int py = r0 + 4 * (h + j) - offf;
+                if (FULL || (py >= 0 && py < P)) col[(size_t)py * n] = cur[j] + cmulc(pv[j], w[h + j]);
+            }
+        }
+    }
 }
 
 // The same transform written for both adjoints.  PROBE: the adjoint with
@@ -1149,6 +1383,14 @@ int ptycho_attrs()
         if constexpr (DET == 128) {
             PT_ATTR(k_ptycho_fwd128<true>, P128_SMEM);
             PT_ATTR(k_ptycho_fwd128<false>, P128_SMEM);
+            PT_ATTR((k_ptycho_fwd128x<true>), P128X_SMEM);
+            PT_ATTR((k_ptycho_fwd128x<false>), P128X_SMEM);
+            PT_ATTR((k_ptycho_fwd128x<true, true>), P128X_SMEM);
+            PT_ATTR((k_ptycho_fwd128x<false, true>), P128X_SMEM);
+            PT_ATTR((k_ptycho_adj128x<true, 0>), P128X_SMEM);
+            PT_ATTR((k_ptycho_adj128x<false, 0>), P128X_SMEM);
+            PT_ATTR((k_ptycho_adj128x<true, 0, true>), P128X_SMEM);
+            PT_ATTR((k_ptycho_adj128x<false, 0, true>), P128X_SMEM);
             PT_ATTR((k_ptycho_adj128<true, 0>), P128_SMEM);
             PT_ATTR((k_ptycho_adj128<false, 0>), P128_SMEM);
             PT_ATTR((k_ptycho_adj128<true, 1>), P128_SMEM_RESID);
@@ -1191,15 +1433,25 @@ int ptycho_adj_launch(pt_ptycho *h, float2 *out, const float2 *in, float scale, 
                     k_ptycho_adj128v<true, RESID, false, S><<<grid, 512, smem, st>>>(
                         in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
                         h->tw128, data, dscale, nullptr, 0, h->shift_ids());
+                else if constexpr (RESID == 0)
+                    k_ptycho_adj128x<true, RESID, S><<<grid, 512, P128X_SMEM, st>>>(
+                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
+                        h->tw128, h->tw, data, dscale, h->shift_ids());
                 else
                     k_ptycho_adj128<true, RESID, S><<<grid, 512, smem, st>>>(
                         in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
                         h->tw128, data, dscale, h->shift_ids());
             }
-            else if (fast128)
-                k_ptycho_adj128<false, RESID, S><<<grid, 512, smem, st>>>(
-                    in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale, h->tw128,
-                    data, dscale, h->shift_ids());
+            else if (fast128) {
+                if constexpr (RESID == 0)
+                    k_ptycho_adj128x<false, RESID, S><<<grid, 512, P128X_SMEM, st>>>(
+                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
+                        h->tw128, h->tw, data, dscale, h->shift_ids());
+                else
+                    k_ptycho_adj128<false, RESID, S><<<grid, 512, smem, st>>>(
+                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
+                        h->tw128, data, dscale, h->shift_ids());
+            }
             else
                 k_ptycho_adj<DET, RESID, S><<<grid, F::NT, F::SMEM, st>>>(
                     in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale, h->tw,
@@ -1244,15 +1496,13 @@ int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scal
         auto go = [&](auto sub) {
             constexpr bool S = decltype(sub)::value;
             if (fast128 && h->P == DET)
-                k_ptycho_fwd128<true, S><<<grid128, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase_tab(),
-                                                                         h->probe_tab(), h->nz, h->n, h->nscan,
-                                                                         nframes, h->P, scale, h->tw128,
-                                                                         h->shift_ids());
+                k_ptycho_fwd128x<true, S><<<grid128, 512, P128X_SMEM, st>>>(
+                    in, out, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, nframes, h->P, scale,
+                    h->tw128, h->tw, h->shift_ids());
             else if (fast128)
-                k_ptycho_fwd128<false, S><<<grid128, 512, P128_SMEM, st>>>(in, out, h->corner, h->phase_tab(),
-                                                                          h->probe_tab(), h->nz, h->n, h->nscan,
-                                                                          nframes, h->P, scale, h->tw128,
-                                                                          h->shift_ids());
+                k_ptycho_fwd128x<false, S><<<grid128, 512, P128X_SMEM, st>>>(
+                    in, out, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, nframes, h->P, scale,
+                    h->tw128, h->tw, h->shift_ids());
             else
                 k_ptycho_fwd<DET, S><<<nframes, F::NT, F::SMEM, st>>>(in, out, h->corner, h->phase_tab(),
                                                                      h->probe_tab(), h->nz, h->n, h->nscan, nframes,
