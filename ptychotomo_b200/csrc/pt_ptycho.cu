@@ -368,167 +368,24 @@ __global__ void __launch_bounds__(PF<DET>::NT, 1)
     }
 }
 
-// ---- det = 128: 16-byte shared-memory traffic ------------------------------
-// Transpose in a "pair" layout: a 16-byte slot holds rows 2q and 2q+1 of one
-// column; slot (q, c) lives at q * 128 + (c ^ (q & 7)), so the 8 threads of a
-// group hit 8 distinct 4-bank groups both when writing (q varies) and when
-// reading (c varies).  The group exchange uses the same trick.
-// frame buffer 128 KB, then a 1 KB twiddle table
-constexpr int P128_SMEM = (64 * 128) * 16 + 128 * 8;
-// the two-exchange det-128 kernels: the 128 KB exchange buffer alone
-constexpr int P128X_SMEM = 128 * 128 * 8;
-// the fused-residual adjoint also stages the frame's 128 x 128 counts.  The
-// plain adjoint stays at P128_SMEM: the remaining ~125 KB of L1 keeps the
-// 128 KB probe table it rereads for every frame mostly resident (with 64 KB
-// more shared memory it ran at twice the time).
-// The fused-residual kernels keep a second 1 KB table, the row pass's
-// twiddles folded with the frame's scale x conj(phase) (see line_dft128).
-constexpr int P128_SMEM_RESID = P128_SMEM + 128 * 8 + 128 * 128 * 4;
-
+// ---- det = 128 ---------------------------------------------------------
+// shared memory: the 128 KB exchange buffer alone.  The remaining ~100 KB of
+// L1 keeps most of the 128 KB probe table, reread for every frame, resident.
+constexpr int P128_SMEM = 128 * 128 * 8;
 
 // The det-128 twiddles a thread needs, w(t k1) for k1 = 0..15, in pairs:
-// entry q * 8 + t of the 64-entry float4 table holds w(2q t) and w((2q+1) t).
-// The 8 threads of a group read 8 consecutive entries (one conflict-free
-// 128-byte access, shared by the warp's 4 groups), 8 loads per line.
-//
-// FOLD: the line still has to be multiplied by a per-frame factor f (the
-// scan's phase and the scale).  Since the transform is linear, f rides on the
-// twiddles: tw4 is then a per-frame table (fold_twiddles) already in the
-// transform's direction and multiplied by f, whose k1 = 0 entries are f
-// itself, so element 0 takes its product from the table as well.
-template <int DIR, bool FOLD>
+// entry q * 8 + t of the 64-entry float4 table holds w(2q t) and w((2q+1) t)
+// (w = exp(-2 pi i / 128); DIR > 0 takes the conjugates).
+template <int DIR>
 __device__ __forceinline__ void twiddle16(float2 (&v)[16], float4 w, int q)
 {
     float2 w0 = make_float2(w.x, w.y), w1 = make_float2(w.z, w.w);
-    if (DIR > 0 && !FOLD) {
+    if (DIR > 0) {
         w0.y = -w0.y;
         w1.y = -w1.y;
     }
-    if (FOLD || q > 0) v[2 * q] = cmul(v[2 * q], w0);
+    if (q > 0) v[2 * q] = cmul(v[2 * q], w0);
     v[2 * q + 1] = cmul(v[2 * q + 1], w1);
-}
-
-template <int DIR, bool FOLD = false>
-__device__ __forceinline__ void line_dft128(float2 (&v)[16], int t, float4 *sc, const float4 *tw4)
-{
-    ptfft::Dft<16, DIR>::run(v);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) twiddle16<DIR, FOLD>(v, tw4[q * 8 + t], q);
-    __syncwarp();
-#pragma unroll
-    for (int q = 0; q < 8; ++q) sc[t * 8 + ((q + t) & 7)] = make_float4(v[2 * q].x, v[2 * q].y, v[2 * q + 1].x, v[2 * q + 1].y);
-    __syncwarp();
-    float2 u0[8], u1[8];
-#pragma unroll
-    for (int n2 = 0; n2 < 8; ++n2) {
-        const float4 w = sc[n2 * 8 + ((t + n2) & 7)];
-        u0[n2] = make_float2(w.x, w.y);
-        u1[n2] = make_float2(w.z, w.w);
-    }
-    ptfft::Dft<8, DIR>::run(u0);
-    ptfft::Dft<8, DIR>::run(u1);
-#pragma unroll
-    for (int k2 = 0; k2 < 8; ++k2) {
-        v[k2] = u0[k2];       // X[2t + 16 k2]
-        v[8 + k2] = u1[k2];   // X[2t + 1 + 16 k2]
-    }
-}
-
-// Per-frame folded twiddle table for line_dft128<DIR, true>: the pair table
-// tw4 in direction DIR times f, the k1 = 0 entries (a twiddle of 1) being f
-// exactly.  Threads 0..63 write one entry each.
-template <int DIR>
-__device__ __forceinline__ void fold_twiddles(float4 *twf, const float4 *__restrict__ tw4, float2 f)
-{
-    const int i = threadIdx.x;
-    if (i < 64) {
-        const float4 w = tw4[i];
-        float2 w0 = make_float2(w.x, w.y), w1 = make_float2(w.z, w.w);
-        if (DIR > 0) {
-            w0.y = -w0.y;
-            w1.y = -w1.y;
-        }
-        const float2 a = i < 8 ? f : cmul(w0, f), b = cmul(w1, f);
-        twf[i] = make_float4(a.x, a.y, b.x, b.y);
-    }
-}
-
-template <bool FULL, bool SUB = false>
-__global__ void __launch_bounds__(512, 1)
-    k_ptycho_fwd128(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
-                    const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                    int nframes, int P, float scale, const float4 *__restrict__ tw,
-                    const int *__restrict__ sid = nullptr)
-{
-    extern __shared__ float4 sm4[];
-    float4 *fr = sm4;
-    // the shared table holds this frame's column twiddles x scale x phase
-    // (line_dft128's FOLD); the row pass reads the plain twiddles from global
-    float4 *twf = sm4 + 64 * 128;
-    const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
-    // exchange slots, one per line: the whole frame buffer is idle during both
-    // passes, so the two lines' exchanges need not wait on each other
-    float4 *sa = fr + grp * 64, *sb = fr + 64 * 64 + grp * 64;
-    const int off = FULL ? 0 : (128 - P) / 2;
-    for (int fid = blockIdx.x; fid < nframes; fid += gridDim.x) {
-        const int th = fid / nscan;
-        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
-        float2 *out = g + (size_t)fid * 128 * 128;
-        if (stx < 0 || sty < 0) {
-            for (int e = threadIdx.x; e < 128 * 128 / 2; e += 512) reinterpret_cast<float4 *>(out)[e] = make_float4(0, 0, 0, 0);
-            continue;
-        }
-        const float2 *src = psi + ((size_t)th * nz + sty) * n + stx;
-        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
-        float2 v[2][16];
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int py = grp + 64 * c - off;
-#pragma unroll
-            for (int m = 0; m < 16; ++m) {
-                const int px = t + 8 * m - off;
-                if (FULL) {
-                    v[c][m] = cmul(__ldg(&pr[py * P + px]), __ldg(&src[(size_t)py * n + px]));
-                } else {
-                    float2 val = czero();
-                    if (py >= 0 && py < P && px >= 0 && px < P)
-                        val = cmul(__ldg(&pr[py * P + px]), __ldg(&src[(size_t)py * n + px]));
-                    v[c][m] = val;
-                }
-            }
-            line_dft128<-1>(v[c], t, c ? sb : sa, tw);
-        }
-        fold_twiddles<-1>(twf, tw, scale * phase[fid]);  // read after the next block barrier
-        __syncthreads();
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int iy = grp + 64 * c;
-#pragma unroll
-            for (int k2 = 0; k2 < 8; ++k2) {
-                const int kp = t + 8 * k2;
-                fr[kp * 128 + (iy ^ (kp & 7))] = make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const float4 q = fr[grp * 128 + ((t + 8 * m) ^ (grp & 7))];
-            v[0][m] = make_float2(q.x, q.y);
-            v[1][m] = make_float2(q.z, q.w);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            line_dft128<-1, true>(v[c], t, c ? sb : sa, twf);
-            // streaming stores: the frames are not read again by this kernel
-            // (3.95 against 3.97 ms at 256^3)
-            float4 *row = reinterpret_cast<float4 *>(out + (2 * grp + c) * 128);
-#pragma unroll
-            for (int k2 = 0; k2 < 8; ++k2)   // ky = 2t + 16 k2, +1
-                __stcs(&row[t + 8 * k2], make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y));
-        }
-        __syncthreads();
-    }
 }
 
 // ---- det-128 frames with two shared-memory exchanges --------------------
@@ -558,7 +415,7 @@ __device__ __forceinline__ int e2_at(int v1, int u, int qb)
 
 // R1 of one frame: v[c][m] holds A[rt + 8 m][q], rt = (tid >> 7) + 4 c;
 // transformed and written to E1.  The caller synchronises before and after.
-// tw4 is line_dft128's pair table; rt is the same across a warp, so its
+// tw4 is twiddle16's pair table; rt is the same across a warp, so its
 // loads are broadcasts.
 template <int DIR>
 __device__ __forceinline__ void frame_r1(float2 (&v)[2][16], float2 *ex, const float4 *__restrict__ tw4)
@@ -569,7 +426,7 @@ __device__ __forceinline__ void frame_r1(float2 (&v)[2][16], float2 *ex, const f
         const int rt = (threadIdx.x >> 7) + 4 * c;
         ptfft::Dft<16, DIR>::run(v[c]);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) twiddle16<DIR, false>(v[c], __ldg(&tw4[k * 8 + rt]), k);
+        for (int k = 0; k < 8; ++k) twiddle16<DIR>(v[c], __ldg(&tw4[k * 8 + rt]), k);
 #pragma unroll
         for (int k1 = 0; k1 < 16; ++k1) ex[e1_at(k1, q >> 5, rt, q & 31)] = v[c][k1];
     }
@@ -626,7 +483,7 @@ __device__ __forceinline__ void frame_r3_read(float2 (&w)[32], const float2 *ex)
 // resident block per SM.  w128[m] = exp(-2 pi i m / 128).
 template <bool FULL, bool SUB = false>
 __global__ void __launch_bounds__(512, 1)
-    k_ptycho_fwd128x(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
+    k_ptycho_fwd128(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
                      const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
                      int nframes, int P, float scale, const float4 *__restrict__ tw4,
                      const float2 *__restrict__ w128, const int *__restrict__ sid = nullptr)
@@ -684,268 +541,58 @@ __global__ void __launch_bounds__(512, 1)
     }
 }
 
-// cp.async helpers (16-byte global -> shared copies, Ampere+ async copy)
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-    const unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
-
-// Rows 0..63 of frame `in` (64 KB) -> shared [row][64 chunks of 16 B], chunk
-// index XORed with (row & 1) << 2 so that Phase A reads are conflict-free.
-__device__ __forceinline__ void prefetch_half_frame(float4 *dst, const float2 *in)
-{
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int id = threadIdx.x + 512 * i;
-        const int row = id >> 6, c16 = id & 63;
-        cp_async16(dst + row * 64 + (c16 ^ ((row & 1) << 2)), in + row * 128 + 2 * c16);
-    }
-    cp_async_commit();
-}
-
-// Row grp of frame `in` -> the group's own 1 KB row of the prefetch buffer,
-// in the layout of prefetch_half_frame.  Only the group's 8 threads touch
-// that row, so a warp barrier orders it against the group's exchange slot
-// there.
-__device__ __forceinline__ void prefetch_group_row(float4 *pre, const float2 *in, int grp, int t)
-{
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const int c16 = t + 8 * j;
-        cp_async16(pre + grp * 64 + (c16 ^ ((grp & 1) << 2)), in + grp * 128 + 2 * c16);
-    }
-    cp_async_commit();
-}
-
-// The 128 x 128 counts of one frame (64 KB) -> shared [row][128], row r's
-// columns rotated by 8 (r & 3) so that four groups reading rows r..r+3 at
-// the same columns hit distinct banks.
-__device__ __forceinline__ void prefetch_counts(float *dst, const float *data)
-{
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int id = threadIdx.x + 512 * i;
-        const int row = id >> 5, c4 = (id & 31) * 4;
-        cp_async16(dst + row * 128 + ((c4 + 8 * (row & 3)) & 127), data + row * 128 + c4);
-    }
-    cp_async_commit();
-}
-__device__ __forceinline__ float staged_count(const float *cnt, int row, int col)
-{
-    return cnt[row * 128 + ((col + 8 * (row & 3)) & 127)];
-}
-
-// row[px] += conj(mul[px]) x v for a thread's 16 pixels px = 2t + j + 16 k2
-// (v[8 j + k2]) with 16-byte accesses: row and mul 16-byte aligned at px = 0,
-// so pixels 2t + 16 k2 and the next share one.  All 8 row loads are issued
-// before any store.  Same arithmetic as the 8-byte form.
-__device__ __forceinline__ void rmw_row16(float2 *row, const float2 *__restrict__ mul, const float2 (&v)[16], int t)
-{
-    float4 *row4 = reinterpret_cast<float4 *>(row);
-    const float4 *mul4 = reinterpret_cast<const float4 *>(mul);
-    float4 cur[8];
-#pragma unroll
-    for (int k2 = 0; k2 < 8; ++k2) cur[k2] = row4[t + 8 * k2];
-#pragma unroll
-    for (int k2 = 0; k2 < 8; ++k2) {
-        const float4 w = __ldg(&mul4[t + 8 * k2]);
-        const float2 a = make_float2(cur[k2].x, cur[k2].y) + cmulc(make_float2(w.x, w.y), v[k2]);
-        const float2 b = make_float2(cur[k2].z, cur[k2].w) + cmulc(make_float2(w.z, w.w), v[8 + k2]);
-        row4[t + 8 * k2] = make_float4(a.x, a.y, b.x, b.y);
-    }
-}
-
-// grid (parts, ntheta): block (part, angle) owns slab dst[angle][part].
-// While the current frame finishes, the next frame's rows 0..63 are already
-// on their way into the idle half of the shared frame buffer.
-template <bool FULL, int RESID, bool SUB = false>
+// The adjoints with two exchanges (see k_ptycho_fwd128).  Object adjoint:
+// grid (parts, ntheta), block (part, angle) owns slab dst[angle][part] and
+// walks that angle's scans part, part + parts, ...  PROBE (the adjoint with
+// respect to the probe, as k_ptycho_adj_probe): grid (blocks, 1), block b
+// walks frames b, b + gridDim.x, ... < nframes and accumulates
+// conj(psi patch) x frame into its P x P partial dst[b].  RESID forms the
+// Poisson / Gaussian residual of each frame value on load.  R3's thread adds
+// pixel column x = u, rows y = v1 + 4 v2, so the 32 lanes of a warp touch
+// 256 consecutive bytes of one slab (or partial) row whatever the frame's
+// column parity.  w128[m] = exp(-2 pi i m / 128).
+template <bool FULL, int RESID, bool SUB = false, bool PROBE = false>
 __global__ void __launch_bounds__(512, 1)
-    k_ptycho_adj128(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
-                    const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                    int P, float scale, const float4 *__restrict__ tw, const float *__restrict__ data,
-                    float dscale, const int *__restrict__ sid = nullptr)
-{
-    // SLOT2: the second line of a group exchanges through the group's own
-    // prefetch row (already in registers), and the next frame's row is
-    // fetched by the group itself after a warp barrier.  FOLD: the frame's
-    // scale x conj(phase) rides on the row-pass twiddles (line_dft128); the
-    // folded table is written for the next frame during the column pass,
-    // after the last read of the current one.  Both measured faster with the
-    // Poisson residual and slower for the plain adjoint.
-    constexpr bool SLOT2 = RESID == 1, FOLD = RESID == 1;
-    extern __shared__ float4 sm4[];
-    float4 *fr = sm4;
-    float4 *pre = sm4 + 64 * 64;  // upper 64 KB of the frame buffer
-    float4 *tws = sm4 + 64 * 128;
-    float4 *twf = tws + 64;  // RESID: the folded row-pass twiddles
-    float *cnt = reinterpret_cast<float *>(sm4 + 64 * 128 + 128);  // RESID: this frame's counts
-    const int part = blockIdx.x, parts = gridDim.x, th = blockIdx.y;
-    float2 *slab = dst + ((size_t)th * parts + part) * nz * n;
-    for (int i = threadIdx.x; i < 64; i += 512) tws[i] = tw[i];
-    for (int e = threadIdx.x; e < nz * n; e += 512) slab[e] = czero();
-    const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
-    float4 *sa = fr + grp * 64, *sb = pre + grp * 64;
-    auto prefetch_frame = [&](const float2 *src) {
-        if constexpr (SLOT2)
-            prefetch_group_row(pre, src, grp, t);
-        else
-            prefetch_half_frame(pre, src);
-    };
-    auto fold_for = [&](int f) {
-        const float2 p = phase[f];
-        fold_twiddles<+1>(twf, tw, make_float2(scale * p.x, -scale * p.y));
-    };
-    const int off = FULL ? 0 : (128 - P) / 2;
-    // plain adjoint: slab rows of frames at an even column take 16-byte
-    // accesses (5.48 against 5.75 ms at 256^3; slower with the Poisson residual)
-    const bool vec = RESID == 0 && FULL && (n & 1) == 0 && ((uintptr_t)dst & 15) == 0;
-    const float2 *gth = g + (size_t)th * nscan * 128 * 128;
-    const float *dth = RESID ? data + (size_t)th * nscan * 128 * 128 : nullptr;
-    if (part < nscan) {
-        if constexpr (FOLD) fold_for(th * nscan + part);
-        prefetch_frame(gth + (size_t)part * 128 * 128);
-        if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)part * 128 * 128);
-    }
-    for (int s = part; s < nscan; s += parts) {
-        const int fid = th * nscan + s;
-        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
-        const float2 *in = gth + (size_t)s * 128 * 128;
-        const bool more = s + parts < nscan;
-        const float2 *in_next = more ? in + (size_t)parts * 128 * 128 : nullptr;
-        cp_async_wait_all();
-        __syncthreads();
-        if (stx < 0 || sty < 0) {  // skipped scan: keep the prefetch chain going
-            __syncthreads();
-            if (more) {
-                if constexpr (FOLD) fold_for(fid + parts);
-                prefetch_frame(in_next);
-                if constexpr (RESID != 0) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
-            }
-            continue;
-        }
-        const float2 ph = FOLD ? make_float2(1.f, 0.f) : phase[fid];
-        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
-        float2 v[2][16];
-        // rows 64..127 from global first, so their latency hides behind row 0..63's work
-#pragma unroll
-        for (int m = 0; m < 16; ++m) v[1][m] = __ldg(&in[(grp + 64) * 128 + t + 8 * m]);
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const int ky = t + 8 * m;
-            const float4 q = pre[grp * 64 + ((ky >> 1) ^ ((grp & 1) << 2))];
-            const float2 x = (ky & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
-            float D = 0.f;
-            if constexpr (RESID != 0) D = staged_count(cnt, grp, ky) * dscale;
-            v[0][m] = FOLD ? resid_of<RESID>(x, D) : scale * cmulc(ph, resid_of<RESID>(x, D));
-        }
-        line_dft128<+1, FOLD>(v[0], t, sa, FOLD ? twf : tws);
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            float D = 0.f;
-            if constexpr (RESID != 0) D = staged_count(cnt, grp + 64, t + 8 * m) * dscale;
-            v[1][m] = FOLD ? resid_of<RESID>(v[1][m], D) : scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
-        }
-        line_dft128<+1, FOLD>(v[1], t, SLOT2 ? sb : sa, FOLD ? twf : tws);
-        __syncthreads();
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int kx = grp + 64 * c;
-#pragma unroll
-            for (int k2 = 0; k2 < 8; ++k2) {
-                const int ip = t + 8 * k2;
-                fr[ip * 128 + (kx ^ (ip & 7))] = make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const float4 q = fr[grp * 128 + ((t + 8 * m) ^ (grp & 7))];
-            v[0][m] = make_float2(q.x, q.y);
-            v[1][m] = make_float2(q.z, q.w);
-        }
-        __syncthreads();
-        if constexpr (FOLD)
-            if (more) fold_for(fid + parts);
-        if (more && !SLOT2) prefetch_half_frame(pre, in_next);
-        if constexpr (RESID != 0)
-            if (more) prefetch_counts(cnt, dth + (size_t)(s + parts) * 128 * 128);
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            line_dft128<+1>(v[c], t, SLOT2 && c ? sb : sa, tws);
-            if (SLOT2 && c == 1) {
-                __syncwarp();  // the group's reads of its slot sb are done before the next frame lands there
-                if (more) prefetch_group_row(pre, in_next, grp, t);
-            }
-            const int py = 2 * grp + c - off;
-            if (!FULL && (py < 0 || py >= P)) continue;
-            float2 *row = slab + (size_t)(sty + py) * n + stx;
-            if (vec && (stx & 1) == 0) {
-                rmw_row16(row, pr + (size_t)py * 128, v[c], t);
-                continue;
-            }
-            // all 16 slab values are loaded before any is stored back, so the
-            // loads overlap instead of waiting on each other's stores
-            float2 cur[16];
-#pragma unroll
-            for (int k2 = 0; k2 < 8; ++k2)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const int px = 2 * t + j + 16 * k2 - off;
-                    cur[j * 8 + k2] = (FULL || (px >= 0 && px < P)) ? row[px] : czero();
-                }
-#pragma unroll
-            for (int k2 = 0; k2 < 8; ++k2)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const int px = 2 * t + j + 16 * k2 - off;
-                    if (FULL || (px >= 0 && px < P))
-                        row[px] = cur[j * 8 + k2] + cmulc(__ldg(&pr[py * P + px]), v[c][j * 8 + k2]);
-                }
-        }
-    }
-    cp_async_wait_all();
-}
-
-// The adjoint with two exchanges (see k_ptycho_fwd128x); grid (parts,
-// ntheta) as k_ptycho_adj128: block (part, angle) owns slab dst[angle][part].
-// R3's thread adds pixel column x = kx, rows y = ky1 + 4 ky2, into the slab,
-// so the 32 lanes of a warp touch 256 consecutive bytes of one slab row
-// whatever the frame's column parity.  w128[m] = exp(-2 pi i m / 128).
-template <bool FULL, int RESID, bool SUB = false>
-__global__ void __launch_bounds__(512, 1)
-    k_ptycho_adj128x(const float2 *__restrict__ g, float2 *dst, const int *__restrict__ corner,
+    k_ptycho_adj128(const float2 *__restrict__ g, float2 *dst, const int *__restrict__ corner,
                      const float2 *__restrict__ phase, const float2 *prbT, int nz, int n, int nscan,
                      int P, float scale, const float4 *__restrict__ tw4, const float2 *__restrict__ w128,
-                     const float *__restrict__ data, float dscale, const int *__restrict__ sid = nullptr)
+                     const float *__restrict__ data, float dscale, const int *__restrict__ sid = nullptr,
+                     const float2 *psi = nullptr, int nframes = 0)
 {
     extern __shared__ float4 sm4[];
     float2 *ex = reinterpret_cast<float2 *>(sm4);
-    const int part = blockIdx.x, parts = gridDim.x, th = blockIdx.y;
-    float2 *slab = dst + ((size_t)th * parts + part) * nz * n;
-    for (int e = threadIdx.x; e < nz * n; e += 512) slab[e] = czero();
+    const int part = blockIdx.x, parts = gridDim.x, th0 = blockIdx.y;
+    float2 *slab = PROBE ? dst + (size_t)part * P * P : dst + ((size_t)th0 * parts + part) * nz * n;
+    for (int e = threadIdx.x; e < (PROBE ? P * P : nz * n); e += 512) slab[e] = czero();
     const int q = threadIdx.x & 127, r0 = threadIdx.x >> 7;  // R1: ky = q, kx = r0 + 4 c + 8 m; R3: x = q
     const int off = FULL ? 0 : (128 - P) / 2;
-    const float2 *gth = g + (size_t)th * nscan * 128 * 128;
-    const float *dth = RESID ? data + (size_t)th * nscan * 128 * 128 : nullptr;
-    for (int s = part; s < nscan; s += parts) {
-        const int fid = th * nscan + s;
+    const int count = PROBE ? nframes : nscan;
+    for (int s = part; s < count; s += parts) {
+        const int fid = PROBE ? s : th0 * nscan + s;
+        const int th = PROBE ? fid / nscan : th0;
         const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
         if (stx < 0 || sty < 0) continue;
         {
-            const float2 *in = gth + (size_t)s * 128 * 128;
+            const float2 *in = g + (size_t)fid * 128 * 128;
+            const float *din = RESID ? data + (size_t)fid * 128 * 128 : nullptr;
+            // all 32 frame values (and counts) are loaded before the first
+            // residual: its branches would otherwise hold each later load back
             float2 v[2][16];
+            float d[2][16];
 #pragma unroll
             for (int c = 0; c < 2; ++c)
 #pragma unroll
                 for (int m = 0; m < 16; ++m) {
                     const int e = (r0 + 4 * c + 8 * m) * 128 + q;
-                    float2 x = __ldg(&in[e]);
-                    if constexpr (RESID != 0) x = resid_of<RESID>(x, __ldg(&dth[(size_t)s * 128 * 128 + e]) * dscale);
-                    v[c][m] = x;
+                    v[c][m] = __ldg(&in[e]);
+                    if constexpr (RESID != 0) d[c][m] = __ldg(&din[e]);
                 }
+            if constexpr (RESID != 0) {
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) v[c][m] = resid_of<RESID>(v[c][m], d[c][m] * dscale);
+            }
             frame_r1<+1>(v, ex, tw4);
         }
         __syncthreads();
@@ -956,19 +603,23 @@ __global__ void __launch_bounds__(512, 1)
         frame_r3_read(w, ex);
         __syncthreads();  // E2 fully read: the next frame's R1 may write
         ptfft::Dft<32, +1>::run(w);
-        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
-        // an opaque per-frame copy of the probe pointer: the 32 row addresses
-        // are formed here, not hoisted out of the frame loop into registers
-        int offf = off;  // likewise the row window's offset and its 32 tests
-        asm volatile("mov.b64 %0, %0;" : "+l"(pr));
+        // object: slab += conj(probe) x value; probe: partial += conj(psi) x value
+        const float2 *mul = PROBE ? psi + ((size_t)th * nz + sty) * n + stx
+                                  : (SUB ? prbT + (size_t)sid[fid] * P * P : prbT);  // sub-pixel: the frame's shifted probe
+        // an opaque per-frame copy of the multiplier pointer: the 32 row
+        // addresses are formed here, not hoisted out of the frame loop into
+        // registers; likewise the row window's offset and its 32 tests
+        int offf = off;
+        asm volatile("mov.b64 %0, %0;" : "+l"(mul));
         asm volatile("mov.b32 %0, %0;" : "+r"(offf));
         const int px = q - offf;
         if (!FULL && (px < 0 || px >= P)) continue;
-        float2 *col = slab + (size_t)sty * n + stx + px;
-        // RB rows at a time: their probe and slab loads are issued before the
-        // first store
+        float2 *col = PROBE ? slab + px : slab + (size_t)sty * n + stx + px;
+        const size_t cs = PROBE ? P : n;                // row stride of col
+        const int ms = PROBE ? n : (FULL ? 128 : P);  // row stride of mul (a constant for the probe table)
+        // RB rows at a time: their multiplier and slab loads are issued
+        // before the first store
         constexpr int RB = 8;
-        const int PS = FULL ? 128 : P;  // a constant row stride: the probe rows are immediate offsets
 #pragma unroll
         for (int h = 0; h < 32; h += RB) {
             float2 cur[RB], pv[RB];
@@ -976,169 +627,16 @@ __global__ void __launch_bounds__(512, 1)
             for (int j = 0; j < RB; ++j) {
                 const int py = r0 + 4 * (h + j) - offf;
                 const bool ok = FULL || (py >= 0 && py < P);
-                pv[j] = ok ? pr[py * PS + px] : czero();
-                cur[j] = ok ? col[(size_t)py * n] : czero();
+                pv[j] = ok ? mul[(size_t)py * ms + px] : czero();
+                cur[j] = ok ? col[py * cs] : czero();
             }
 #pragma unroll
             for (int j = 0; j < RB; ++j) {
                 const int py = r0 + 4 * (h + j) - offf;
-                if (FULL || (py >= 0 && py < P)) col[(size_t)py * n] = cur[j] + cmulc(pv[j], w[h + j]);
+                if (FULL || (py >= 0 && py < P)) col[py * cs] = cur[j] + cmulc(pv[j], w[h + j]);
             }
         }
     }
-}
-
-// The same transform written for both adjoints.  PROBE: the adjoint with
-// respect to the probe (as k_ptycho_adj_probe): grid (blocks, 1), block b
-// walks frames b, b + gridDim.x, ... and accumulates conj(psi patch) x frame
-// into its P x P partial dst[b].  Otherwise as k_ptycho_adj128 with the
-// second line exchanging through the group's own prefetch row.  The compiler
-// schedules this formulation differently at the 128-register ceiling; it
-// measured faster for the Gaussian residual (11.0 ms for k_ptycho_adj128's)
-// and the probe adjoint (12.3 ms for k_ptycho_adj_probe) and slower for the
-// plain and Poisson object adjoints, so each launch takes the faster one.
-template <bool FULL, int RESID, bool PROBE, bool SUB = false>
-__global__ void __launch_bounds__(512, 1)
-    k_ptycho_adj128v(const float2 *__restrict__ g, float2 *__restrict__ dst, const int *__restrict__ corner,
-                    const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                    int P, float scale, const float4 *__restrict__ tw, const float *__restrict__ data,
-                    float dscale, const float2 *__restrict__ psi = nullptr, int nframes = 0,
-                    const int *__restrict__ sid = nullptr)
-{
-    extern __shared__ float4 sm4[];
-    float4 *fr = sm4;
-    float4 *pre = sm4 + 64 * 64;  // upper 64 KB of the frame buffer
-    float4 *tws = sm4 + 64 * 128;
-    // FOLD (object adjoint): the frame's scale x conj(phase) rides on the
-    // row-pass twiddles, as in k_ptycho_adj128
-    constexpr bool FOLD = !PROBE;
-    float4 *twf = tws + 64;
-    float *cnt = reinterpret_cast<float *>(sm4 + 64 * 128 + 128);  // RESID: this frame's counts
-    auto fold_for = [&](size_t f) {
-        const float2 p = phase[f];
-        fold_twiddles<+1>(twf, tw, make_float2(scale * p.x, -scale * p.y));
-    };
-    const int part = blockIdx.x, parts = gridDim.x;
-    const int th0 = blockIdx.y;   // the angle (object slabs)
-    float2 *slab = PROBE ? dst + (size_t)part * P * P : dst + ((size_t)th0 * parts + part) * nz * n;
-    for (int i = threadIdx.x; i < 64; i += 512) tws[i] = tw[i];
-    for (int e = threadIdx.x; e < (PROBE ? P * P : nz * n); e += 512) slab[e] = czero();
-    const int t = threadIdx.x & 7, grp = threadIdx.x >> 3;
-    // exchange slots: sa in the lower half, sb = the group's own prefetch row
-    float4 *sa = fr + grp * 64, *sb = pre + grp * 64;
-    const int off = FULL ? 0 : (128 - P) / 2;
-    // object adjoint: slab rows of frames at an even column take 16-byte
-    // accesses (7.36 against 7.58 ms for the Gaussian residual at 256^3; no
-    // steady gain for the probe adjoint)
-    const bool vec = !PROBE && FULL && (n & 1) == 0 && ((uintptr_t)dst & 15) == 0;
-    // frames k = part, part + parts, ... < count: fid = k (probe) or angle th0's scan k
-    const int count = PROBE ? nframes : nscan;
-    const size_t fid0 = PROBE ? (size_t)part : (size_t)th0 * nscan + part;
-    if (part < count) {
-        if constexpr (FOLD) fold_for(fid0);
-        prefetch_group_row(pre, g + fid0 * 128 * 128, grp, t);
-        if constexpr (RESID != 0) prefetch_counts(cnt, data + fid0 * 128 * 128);
-    }
-    for (int s = part; s < count; s += parts) {
-        const int fid = PROBE ? s : th0 * nscan + s;
-        const int th = PROBE ? fid / nscan : th0;
-        const int stx = corner[2 * fid], sty = corner[2 * fid + 1];
-        const float2 *in = g + (size_t)fid * 128 * 128;
-        const bool more = s + parts < count;
-        const float2 *in_next = more ? in + (size_t)parts * 128 * 128 : nullptr;
-        cp_async_wait_all();
-        __syncthreads();
-        if (stx < 0 || sty < 0) {  // skipped scan: keep the prefetch chain going
-            __syncthreads();
-            if (more) {
-                if constexpr (FOLD) fold_for((size_t)fid + parts);
-                prefetch_group_row(pre, in_next, grp, t);
-                if constexpr (RESID != 0) prefetch_counts(cnt, data + (size_t)(fid + parts) * 128 * 128);
-            }
-            continue;
-        }
-        const float2 ph = FOLD ? make_float2(1.f, 0.f) : phase[fid];
-        const float2 *pr = SUB ? prbT + (size_t)sid[fid] * P * P : prbT;  // sub-pixel: the frame's shifted probe
-        float2 v[2][16];
-        // rows 64..127 from global first, so their latency hides behind row 0..63's work
-#pragma unroll
-        for (int m = 0; m < 16; ++m) v[1][m] = __ldg(&in[(grp + 64) * 128 + t + 8 * m]);
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const int ky = t + 8 * m;
-            const float4 q = pre[grp * 64 + ((ky >> 1) ^ ((grp & 1) << 2))];
-            const float2 x = (ky & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
-            float D = 0.f;
-            if constexpr (RESID != 0) D = staged_count(cnt, grp, ky) * dscale;
-            v[0][m] = FOLD ? resid_of<RESID>(x, D) : scale * cmulc(ph, resid_of<RESID>(x, D));
-        }
-        line_dft128<+1, FOLD>(v[0], t, sa, FOLD ? twf : tws);
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            float D = 0.f;
-            if constexpr (RESID != 0) D = staged_count(cnt, grp + 64, t + 8 * m) * dscale;
-            v[1][m] = FOLD ? resid_of<RESID>(v[1][m], D) : scale * cmulc(ph, resid_of<RESID>(v[1][m], D));
-        }
-        line_dft128<+1, FOLD>(v[1], t, sb, FOLD ? twf : tws);
-        __syncthreads();
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int kx = grp + 64 * c;
-#pragma unroll
-            for (int k2 = 0; k2 < 8; ++k2) {
-                const int ip = t + 8 * k2;
-                fr[ip * 128 + (kx ^ (ip & 7))] = make_float4(v[c][k2].x, v[c][k2].y, v[c][8 + k2].x, v[c][8 + k2].y);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int m = 0; m < 16; ++m) {
-            const float4 q = fr[grp * 128 + ((t + 8 * m) ^ (grp & 7))];
-            v[0][m] = make_float2(q.x, q.y);
-            v[1][m] = make_float2(q.z, q.w);
-        }
-        __syncthreads();
-        if constexpr (FOLD)
-            if (more) fold_for((size_t)fid + parts);
-        if constexpr (RESID != 0)
-            if (more) prefetch_counts(cnt, data + (size_t)(fid + parts) * 128 * 128);
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            line_dft128<+1>(v[c], t, c ? sb : sa, tws);
-            if (c == 1) {
-                __syncwarp();  // the group's reads of its slot sb are done before the next frame lands there
-                if (more) prefetch_group_row(pre, in_next, grp, t);
-            }
-            const int py = 2 * grp + c - off;
-            if (!FULL && (py < 0 || py >= P)) continue;
-            // object: slab row += conj(c prbT) x; probe: partial row += conj(psi) x
-            float2 *row = PROBE ? slab + (size_t)py * P : slab + (size_t)(sty + py) * n + stx;
-            const float2 *mul = PROBE ? psi + ((size_t)th * nz + sty + py) * n + stx : pr + (size_t)py * P;
-            if (vec && (stx & 1) == 0) {
-                rmw_row16(row, mul, v[c], t);
-                continue;
-            }
-            // all 16 slab values are loaded before any is stored back, so the
-            // loads overlap instead of waiting on each other's stores
-            float2 cur[16];
-#pragma unroll
-            for (int k2 = 0; k2 < 8; ++k2)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const int px = 2 * t + j + 16 * k2 - off;
-                    cur[j * 8 + k2] = (FULL || (px >= 0 && px < P)) ? row[px] : czero();
-                }
-#pragma unroll
-            for (int k2 = 0; k2 < 8; ++k2)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const int px = 2 * t + j + 16 * k2 - off;
-                    if (FULL || (px >= 0 && px < P))
-                        row[px] = cur[j * 8 + k2] + cmulc(__ldg(&mul[px]), v[c][j * 8 + k2]);
-                }
-        }
-    }
-    cp_async_wait_all();
 }
 
 // out[angle] = sum over parts of dst[angle][part], fixed order
@@ -1324,7 +822,7 @@ struct pt_ptycho {
     bool ready = false;
     float c = 0.f;
     float2 *tw = nullptr, *prb = nullptr, *prbT = nullptr, *phase = nullptr, *partial = nullptr;
-    float4 *tw128 = nullptr;  // det = 128: the twiddles in line_dft128's pair layout
+    float4 *tw128 = nullptr;  // det = 128: the twiddles in twiddle16's pair layout
     int *corner = nullptr;
     // probe retrieval: a second transposed probe table (forward with a given
     // probe) and one P x P partial per block of the probe adjoint
@@ -1371,36 +869,25 @@ int ptycho_attrs()
         PT_ATTR((k_ptycho_adj<DET, 1, true>), s);
         PT_ATTR((k_ptycho_adj<DET, 2, true>), s);
         if constexpr (DET == 128) {
+            PT_ATTR((k_ptycho_fwd128<true>), P128_SMEM);
+            PT_ATTR((k_ptycho_fwd128<false>), P128_SMEM);
             PT_ATTR((k_ptycho_fwd128<true, true>), P128_SMEM);
             PT_ATTR((k_ptycho_fwd128<false, true>), P128_SMEM);
-            PT_ATTR((k_ptycho_adj128<true, 0, true>), P128_SMEM);
-            PT_ATTR((k_ptycho_adj128<false, 0, true>), P128_SMEM);
-            PT_ATTR((k_ptycho_adj128<true, 1, true>), P128_SMEM_RESID);
-            PT_ATTR((k_ptycho_adj128<false, 1, true>), P128_SMEM_RESID);
-            PT_ATTR((k_ptycho_adj128<false, 2, true>), P128_SMEM_RESID);
-            PT_ATTR((k_ptycho_adj128v<true, 2, false, true>), P128_SMEM_RESID);
-        }
-        if constexpr (DET == 128) {
-            PT_ATTR(k_ptycho_fwd128<true>, P128_SMEM);
-            PT_ATTR(k_ptycho_fwd128<false>, P128_SMEM);
-            PT_ATTR((k_ptycho_fwd128x<true>), P128X_SMEM);
-            PT_ATTR((k_ptycho_fwd128x<false>), P128X_SMEM);
-            PT_ATTR((k_ptycho_fwd128x<true, true>), P128X_SMEM);
-            PT_ATTR((k_ptycho_fwd128x<false, true>), P128X_SMEM);
-            PT_ATTR((k_ptycho_adj128x<true, 0>), P128X_SMEM);
-            PT_ATTR((k_ptycho_adj128x<false, 0>), P128X_SMEM);
-            PT_ATTR((k_ptycho_adj128x<true, 0, true>), P128X_SMEM);
-            PT_ATTR((k_ptycho_adj128x<false, 0, true>), P128X_SMEM);
             PT_ATTR((k_ptycho_adj128<true, 0>), P128_SMEM);
             PT_ATTR((k_ptycho_adj128<false, 0>), P128_SMEM);
-            PT_ATTR((k_ptycho_adj128<true, 1>), P128_SMEM_RESID);
-            PT_ATTR((k_ptycho_adj128<false, 1>), P128_SMEM_RESID);
-            PT_ATTR((k_ptycho_adj128<true, 2>), P128_SMEM_RESID);
-            PT_ATTR((k_ptycho_adj128<false, 2>), P128_SMEM_RESID);
-            PT_ATTR((k_ptycho_adj128v<true, 2, false>), P128_SMEM_RESID);
-            PT_ATTR((k_ptycho_adj128v<true, 0, true>), P128_SMEM);
-            PT_ATTR((k_ptycho_adj128v<true, 1, true>), P128_SMEM_RESID);
-            PT_ATTR((k_ptycho_adj128v<true, 2, true>), P128_SMEM_RESID);
+            PT_ATTR((k_ptycho_adj128<true, 0, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<false, 0, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 1>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<false, 1>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 1, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<false, 1, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 2>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<false, 2>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 2, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<false, 2, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 0, false, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 1, false, true>), P128_SMEM);
+            PT_ATTR((k_ptycho_adj128<true, 2, false, true>), P128_SMEM);
         }
     }
 #undef PT_ATTR
@@ -1421,37 +908,20 @@ int ptycho_adj_launch(pt_ptycho *h, float2 *out, const float2 *in, float scale, 
         using F = PF<DET>;
         float2 *dst = h->parts > 1 ? h->partial : out;
         const dim3 grid(h->parts, h->ntheta);
-        // the det = 128 adjoint prefetches frames (and counts) with 16-byte async copies
+        // the det = 128 adjoint (k_ptycho_adj128) for 16-byte aligned frames
         const bool fast128 = DET == 128 && ((uintptr_t)in % 16) == 0 && (RESID == 0 || (uintptr_t)data % 16 == 0);
-        const int smem = RESID ? P128_SMEM_RESID : P128_SMEM;
         // SUB: the sub-pixel model's per-frame probe tables (a separate
         // instantiation, so the reference model's kernels are unchanged)
         auto go = [&](auto sub) {
             constexpr bool S = decltype(sub)::value;
-            if (fast128 && h->P == DET) {
-                if constexpr (RESID == 2)
-                    k_ptycho_adj128v<true, RESID, false, S><<<grid, 512, smem, st>>>(
-                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
-                        h->tw128, data, dscale, nullptr, 0, h->shift_ids());
-                else if constexpr (RESID == 0)
-                    k_ptycho_adj128x<true, RESID, S><<<grid, 512, P128X_SMEM, st>>>(
-                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
-                        h->tw128, h->tw, data, dscale, h->shift_ids());
-                else
-                    k_ptycho_adj128<true, RESID, S><<<grid, 512, smem, st>>>(
-                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
-                        h->tw128, data, dscale, h->shift_ids());
-            }
-            else if (fast128) {
-                if constexpr (RESID == 0)
-                    k_ptycho_adj128x<false, RESID, S><<<grid, 512, P128X_SMEM, st>>>(
-                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
-                        h->tw128, h->tw, data, dscale, h->shift_ids());
-                else
-                    k_ptycho_adj128<false, RESID, S><<<grid, 512, smem, st>>>(
-                        in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale,
-                        h->tw128, data, dscale, h->shift_ids());
-            }
+            if (fast128 && h->P == DET)
+                k_ptycho_adj128<true, RESID, S><<<grid, 512, P128_SMEM, st>>>(
+                    in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale, h->tw128,
+                    h->tw, data, dscale, h->shift_ids());
+            else if (fast128)
+                k_ptycho_adj128<false, RESID, S><<<grid, 512, P128_SMEM, st>>>(
+                    in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale, h->tw128,
+                    h->tw, data, dscale, h->shift_ids());
             else
                 k_ptycho_adj<DET, RESID, S><<<grid, F::NT, F::SMEM, st>>>(
                     in, dst, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, h->P, scale, h->tw,
@@ -1496,11 +966,11 @@ int ptycho_run(pt_ptycho *h, bool adj, float2 *out, const float2 *in, float scal
         auto go = [&](auto sub) {
             constexpr bool S = decltype(sub)::value;
             if (fast128 && h->P == DET)
-                k_ptycho_fwd128x<true, S><<<grid128, 512, P128X_SMEM, st>>>(
+                k_ptycho_fwd128<true, S><<<grid128, 512, P128_SMEM, st>>>(
                     in, out, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, nframes, h->P, scale,
                     h->tw128, h->tw, h->shift_ids());
             else if (fast128)
-                k_ptycho_fwd128x<false, S><<<grid128, 512, P128X_SMEM, st>>>(
+                k_ptycho_fwd128<false, S><<<grid128, 512, P128_SMEM, st>>>(
                     in, out, h->corner, h->phase_tab(), h->probe_tab(), h->nz, h->n, h->nscan, nframes, h->P, scale,
                     h->tw128, h->tw, h->shift_ids());
             else
@@ -1556,15 +1026,14 @@ int probe_adj_launch(pt_ptycho *h, float2 *gprb, const float2 *in, const float2 
     } else {
         using F = PF<DET>;
         const int nframes = h->ntheta * h->nscan;
-        // det 128 with a 128 probe: the specialised adjoint in its probe mode (16-byte
-        // frame and count reads); smaller probes keep the generic kernel
+        // det 128 with a 128 probe: the two-exchange adjoint in its probe mode;
+        // smaller probes keep the generic kernel
         const bool fast128 = DET == 128 && h->P == DET && ((uintptr_t)in % 16) == 0 &&
                              (RESID == 0 || (uintptr_t)data % 16 == 0);
-        const int smem = RESID ? P128_SMEM_RESID : P128_SMEM;
         if (fast128)
-            k_ptycho_adj128v<true, RESID, true><<<h->prb_blocks, 512, smem, st>>>(
-                in, h->prb_part, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw128, data,
-                dscale, psi, nframes);
+            k_ptycho_adj128<true, RESID, false, true><<<h->prb_blocks, 512, P128_SMEM, st>>>(
+                in, h->prb_part, h->corner, h->phase, h->prbT, h->nz, h->n, h->nscan, h->P, scale, h->tw128, h->tw,
+                data, dscale, nullptr, psi, nframes);
         else
             k_ptycho_adj_probe<DET, RESID><<<h->prb_blocks, F::NT, F::SMEM, st>>>(
                 in, h->prb_part, psi, h->corner, h->phase, h->nz, h->n, h->nscan, nframes, h->P, scale, h->tw, data,
