@@ -91,7 +91,7 @@ def config_dict(c, extra=None):
 # 148 angles are one wave of one-slab angle blocks (parts x 148 blocks for a
 # split), the per-wave layout of the 384-angle workload, so the figure is
 # scaled by the frame count of the run.
-PTYCHO_ADJ128_DRAM_PER_FRAME = {1: (3691507712 + 500559104) / 25012, 3: (3956107008 + 983063552) / 25012}
+PTYCHO_ADJ128_DRAM_PER_FRAME = {1: (3675596800 + 500556032) / 25012, 3: (3934423552 + 988413184) / 25012}
 
 
 def traffic_source(parts):
