@@ -484,9 +484,9 @@ __device__ __forceinline__ void frame_r3_read(float2 (&w)[32], const float2 *ex)
 template <bool FULL, bool SUB = false>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_fwd128(const float2 *__restrict__ psi, float2 *__restrict__ g, const int *__restrict__ corner,
-                     const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
-                     int nframes, int P, float scale, const float4 *__restrict__ tw4,
-                     const float2 *__restrict__ w128, const int *__restrict__ sid = nullptr)
+                    const float2 *__restrict__ phase, const float2 *__restrict__ prbT, int nz, int n, int nscan,
+                    int nframes, int P, float scale, const float4 *__restrict__ tw4,
+                    const float2 *__restrict__ w128, const int *__restrict__ sid = nullptr)
 {
     extern __shared__ float4 sm4[];
     float2 *ex = reinterpret_cast<float2 *>(sm4);
@@ -578,10 +578,10 @@ __device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
 template <bool FULL, int RESID, bool SUB = false, bool PROBE = false>
 __global__ void __launch_bounds__(512, 1)
     k_ptycho_adj128(const float2 *__restrict__ g, float2 *dst, const int *__restrict__ corner,
-                     const float2 *__restrict__ phase, const float2 *prbT, int nz, int n, int nscan,
-                     int P, float scale, const float4 *__restrict__ tw4, const float2 *__restrict__ w128,
-                     const float *__restrict__ data, float dscale, const int *__restrict__ sid = nullptr,
-                     const float2 *psi = nullptr, int nframes = 0)
+                    const float2 *__restrict__ phase, const float2 *prbT, int nz, int n, int nscan,
+                    int P, float scale, const float4 *__restrict__ tw4, const float2 *__restrict__ w128,
+                    const float *__restrict__ data, float dscale, const int *__restrict__ sid = nullptr,
+                    const float2 *psi = nullptr, int nframes = 0)
 {
     extern __shared__ float4 sm4[];
     float2 *ex = reinterpret_cast<float2 *>(sm4);
