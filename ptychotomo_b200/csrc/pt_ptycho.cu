@@ -16,6 +16,11 @@
 //    accumulates conj(probe) x frame into its own slab; with parts > 1 the
 //    slabs are summed in a fixed order by a second kernel.  Deterministic,
 //    no atomics.
+//  Detector 128x128 (k_ptycho_fwd128, k_ptycho_adj128) splits the 2-D
+//    transform 16 x 8 by 4 x 32 instead, so a frame passes through shared
+//    memory twice rather than three times, with coalesced 256-byte warp
+//    accesses on both sides; one 512-thread block per SM.  The adjoint also
+//    serves the residual-on-load and probe adjoints.
 //  Detector 8x8 uses a plain shared-memory Stockham path.
 #include <algorithm>
 #include <cmath>
